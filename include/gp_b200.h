@@ -1,0 +1,181 @@
+/*
+ * gp_b200.h -- C ABI of the B200 grand-potential explicit step.
+ *
+ * Drop-in replacement for the explicit-Euler loop of MicroSim's
+ * Grand_potential_Finite_difference_2D solver (serial twin, 2D, isothermal,
+ * Function_F = 1 quadratic free energies).  Plain C types only: handles,
+ * pointers, sizes.  Every function returns 0 or a negative GP_E* code.
+ *
+ * The reference exposes its path as process-global state plus function-pointer
+ * "plugins" (functions/global_vars.h:384-415, bound in
+ * solverloop/initialize_functions_solverloop.h:4-58) and three step entry
+ * points called from main (microsim_gp.c:103-106):
+ *     solverloop_phasefield(start, end)      solverloop/solverloop.h:21
+ *     apply_boundary_conditions(0)           solverloop/boundary_serial.h:176
+ *     solverloop_concentration(start, end)   solverloop/solverloop.h:35
+ * Here the same step is one call on an opaque context; the plugin choices
+ * (Function_W, Function_anisotropy, BINARY/TERNARY/DILUTE) are fields of
+ * gp_model.  Paths below are relative to Grand_potential_Finite_difference_2D_serial/.
+ *
+ * Field layout at this boundary: interior cells only, structure of arrays,
+ * double precision, plane-major: phi[a][x][y] with y fastest (the reference's
+ * index y + x*rows_y with the three ghost layers removed), then
+ * mu[k][x][y].  Ghost layers are never stored: the Neumann and periodic copies
+ * of the reference are applied as index maps when a kernel reads past an edge.
+ */
+#ifndef GP_B200_H_
+#define GP_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GP_MAX_PHASES 6 /* NUMPHASES supported by the kernels               */
+#define GP_MAX_K1 3     /* NUMCOMPONENTS-1 supported by the kernels         */
+#define GP_NAME_LEN 52  /* Phases/Components names (reference: 51 chars)    */
+
+/* error codes */
+#define GP_OK 0
+#define GP_E_ARG -1         /* bad argument / NULL pointer                          */
+#define GP_E_IO -2          /* file could not be opened / read / written            */
+#define GP_E_PARSE -3       /* Input.in / Filling.in content not understood        */
+#define GP_E_UNSUPPORTED -4 /* input asks for a feature outside this path          */
+#define GP_E_CUDA -5        /* CUDA runtime error                                  */
+#define GP_E_NONFINITE -6   /* NaN/Inf found in the fields (stability watchdog)    */
+#define GP_E_NOMEM -7       /* host or device allocation failed                    */
+#define GP_E_TIMEOUT -8     /* a bounded device wait gave up                        */
+#define GP_E_SIZE -9        /* request exceeds a documented size limit              */
+
+/* mu-update solver, calculate_divergence_concentration.h:238-270 */
+#define GP_MU_BINARY 0  /* BINARY = 1: 1/x                         */
+#define GP_MU_TERNARY 1 /* TERNARY = 1: closed-form 2x2 inverse    */
+#define GP_MU_DILUTE 2  /* DILUTE = 1: diagonal                    */
+#define GP_MU_LU 3      /* none set: the reference's LU inverse    */
+
+/* precision of a device context */
+#define GP_FP64 0 /* plain form: FP64 storage and arithmetic, bit-faithful to the reference */
+#define GP_FP32 1 /* chosen form: FP32 storage/update, FP64 reductions                       */
+
+/* boundary types, functions/utility_functions.h:471-653 */
+#define GP_BC_NEUMANN 1
+#define GP_BC_PERIODIC 3
+
+/*
+ * Model constants of one simulation instance, all derived on the host with
+ * the reference's own operation order (functions/functionF_01.h:169-230
+ * init_propertymatrices, functions/matrix.h:50 matinvnew,
+ * functions/utility_functions.h:700 populate_rotation_matrix) so that the
+ * device step reproduces the reference's doubles.
+ */
+typedef struct gp_model {
+  int32_t N;  /* NUMPHASES (last phase = liquid)      */
+  int32_t K1; /* NUMCOMPONENTS - 1                     */
+  int64_t mesh_x, mesh_y;
+  double dx, dy, dt;
+  double epsilon, tau; /* interface width; FunctionTau fallback */
+  double T, Teq;
+  int32_t obstacle;   /* 1: Function_W=1 obstacle, 0: Function_W=2 well */
+  int32_t anisotropy; /* Function_anisotropy (4-fold cubic when 1)      */
+  int32_t mu_solver;  /* GP_MU_*                                        */
+  int32_t bc_phi[4];  /* boundary[0..3] for phi: x-lo, x-hi, y-hi, y-lo */
+  int32_t bc_mu[4];   /* same for mu                                    */
+  int32_t pad0;
+  double Gamma[GP_MAX_PHASES][GP_MAX_PHASES];
+  double Gamma_abc[GP_MAX_PHASES][GP_MAX_PHASES][GP_MAX_PHASES];
+  double tau_ab[GP_MAX_PHASES][GP_MAX_PHASES];
+  double dab[GP_MAX_PHASES][GP_MAX_PHASES];
+  double R[GP_MAX_PHASES][GP_MAX_PHASES][2][2];    /* Rotation_matrix, 2x2 block     */
+  double Rinv[GP_MAX_PHASES][GP_MAX_PHASES][2][2]; /* Inv_Rotation_matrix, 2x2 block */
+  double cmu[GP_MAX_PHASES][GP_MAX_K1][GP_MAX_K1];  /* (d mu/dc)^-1                  */
+  double A[GP_MAX_PHASES][GP_MAX_K1][GP_MAX_K1];
+  double Beff[GP_MAX_PHASES][GP_MAX_K1]; /* Beq + dBbdT*(T - Teq) (c_mu, Mu at T)     */
+  double Bfill[GP_MAX_PHASES][GP_MAX_K1]; /* Beq + dBbdT*(Teq - Teq) (filling)        */
+  double B[GP_MAX_PHASES][GP_MAX_K1];    /* B(T) of free_energy                        */
+  double C[GP_MAX_PHASES];               /* C(T) of free_energy                        */
+  double Diff[GP_MAX_PHASES][GP_MAX_K1][GP_MAX_K1];
+  /* constants folded on the host exactly as the reference evaluates them */
+  double inv_eps;     /* 1.0/epsilon                                */
+  double w_obstacle;  /* 16.0/(M_PI*M_PI)                           */
+  double jat_obst;    /* -0.25*M_PI*epsilon                         */
+  double jat_well;    /* -1.0*epsilon                               */
+  double s_well;      /* 0.5/sqrt(2.0)                              */
+} gp_model;
+
+/* Parsed Input.in (+ its BOUNDARY lines) and Filling.in. */
+typedef struct gp_input gp_input;
+
+/* Running statistics, microsim_gp.c:139-148 (interior cells; FP64). */
+typedef struct gp_stats {
+  double phi_max[GP_MAX_PHASES], phi_min[GP_MAX_PHASES], rel_change_phi[GP_MAX_PHASES];
+  double mu_max[GP_MAX_K1], mu_min[GP_MAX_K1], rel_change_mu[GP_MAX_K1];
+  double solute[GP_MAX_K1]; /* sum over cells of sum_a c_a(mu) h_a(phi) (file_writer.h:203-235 integrand) */
+  double phase_fraction[GP_MAX_PHASES]; /* sum over cells of phi_a                                      */
+  int64_t nonfinite;  /* number of non-finite phi/mu values found                                         */
+} gp_stats;
+
+/* ---------------- host side: files (reference L3/L4) ---------------- */
+
+/* Parse Input.in with the reference's line grammar and key order rules
+ * (functions/reading_input_parameters.h:1-308, read_boundary_conditions.h:4-57).
+ * filling_in may be NULL (no FILL* lines). */
+int gp_input_read(const char *input_in, const char *filling_in, gp_input **out);
+void gp_input_free(gp_input *in);
+/* Simple scalar queries on a parsed input (NTIMESTEPS, SAVET, ...). Returns
+ * GP_E_ARG for an unknown key. */
+int gp_input_get_long(const gp_input *in, const char *key, int64_t *value);
+int gp_input_get_double(const gp_input *in, const char *key, double *value);
+/* Phase (which = 0) or component (which = 1) name, verbatim (leading blanks kept). */
+int gp_input_name(const gp_input *in, int which, int index, char *buf, size_t len);
+
+/* Derive the model constants (initialize_variables.h:4-28, init_propertymatrices). */
+int gp_model_from_input(const gp_input *in, gp_model *out);
+
+/* Initial fields from the FILL* lines (functions/fill_domain.h:4-151,
+ * functions/filling.h:6-270): phi[N][mx][my], mu[K1][mx][my], interior only. */
+int gp_fill(const gp_input *in, const gp_model *m, double *phi, double *mu);
+
+/* Write DATA/<out>_<t>.vtk (solverloop/file_writer.h:23-255), BINARY or ASCII
+ * as Input.in's WRITEFORMAT says; Composition_* fields when Writecomposition. */
+int gp_write_vtk(const gp_input *in, const gp_model *m, const char *path, const double *phi, const double *mu);
+/* Read fields back (solverloop/file_writer.h:256-386, restart). */
+int gp_read_vtk(const gp_input *in, const gp_model *m, const char *path, double *phi, double *mu);
+
+/* ---------------- device side: the step (reference L2 + L1) ---------------- */
+
+typedef struct gp_ctx gp_ctx;
+
+/* Allocate device state for one instance on the current CUDA device.
+ * precision: GP_FP64 (plain) or GP_FP32 (chosen form). */
+int gp_create(const gp_model *m, int precision, gp_ctx **out);
+int gp_destroy(gp_ctx *ctx);
+/* Host <-> device copies of the interior fields (double on the host side). */
+int gp_upload(gp_ctx *ctx, const double *phi, const double *mu);
+int gp_download(gp_ctx *ctx, double *phi, double *mu);
+/* nsteps explicit steps: phase-field half step, ghost fill, concentration
+ * half step, ghost fill -- microsim_gp.c:102-106 for t = 1..nsteps.
+ * Asynchronous on the context's stream; errors of earlier launches surface here
+ * or in gp_sync. */
+int gp_step(gp_ctx *ctx, int64_t nsteps);
+int gp_sync(gp_ctx *ctx);
+/* FP64 statistics of the current state (max/min/rel-change of the last step,
+ * solute and phase sums, NaN watchdog). Synchronous. */
+int gp_get_stats(gp_ctx *ctx, gp_stats *out);
+/* Delta-phi of the most recent phase-field half step on the interior plus one
+ * ring, dphi[N][mx+2][my+2] (FP64 context only; for tests). */
+int gp_download_dphi(gp_ctx *ctx, double *dphi);
+/* The CUDA stream (cudaStream_t) the context launches on. */
+void *gp_stream(gp_ctx *ctx);
+/* Number of kernel launches this context issued since creation. */
+int64_t gp_launch_count(const gp_ctx *ctx);
+/* sizeof(gp_model) as compiled into the library (binding layout check). */
+size_t gp_model_sizeof(void);
+/* Text of the last error on this thread. */
+const char *gp_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

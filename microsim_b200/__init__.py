@@ -1,0 +1,257 @@
+"""B200-native grand-potential explicit step (MicroSim GP solver drop-in).
+
+Thin Python binding over the C ABI of ``include/gp_b200.h`` (``libgp_b200.so``,
+built in-tree).  Everything that computes runs in that library: the host I/O
+(Input.in / Filling.in / VTK with the reference's semantics) and the sm_100a
+kernels.  There is no Python or CPU fallback: if the library is missing the
+import of :func:`lib` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgp_b200.so")
+DRIVER_PATH = os.path.join(HERE, "microsim_gp_b200")
+
+GP_MAX_PHASES = 6
+GP_MAX_K1 = 3
+GP_NAME_LEN = 52
+
+GP_OK, GP_E_ARG, GP_E_IO, GP_E_PARSE, GP_E_UNSUPPORTED, GP_E_CUDA, GP_E_NONFINITE, GP_E_NOMEM, \
+    GP_E_TIMEOUT, GP_E_SIZE = 0, -1, -2, -3, -4, -5, -6, -7, -8, -9
+GP_MU_BINARY, GP_MU_TERNARY, GP_MU_DILUTE, GP_MU_LU = 0, 1, 2, 3
+GP_FP64, GP_FP32 = 0, 1
+GP_BC_NEUMANN, GP_BC_PERIODIC = 1, 3
+
+_P, _K = GP_MAX_PHASES, GP_MAX_K1
+
+
+class GpModel(C.Structure):
+    """ctypes mirror of ``gp_model`` (layout checked against gp_model_sizeof())."""
+    _fields_ = [
+        ("N", C.c_int32), ("K1", C.c_int32),
+        ("mesh_x", C.c_int64), ("mesh_y", C.c_int64),
+        ("dx", C.c_double), ("dy", C.c_double), ("dt", C.c_double),
+        ("epsilon", C.c_double), ("tau", C.c_double), ("T", C.c_double), ("Teq", C.c_double),
+        ("obstacle", C.c_int32), ("anisotropy", C.c_int32), ("mu_solver", C.c_int32),
+        ("bc_phi", C.c_int32 * 4), ("bc_mu", C.c_int32 * 4), ("pad0", C.c_int32),
+        ("Gamma", C.c_double * (_P * _P)),
+        ("Gamma_abc", C.c_double * (_P * _P * _P)),
+        ("tau_ab", C.c_double * (_P * _P)),
+        ("dab", C.c_double * (_P * _P)),
+        ("R", C.c_double * (_P * _P * 4)),
+        ("Rinv", C.c_double * (_P * _P * 4)),
+        ("cmu", C.c_double * (_P * _K * _K)),
+        ("A", C.c_double * (_P * _K * _K)),
+        ("Beff", C.c_double * (_P * _K)),
+        ("Bfill", C.c_double * (_P * _K)),
+        ("B", C.c_double * (_P * _K)),
+        ("C", C.c_double * _P),
+        ("Diff", C.c_double * (_P * _K * _K)),
+        ("inv_eps", C.c_double), ("w_obstacle", C.c_double), ("jat_obst", C.c_double),
+        ("jat_well", C.c_double), ("s_well", C.c_double),
+    ]
+
+    def arr(self, name):
+        """numpy view of an array field with its natural shape."""
+        shapes = {"Gamma": (_P, _P), "Gamma_abc": (_P, _P, _P), "tau_ab": (_P, _P), "dab": (_P, _P),
+                  "R": (_P, _P, 2, 2), "Rinv": (_P, _P, 2, 2), "cmu": (_P, _K, _K), "A": (_P, _K, _K),
+                  "Beff": (_P, _K), "Bfill": (_P, _K), "B": (_P, _K), "C": (_P,), "Diff": (_P, _K, _K)}
+        return np.ctypeslib.as_array(getattr(self, name)).reshape(shapes[name])
+
+    def copy(self) -> "GpModel":
+        m = GpModel()
+        C.memmove(C.byref(m), C.byref(self), C.sizeof(GpModel))
+        return m
+
+
+class GpStats(C.Structure):
+    _fields_ = [
+        ("phi_max", C.c_double * _P), ("phi_min", C.c_double * _P), ("rel_change_phi", C.c_double * _P),
+        ("mu_max", C.c_double * _K), ("mu_min", C.c_double * _K), ("rel_change_mu", C.c_double * _K),
+        ("solute", C.c_double * _K), ("phase_fraction", C.c_double * _P), ("nonfinite", C.c_int64),
+    ]
+
+
+_lib = None
+
+_SIGS = {
+    "gp_input_read": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "gp_input_free": (None, [C.c_void_p]),
+    "gp_input_get_long": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64)]),
+    "gp_input_get_double": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double)]),
+    "gp_input_name": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t]),
+    "gp_model_from_input": (C.c_int, [C.c_void_p, C.POINTER(GpModel)]),
+    "gp_fill": (C.c_int, [C.c_void_p, C.POINTER(GpModel), C.c_void_p, C.c_void_p]),
+    "gp_write_vtk": (C.c_int, [C.c_void_p, C.POINTER(GpModel), C.c_char_p, C.c_void_p, C.c_void_p]),
+    "gp_read_vtk": (C.c_int, [C.c_void_p, C.POINTER(GpModel), C.c_char_p, C.c_void_p, C.c_void_p]),
+    "gp_create": (C.c_int, [C.POINTER(GpModel), C.c_int, C.POINTER(C.c_void_p)]),
+    "gp_destroy": (C.c_int, [C.c_void_p]),
+    "gp_upload": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gp_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gp_step": (C.c_int, [C.c_void_p, C.c_int64]),
+    "gp_sync": (C.c_int, [C.c_void_p]),
+    "gp_get_stats": (C.c_int, [C.c_void_p, C.POINTER(GpStats)]),
+    "gp_download_dphi": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gp_stream": (C.c_void_p, [C.c_void_p]),
+    "gp_launch_count": (C.c_int64, [C.c_void_p]),
+    "gp_model_sizeof": (C.c_size_t, []),
+    "gp_last_error": (C.c_char_p, []),
+}
+
+
+def lib():
+    """Load libgp_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `make -C {HERE}` (or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        if L.gp_model_sizeof() != C.sizeof(GpModel):
+            raise ImportError("gp_model layout mismatch between binding and library")
+        _lib = L
+    return _lib
+
+
+class GpError(RuntimeError):
+    def __init__(self, what: str, rc: int):
+        msg = lib().gp_last_error() or b""
+        super().__init__(f"{what} failed ({rc}): {msg.decode(errors='replace')}")
+        self.rc = rc
+
+
+def _check(what, rc):
+    if rc != GP_OK:
+        raise GpError(what, rc)
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data
+
+
+class Input:
+    """Parsed Input.in + Filling.in (reference semantics, C side)."""
+
+    def __init__(self, input_in: str, filling_in: str | None = None):
+        h = C.c_void_p()
+        _check("gp_input_read", lib().gp_input_read(input_in.encode(), filling_in.encode() if filling_in else None,
+                                                     C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().gp_input_free(self._h)
+            self._h = None
+
+    def get_long(self, key: str) -> int:
+        v = C.c_int64()
+        _check("gp_input_get_long(%s)" % key, lib().gp_input_get_long(self._h, key.encode(), C.byref(v)))
+        return v.value
+
+    def get_double(self, key: str) -> float:
+        v = C.c_double()
+        _check("gp_input_get_double(%s)" % key, lib().gp_input_get_double(self._h, key.encode(), C.byref(v)))
+        return v.value
+
+    def name(self, which: int, index: int) -> str:
+        buf = C.create_string_buffer(GP_NAME_LEN)
+        _check("gp_input_name", lib().gp_input_name(self._h, which, index, buf, GP_NAME_LEN))
+        return buf.value.decode()
+
+    def model(self) -> GpModel:
+        m = GpModel()
+        _check("gp_model_from_input", lib().gp_model_from_input(self._h, C.byref(m)))
+        return m
+
+    def fill(self, m: GpModel):
+        phi = np.zeros((m.N, m.mesh_x, m.mesh_y))
+        mu = np.zeros((m.K1, m.mesh_x, m.mesh_y))
+        _check("gp_fill", lib().gp_fill(self._h, C.byref(m), _ptr(phi), _ptr(mu)))
+        return phi, mu
+
+    def write_vtk(self, m: GpModel, path: str, phi: np.ndarray, mu: np.ndarray):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)  # held: the C call reads them
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        _check("gp_write_vtk", lib().gp_write_vtk(self._h, C.byref(m), path.encode(), _ptr(phi), _ptr(mu)))
+
+    def read_vtk(self, m: GpModel, path: str):
+        phi = np.zeros((m.N, m.mesh_x, m.mesh_y))
+        mu = np.zeros((m.K1, m.mesh_x, m.mesh_y))
+        _check("gp_read_vtk", lib().gp_read_vtk(self._h, C.byref(m), path.encode(), _ptr(phi), _ptr(mu)))
+        return phi, mu
+
+
+class Context:
+    """One simulation instance resident on the current CUDA device."""
+
+    def __init__(self, model: GpModel, precision: int = GP_FP64):
+        h = C.c_void_p()
+        self.model = model.copy()
+        _check("gp_create", lib().gp_create(C.byref(self.model), precision, C.byref(h)))
+        self._h = h
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gp_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload(self, phi: np.ndarray, mu: np.ndarray):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)  # held: the C call reads them
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        _check("gp_upload", lib().gp_upload(self._h, _ptr(phi), _ptr(mu)))
+
+    def download(self):
+        m = self.model
+        phi = np.empty((m.N, m.mesh_x, m.mesh_y))
+        mu = np.empty((m.K1, m.mesh_x, m.mesh_y))
+        _check("gp_download", lib().gp_download(self._h, _ptr(phi), _ptr(mu)))
+        return phi, mu
+
+    def download_dphi(self):
+        m = self.model
+        d = np.empty((m.N, m.mesh_x + 2, m.mesh_y + 2))
+        _check("gp_download_dphi", lib().gp_download_dphi(self._h, _ptr(d)))
+        return d
+
+    def step(self, nsteps: int = 1):
+        _check("gp_step", lib().gp_step(self._h, int(nsteps)))
+
+    def sync(self):
+        _check("gp_sync", lib().gp_sync(self._h))
+
+    def stats(self, allow_nonfinite: bool = False) -> dict:
+        st = GpStats()
+        rc = lib().gp_get_stats(self._h, C.byref(st))
+        if rc != GP_OK and not (allow_nonfinite and rc == GP_E_NONFINITE):
+            raise GpError("gp_get_stats", rc)
+        N, K1 = self.model.N, self.model.K1
+        out = {n: np.array(getattr(st, n)[: (N if ("phi" in n or "phase" in n) else K1)])
+               for n, _ in GpStats._fields_ if n != "nonfinite"}
+        out["nonfinite"] = st.nonfinite
+        return out
+
+    @property
+    def stream(self) -> int:
+        return lib().gp_stream(self._h) or 0
+
+    @property
+    def launches(self) -> int:
+        return lib().gp_launch_count(self._h)

@@ -1,0 +1,135 @@
+/*
+ * gp_driver.c -- `microsim_gp_b200 Input.in Filling.in Out [fp64|fp32]`
+ *
+ * Drop-in for the reference's CLI driver (Grand_potential_Finite_difference_2D_serial/
+ * microsim_gp.c:41-151): same arguments, same DATA/<Out>_<t>.vtk files every
+ * SAVET steps, same DATA/shift.dat lines and the same progress lines every
+ * TRACK_PROGRESS steps, with the time loop running on the GPU through the C ABI.
+ * The optional fourth argument (or GP_PRECISION=fp32) selects the FP32 form.
+ *
+ * Differences, stated: the progress extrema are sampled when they are printed
+ * (the reference updates them every step, ghost rings included); NSMOOTH > 1,
+ * Shift = 1 and non-isothermal inputs are rejected with a message.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+
+#include "gp_b200.h"
+
+static int fail(const char *what, int rc) {
+  fprintf(stderr, "microsim_gp_b200: %s failed (%d): %s\n", what, rc, gp_last_error());
+  return 1;
+}
+
+int main(int argc, char *argv[]) {
+  gp_input *in = NULL;
+  gp_model m;
+  gp_ctx *ctx = NULL;
+  int64_t ntimesteps, saveT, nsmooth, starttime, restart, track, shift;
+  int precision = GP_FP64;
+  int rc;
+  if (argc < 4) {
+    fprintf(stderr, "usage: %s Input.in Filling.in Out [fp64|fp32]\n", argv[0]);
+    return 2;
+  }
+  if ((argc > 4 && !strcmp(argv[4], "fp32")) || (getenv("GP_PRECISION") && !strcmp(getenv("GP_PRECISION"), "fp32")))
+    precision = GP_FP32;
+  mkdir("DATA", 0777);
+  if ((rc = gp_input_read(argv[1], argv[2], &in)) != GP_OK) return fail("reading inputs", rc);
+  if ((rc = gp_model_from_input(in, &m)) != GP_OK) return fail("model constants", rc);
+  gp_input_get_long(in, "NTIMESTEPS", &ntimesteps);
+  gp_input_get_long(in, "SAVET", &saveT);
+  gp_input_get_long(in, "NSMOOTH", &nsmooth);
+  gp_input_get_long(in, "STARTTIME", &starttime);
+  gp_input_get_long(in, "RESTART", &restart);
+  gp_input_get_long(in, "TRACK_PROGRESS", &track);
+  gp_input_get_long(in, "Shift", &shift);
+  if (nsmooth > 1) {
+    fprintf(stderr, "microsim_gp_b200: NSMOOTH=%lld pre-steps are not implemented here; set NSMOOTH <= 1\n",
+            (long long)nsmooth);
+    return 1;
+  }
+  if (shift) {
+    fprintf(stderr, "microsim_gp_b200: Shift=1 (moving frame) is not implemented here\n");
+    return 1;
+  }
+  if (saveT <= 0) saveT = ntimesteps > 0 ? ntimesteps : 1;
+  const size_t np = (size_t)m.mesh_x * (size_t)m.mesh_y;
+  double *phi = (double *)malloc(sizeof(double) * np * m.N);
+  double *mu = (double *)malloc(sizeof(double) * np * m.K1);
+  if (!phi || !mu) return fail("host allocation", GP_E_NOMEM);
+  char name[1200];
+  if (starttime == 0 && restart == 0) {
+    if ((rc = gp_fill(in, &m, phi, mu)) != GP_OK) return fail("filling", rc);
+  } else {
+    snprintf(name, sizeof name, "DATA/%s_%lld.vtk", argv[3], (long long)starttime);
+    if ((rc = gp_read_vtk(in, &m, name, phi, mu)) != GP_OK) return fail("restart read", rc);
+  }
+  if ((rc = gp_create(&m, precision, &ctx)) != GP_OK) return fail("gp_create", rc);
+  if ((rc = gp_upload(ctx, phi, mu)) != GP_OK) return fail("gp_upload", rc);
+  if (restart == 0 || starttime == 0) {
+    snprintf(name, sizeof name, "DATA/%s_%lld.vtk", argv[3], (long long)0);
+    if ((rc = gp_write_vtk(in, &m, name, phi, mu)) != GP_OK) return fail("vtk write", rc);
+  }
+  int max_length = 0, a, k;
+  char pname[GP_MAX_PHASES][GP_NAME_LEN], cname[GP_MAX_K1][GP_NAME_LEN];
+  for (a = 0; a < m.N; a++) {
+    gp_input_name(in, 0, a, pname[a], GP_NAME_LEN);
+    if ((int)strlen(pname[a]) > max_length) max_length = (int)strlen(pname[a]);
+  }
+  for (k = 0; k < m.K1; k++) {
+    gp_input_name(in, 1, k, cname[k], GP_NAME_LEN);
+    if ((int)strlen(cname[k]) > max_length) max_length = (int)strlen(cname[k]);
+  }
+  int64_t t = 0;
+  while (t < ntimesteps) {
+    /* advance to the next step that writes or prints (microsim_gp.c:129-148) */
+    int64_t next = ntimesteps;
+    int64_t ns = (t / saveT + 1) * saveT;
+    if (ns < next) next = ns;
+    if (track > 0) {
+      int64_t nt = (t / track + 1) * track;
+      if (nt < next) next = nt;
+    }
+    if ((rc = gp_step(ctx, next - t)) != GP_OK) return fail("gp_step", rc);
+    t = next;
+    if (t % saveT == 0) {
+      if ((rc = gp_download(ctx, phi, mu)) != GP_OK) return fail("gp_download", rc);
+      snprintf(name, sizeof name, "DATA/%s_%lld.vtk", argv[3], (long long)(t + starttime));
+      if ((rc = gp_write_vtk(in, &m, name, phi, mu)) != GP_OK) return fail("vtk write", rc);
+      FILE *fp = fopen("DATA/shift.dat", "a");
+      if (fp) {
+        fprintf(fp, "%ld %ld\n", (long)(t + starttime), (long)0);
+        fclose(fp);
+      }
+    }
+    if (track > 0 && t % track == 0) {
+      gp_stats st;
+      rc = gp_get_stats(ctx, &st);
+      if (rc != GP_OK && rc != GP_E_NONFINITE) return fail("gp_get_stats", rc);
+      double dt;
+      gp_input_get_double(in, "DELTA_t", &dt);
+      fprintf(stdout, "Time=%le\n", t * dt);
+      for (a = 0; a < m.N; a++)
+        fprintf(stdout, "%*s, Max = %le, Min = %le, Relative_Change=%le\n", max_length, pname[a], st.phi_max[a],
+                st.phi_min[a], sqrt(st.rel_change_phi[a]));
+      for (k = 0; k < m.K1; k++)
+        fprintf(stdout, "%*s, Max = %le, Min = %le, Relative_Change=%le\n", max_length, cname[k], st.mu_max[k],
+                st.mu_min[k], sqrt(st.rel_change_mu[k]));
+      fprintf(stdout, "\n");
+      if (rc == GP_E_NONFINITE) {
+        fprintf(stderr, "microsim_gp_b200: non-finite values at t=%lld (unstable DELTA_t?)\n", (long long)t);
+        return 3;
+      }
+    }
+  }
+  if ((rc = gp_sync(ctx)) != GP_OK) return fail("gp_sync", rc);
+  gp_destroy(ctx);
+  gp_input_free(in);
+  free(phi);
+  free(mu);
+  return 0;
+}
