@@ -170,6 +170,22 @@ int gp_download_dphi(gp_ctx *ctx, double *dphi);
 void *gp_stream(gp_ctx *ctx);
 /* Number of kernel launches this context issued since creation. */
 int64_t gp_launch_count(const gp_ctx *ctx);
+/* One plain (FP64) step that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that own their device buffers and cannot
+ * allocate device memory (a framework pool that owns the whole GPU, a fixed
+ * start-up memory budget).  phi/mu (inputs) and phi_out/mu_out (outputs) are
+ * device buffers in this header's layout with the given row pitch (elements,
+ * >= mesh_y; plane stride mesh_x*pitch); inputs and outputs must differ.  The
+ * Delta-phi ring between the step's two kernels lives in a fixed device array of
+ * GP_NOALLOC_SCRATCH_BYTES per GPU, held until the process exits and shared by
+ * every call (contents of the last call kept; calls that overlap on the GPU
+ * race on it).  Grids needing more than N*(mesh_x+2)*round_up(mesh_y+2,32)
+ * doubles of it get GP_E_SIZE.  The first call on a device looks up the array's
+ * address and should come before any stream capture.  stream: a cudaStream_t
+ * (NULL = legacy default stream); the call is asynchronous on it. */
+#define GP_NOALLOC_SCRATCH_BYTES (8u << 20)
+int gp_step_f64_noalloc(const gp_model *m, const double *phi, const double *mu, double *phi_out, double *mu_out,
+                        int64_t pitch, void *stream);
 /* sizeof(gp_model) as compiled into the library (binding layout check). */
 size_t gp_model_sizeof(void);
 /* Text of the last error on this thread. */
