@@ -191,6 +191,43 @@ def run_reference_arm(args, world, rank):
 
 # --------------------------------------------------------------------------------------------- our arm
 
+def prepare(models, fields, steps):
+    """Advance the synthetic initial state `steps` steps with the FP32 form (input
+    preparation, before any timing): the benchmark state is the workload part-way
+    through its run, where the interface has grown, instead of the first steps of a
+    small seed."""
+    import microsim_b200 as mb
+    if steps <= 0:
+        return fields
+    with mb.Batch(models) as b:
+        for i, (p, u) in enumerate(fields):
+            b.upload(i, p, u)
+        b.step(steps)
+        b.sync()
+        return [b.download(i) for i in range(len(models))]
+
+
+def timed_single(ctx, steps, warmup, flush, stream):
+    """Per-step CUDA events on the context's stream, L2 flushed between steps."""
+    import torch
+    for _ in range(warmup):
+        ctx.step(1)
+    ctx.sync()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    l0 = ctx.launches
+    for i in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            evs[i][0].record(stream)
+        ctx.step(1)
+        with torch.cuda.stream(stream):
+            evs[i][1].record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs), ctx.launches - l0
+
+
 def run_ours(args, world, rank, local):
     import torch
     import microsim_b200 as mb
@@ -198,106 +235,128 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     wname, cases = workload(args.workload)
-    case = cases[0]
-    prec = mb.GP_FP32 if args.precision == "fp32" else mb.GP_FP64
-    with tempfile.TemporaryDirectory() as d:
-        ip, fp = case.write(d)
-        inp = mb.Input(ip, fp)
-        m = inp.model()
-        phi0, mu0 = inp.fill(m)
-    try:
+    loaded = [mb.load_case(c) for c in cases]
+    models = [m for m, _, _ in loaded]
+    prep = args.prep_steps if args.prep_steps >= 0 else {"c2": 25000, "c1": 5000, "c4": 2500}[args.workload]
+    fields = prepare(models, [(p, u) for _, p, u in loaded], prep)
+    cells = sum(m.mesh_x * m.mesh_y for m in models)
+    N, K1 = models[0].N, models[0].K1
+    peak, peak_kind = measured_peaks()
+    fp64 = None
+    barrier(world)
+    if len(models) == 1:
+        m = models[0]
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        prec = mb.GP_FP32 if args.precision == "fp32" else mb.GP_FP64
         ctx = mb.Context(m, prec)
-    except mb.GpError as e:
-        if prec == mb.GP_FP32 and e.rc == mb.GP_E_UNSUPPORTED:
-            prec = mb.GP_FP64
-            args.precision = "fp64"
-            ctx = mb.Context(m, prec)
-        else:
-            raise
-    ctx.upload(phi0, mu0)
-    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    cells = m.mesh_x * m.mesh_y
-    N, K1 = m.N, m.K1
-    esize = 4 if prec == mb.GP_FP32 else 8
-    alg_bytes = 2 * (N + K1) * esize  # read and write phi, mu once per cell-update
-
-    for _ in range(args.warmup):
-        ctx.step(1)
-    ctx.sync()
-    barrier(world)
-    torch.cuda.synchronize()
-    l0 = ctx.launches
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with ClockSampler(local) as clk:
-        for i in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-                evs[i][0].record(stream)
-            ctx.step(1)
-            with torch.cuda.stream(stream):
-                evs[i][1].record(stream)
+        ctx.upload(*fields[0])
+        stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+        with ClockSampler(local) as clk:
+            ms, launches = timed_single(ctx, args.steps, args.warmup, flush, stream)
+        l2 = "flushed between timed steps (256 MiB write outside the events)"
+        if prec == mb.GP_FP32 and not args.no_fp64:
+            c64 = mb.Context(m, mb.GP_FP64)
+            c64.upload(*fields[0])
+            s64 = torch.cuda.ExternalStream(c64.stream, device=dev)
+            ms64, _ = timed_single(c64, args.steps, args.warmup, flush, s64)
+            c64.close()
+            ms64 = allmax(ms64, world)
+            fp64 = {"value": world * cells * args.steps / (ms64 / 1e3), "unit": UNIT,
+                    "ms_per_step": ms64 / args.steps}
+    else:
+        prec = mb.GP_FP32
+        ctx = mb.Batch(models)
+        for i, f in enumerate(fields):
+            ctx.upload(i, *f)
+        if args.autotune:
+            ctx.autotune(os.path.join(ROOT, "microsim_b200", "tile_cache.txt"))
+        stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+        ctx.step(args.warmup)
         ctx.sync()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.launches
+        with ClockSampler(local) as clk:
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+            ctx.step(args.steps)
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            ctx.sync()
+        launches = ctx.launches - l0
+        ms = e0.elapsed_time(e1)
+        l2 = "inputs larger than L2 (state %.0f MB per buffer)" % (cells * (N + K1) * 4 / 1e6)
     torch.cuda.synchronize()
     barrier(world)
-    launches = ctx.launches - l0
-    ms = sum(a.elapsed_time(b) for a, b in evs)
     ms = allmax(ms, world)
     step_ms = ms / args.steps
     value = world * cells * args.steps / (ms / 1e3)
-    per_gpu = cells / (step_ms / 1e3)
-    peak, peak_kind = measured_peaks()
-    achieved = per_gpu * alg_bytes / 1e9
+    esize = 4 if prec == mb.GP_FP32 else 8
+    alg_bytes = 2 * (N + K1) * esize
+    achieved = cells / (step_ms / 1e3) * alg_bytes / 1e9
 
     # end to end through the C ABI: pinned host state in, K steps with the
     # progress statistics read back each step, state out
-    ph_t = torch.empty(phi0.shape, dtype=torch.float64, pin_memory=True)
-    mu_t = torch.empty(mu0.shape, dtype=torch.float64, pin_memory=True)
-    ph_h, mu_h = ph_t.numpy(), mu_t.numpy()
-    ph_h[...] = phi0
-    mu_h[...] = mu0
-    ctx.sync()
+    pinned = []
+    for p, u in fields:
+        pt = torch.empty(p.shape, dtype=torch.float64, pin_memory=True)
+        ut = torch.empty(u.shape, dtype=torch.float64, pin_memory=True)
+        pt.numpy()[...] = p
+        ut.numpy()[...] = u
+        pinned.append((pt.numpy(), ut.numpy()))
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         e0.record(stream)
-    ctx.upload(ph_h, mu_h)
-    for _ in range(args.steps):
-        ctx.step(1)
-        ctx.stats(allow_nonfinite=True)
-    out_p, out_m = ctx.download()
+    if len(models) == 1:
+        ctx.upload(*pinned[0])
+        for _ in range(args.steps):
+            ctx.step(1)
+            ctx.stats(allow_nonfinite=True)
+        ctx.download()
+    else:
+        for i, (p, u) in enumerate(pinned):
+            ctx.upload(i, p, u)
+        for _ in range(args.steps):
+            ctx.step(1)
+            ctx.stats(0, allow_nonfinite=True)
+        for i in range(len(models)):
+            ctx.download(i)
     with torch.cuda.stream(stream):
         e1.record(stream)
     e1.synchronize()
     e2e_ms = allmax(e0.elapsed_time(e1), world)
     e2e = world * cells * args.steps / (e2e_ms / 1e3)
     state_bytes = (N + K1) * cells * 8
-    stats_bytes = 64 * 8
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r, sample = reference_rate(cases, args.ref_steps, max(1, min(os.cpu_count() or 1, 64)))
+        procs = max(1, min(os.cpu_count() or 1, 64))
+        r, sample = reference_rate(cases, args.ref_steps, procs)
         if r is not None:
-            cpu = {"value": r, "unit": UNIT, "cores": max(1, min(os.cpu_count() or 1, 64)), "kind": "reference",
-                   "sample": sample}
+            cpu = {"value": r, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample}
     ctx.close()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if prec == mb.GP_FP32 else "f64", "data": "synthetic",
-            "config": {"workload": wname, "precision": args.precision, "cells_per_gpu": cells,
-                       "parallelism": f"replicas{world}" if world > 1 else "single",
-                       "l2": "flushed between timed steps (256 MiB write outside the events)"},
+            "config": {"workload": wname, "precision": args.precision if len(models) == 1 else "fp32",
+                       "instances": len(models), "cells_per_gpu": cells, "state_prepared_steps": prep,
+                       "parallelism": f"replicas{world}" if world > 1 else "single", "l2": l2},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
-                         "note": f"algorithmic {alg_bytes} B/cell-update over the whole step; peak {peak_kind}"},
+                         "note": f"algorithmic {alg_bytes} B/cell-update (read+write phi, mu once) per "
+                                 f"launch of the fused step kernel; peak {peak_kind}"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
-                    "d2h_bytes_per_step": state_bytes / args.steps + stats_bytes},
+                    "d2h_bytes_per_step": state_bytes / args.steps + 64 * 8},
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
+        if fp64:
+            line["fp64_plain"] = fp64
+            line["fp32_over_fp64"] = value / fp64["value"]
         print(json.dumps(line))
 
 
@@ -310,7 +369,11 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c4"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--ref-steps", type=int, default=3)
+    ap.add_argument("--prep-steps", type=int, default=-1,
+                    help="steps of the FP32 form run before timing to reach a mid-run state (-1: half the run)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--autotune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -170,6 +170,31 @@ int gp_download_dphi(gp_ctx *ctx, double *dphi);
 void *gp_stream(gp_ctx *ctx);
 /* Number of kernel launches this context issued since creation. */
 int64_t gp_launch_count(const gp_ctx *ctx);
+/* ---------------- batches: many independent instances, FP32 chosen form ---------------- */
+
+/* A batch of n instances (uneven sizes and parameters allowed; they must share
+ * N, K1 and the anisotropy switch).  One kernel launch per time step covers
+ * every tile of every instance; gp_batch_step replays the launches from a
+ * captured CUDA graph.  No counterpart in the reference (one process = one
+ * simulation there). */
+typedef struct gp_batch gp_batch;
+int gp_batch_create(const gp_model *models, int n, gp_batch **out);
+int gp_batch_destroy(gp_batch *b);
+int gp_batch_upload(gp_batch *b, int i, const double *phi, const double *mu);
+int gp_batch_download(gp_batch *b, int i, double *phi, double *mu);
+int gp_batch_step(gp_batch *b, int64_t nsteps);
+int gp_batch_sync(gp_batch *b);
+int gp_batch_get_stats(gp_batch *b, int i, gp_stats *out);
+/* Tile shape of the fused kernel (tx along x, ty along y): 16x32, 8x32, 32x32, 16x64. */
+int gp_batch_set_tile(gp_batch *b, int tx, int ty);
+/* Measured sweep over the tile shapes on the batch's own state (restored
+ * afterwards); the winner is cached in cache_path (may be NULL) per batch
+ * signature and read back on the next call. */
+int gp_batch_autotune(gp_batch *b, const char *cache_path, int *tx, int *ty);
+void *gp_batch_stream(gp_batch *b);
+int64_t gp_batch_launch_count(const gp_batch *b);
+int64_t gp_batch_cells(const gp_batch *b);
+
 /* One plain (FP64) step that allocates nothing.  No counterpart in the
  * reference: it exists for callers that own their device buffers and cannot
  * allocate device memory (a framework pool that owns the whole GPU, a fixed

@@ -100,6 +100,18 @@ _SIGS = {
     "gp_stream": (C.c_void_p, [C.c_void_p]),
     "gp_launch_count": (C.c_int64, [C.c_void_p]),
     "gp_model_sizeof": (C.c_size_t, []),
+    "gp_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "gp_batch_destroy": (C.c_int, [C.c_void_p]),
+    "gp_batch_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "gp_batch_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "gp_batch_step": (C.c_int, [C.c_void_p, C.c_int64]),
+    "gp_batch_sync": (C.c_int, [C.c_void_p]),
+    "gp_batch_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(GpStats)]),
+    "gp_batch_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "gp_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "gp_batch_stream": (C.c_void_p, [C.c_void_p]),
+    "gp_batch_launch_count": (C.c_int64, [C.c_void_p]),
+    "gp_batch_cells": (C.c_int64, [C.c_void_p]),
     "gp_last_error": (C.c_char_p, []),
 }
 
@@ -255,3 +267,94 @@ class Context:
     @property
     def launches(self) -> int:
         return lib().gp_launch_count(self._h)
+
+
+def _stats_dict(st: GpStats, N: int, K1: int) -> dict:
+    out = {n: np.array(getattr(st, n)[: (N if ("phi" in n or "phase" in n) else K1)])
+           for n, _ in GpStats._fields_ if n != "nonfinite"}
+    out["nonfinite"] = st.nonfinite
+    return out
+
+
+class Batch:
+    """Many independent instances stepped together (FP32 chosen form)."""
+
+    def __init__(self, models):
+        self.models = [m.copy() for m in models]
+        arr = (GpModel * len(models))(*self.models)
+        h = C.c_void_p()
+        _check("gp_batch_create", lib().gp_batch_create(C.cast(arr, C.c_void_p), len(models), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gp_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return len(self.models)
+
+    def upload(self, i: int, phi: np.ndarray, mu: np.ndarray):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)  # held: the C call reads them
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        _check("gp_batch_upload", lib().gp_batch_upload(self._h, i, _ptr(phi), _ptr(mu)))
+
+    def download(self, i: int):
+        m = self.models[i]
+        phi = np.empty((m.N, m.mesh_x, m.mesh_y))
+        mu = np.empty((m.K1, m.mesh_x, m.mesh_y))
+        _check("gp_batch_download", lib().gp_batch_download(self._h, i, _ptr(phi), _ptr(mu)))
+        return phi, mu
+
+    def step(self, nsteps: int = 1):
+        _check("gp_batch_step", lib().gp_batch_step(self._h, int(nsteps)))
+
+    def sync(self):
+        _check("gp_batch_sync", lib().gp_batch_sync(self._h))
+
+    def stats(self, i: int, allow_nonfinite: bool = False) -> dict:
+        st = GpStats()
+        rc = lib().gp_batch_get_stats(self._h, i, C.byref(st))
+        if rc != GP_OK and not (allow_nonfinite and rc == GP_E_NONFINITE):
+            raise GpError("gp_batch_get_stats", rc)
+        return _stats_dict(st, self.models[i].N, self.models[i].K1)
+
+    def set_tile(self, tx: int, ty: int):
+        _check("gp_batch_set_tile", lib().gp_batch_set_tile(self._h, tx, ty))
+
+    def autotune(self, cache_path: str | None = None):
+        tx, ty = C.c_int(), C.c_int()
+        _check("gp_batch_autotune", lib().gp_batch_autotune(self._h, cache_path.encode() if cache_path else None,
+                                                            C.byref(tx), C.byref(ty)))
+        return tx.value, ty.value
+
+    @property
+    def stream(self) -> int:
+        return lib().gp_batch_stream(self._h) or 0
+
+    @property
+    def launches(self) -> int:
+        return lib().gp_batch_launch_count(self._h)
+
+    @property
+    def cells(self) -> int:
+        return lib().gp_batch_cells(self._h)
+
+
+def load_case(case):
+    """Input files of a configs.Case -> (model, phi, mu) through the C parser."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        ip, fp = case.write(d)
+        inp = Input(ip, fp)
+        m = inp.model()
+        phi, mu = inp.fill(m)
+    return m, phi, mu

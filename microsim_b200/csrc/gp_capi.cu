@@ -19,9 +19,17 @@ extern "C" void gp_set_error(const char* fmt, ...);
 
 cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch, int64_t rplane, const double* phi,
                         const double* mu, double* dphi, double* phi_out, double* mu_out, cudaStream_t s);
-cudaError_t gp_f32_step(const gp_model& m, int pitch, int64_t plane, const float* phi, const float* mu,
-                        float* phi_out, float* mu_out, cudaStream_t s, int* launches);
+struct gp_f32_batch;
 int gp_f32_supported(const gp_model& m);
+cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** out);
+void gp_f32_batch_destroy(gp_f32_batch* b);
+void gp_f32_batch_bind(gp_f32_batch* b, int i, float* phiA, float* muA, float* phiB, float* muB, int pitch,
+                       int64_t plane);
+cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty);
+int gp_f32_batch_tiles(const gp_f32_batch* b);
+cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s);
+int gp_f32_tile_shape_count();
+void gp_f32_tile_shape(int i, int* tx, int* ty);
 
 #define GP_CUDA(call)                                                                      \
   do {                                                                                     \
@@ -45,6 +53,7 @@ struct gp_ctx {
   void* phi[2];
   void* mu[2];
   double* dphi;    // FP64 form: Delta-phi of the last phase-field half step
+  gp_f32_batch* f32;  // FP32 form: a batch of one instance over phi/mu
   int cur;         // which buffer holds the current state
   int have_prev;   // buffer 1-cur holds the previous step's state
   double* partials;  // statistics: per-block partial results
@@ -126,6 +135,14 @@ extern "C" int gp_create(const gp_model* m, int precision, gp_ctx** out) {
   }
   if (ok) ok = cudaMalloc(&c->partials, (size_t)c->red_blocks * 64 * sizeof(double)) == cudaSuccess &&
                cudaMalloc(&c->reduced, 64 * sizeof(double)) == cudaSuccess;
+  if (ok && precision == GP_FP32) {
+    ok = gp_f32_batch_create(m, 1, &c->f32) == cudaSuccess;
+    if (ok) {
+      gp_f32_batch_bind(c->f32, 0, (float*)c->phi[0], (float*)c->mu[0], (float*)c->phi[1], (float*)c->mu[1], c->pitch,
+                        c->plane);
+      ok = gp_f32_batch_set_tiles(c->f32, 16, 32) == cudaSuccess;
+    }
+  }
   if (!ok) {
     gp_set_error("device allocation failed: %s", cudaGetErrorString(cudaGetLastError()));
     gp_destroy(c);
@@ -143,6 +160,7 @@ extern "C" int gp_destroy(gp_ctx* c) {
     if (c->mu[i]) cudaFree(c->mu[i]);
   }
   if (c->dphi) cudaFree(c->dphi);
+  if (c->f32) gp_f32_batch_destroy(c->f32);
   if (c->partials) cudaFree(c->partials);
   if (c->reduced) cudaFree(c->reduced);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -244,10 +262,8 @@ extern "C" int gp_step(gp_ctx* c, int64_t nsteps) {
                           c->stream));
       c->launches += 2;
     } else {
-      int nl = 0;
-      GP_CUDA(gp_f32_step(c->m, c->pitch, c->plane, (const float*)c->phi[c->cur], (const float*)c->mu[c->cur],
-                          (float*)c->phi[nxt], (float*)c->mu[nxt], c->stream, &nl));
-      c->launches += nl;
+      GP_CUDA(gp_f32_batch_launch(c->f32, c->cur, c->stream));
+      c->launches += 1;
     }
     c->cur = nxt;
     c->have_prev = 1;
@@ -418,4 +434,323 @@ extern "C" int gp_get_stats(gp_ctx* c, gp_stats* out) {
   }
   out->nonfinite = (int64_t)v[L.nonfinite()];
   return out->nonfinite ? GP_E_NONFINITE : GP_OK;
+}
+
+// ------------------------------------------------------------------ batches (FP32 chosen form)
+
+#include <string>
+#include <vector>
+
+struct gp_batch {
+  int n = 0;
+  int device = 0;
+  std::vector<gp_model> models;
+  std::vector<int> pitch;
+  std::vector<int64_t> plane;
+  std::vector<size_t> off_phi[2], off_mu[2];  // float offsets into the pool, per buffer
+  float* pool = nullptr;
+  size_t pool_floats = 0;
+  gp_f32_batch* f32 = nullptr;
+  cudaStream_t stream = nullptr;
+  int parity = 0;     // which buffer holds the current state
+  int have_prev = 0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_steps = 16;
+  double* partials = nullptr;
+  double* reduced = nullptr;
+  int red_blocks = 296;
+  int64_t launches = 0;
+  int tx = 16, ty = 32;
+};
+
+static void batch_drop_graphs(gp_batch* b) {
+  for (int p = 0; p < 2; p++)
+    if (b->graph[p]) {
+      cudaGraphExecDestroy(b->graph[p]);
+      b->graph[p] = nullptr;
+    }
+}
+
+extern "C" int gp_batch_destroy(gp_batch* b) {
+  if (!b) return GP_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop_graphs(b);
+  if (b->f32) gp_f32_batch_destroy(b->f32);
+  if (b->pool) cudaFree(b->pool);
+  if (b->partials) cudaFree(b->partials);
+  if (b->reduced) cudaFree(b->reduced);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return GP_OK;
+}
+
+extern "C" int gp_batch_create(const gp_model* models, int n, gp_batch** out) {
+  if (!models || n < 1 || !out) return GP_E_ARG;
+  for (int i = 0; i < n; i++) {
+    int rc = check_model(&models[i]);
+    if (rc != GP_OK) return rc;
+    if (models[i].N != models[0].N || models[i].K1 != models[0].K1 || models[i].anisotropy != models[0].anisotropy) {
+      gp_set_error("gp_batch_create: instances of one batch must share N, K1 and the anisotropy switch");
+      return GP_E_ARG;
+    }
+  }
+  if (!gp_f32_supported(models[0])) {
+    gp_set_error("FP32 form not available for N=%d, K1=%d", models[0].N, models[0].K1);
+    return GP_E_UNSUPPORTED;
+  }
+  gp_batch* b = new (std::nothrow) gp_batch();
+  if (!b) return GP_E_NOMEM;
+  b->n = n;
+  b->models.assign(models, models + n);
+  GP_CUDA(cudaGetDevice(&b->device));
+  const int N = models[0].N, K1 = models[0].K1;
+  size_t off = 0;
+  for (int i = 0; i < n; i++) {
+    const int pitch = (int)gp_round_up(models[i].mesh_y, 32);
+    const int64_t plane = models[i].mesh_x * (int64_t)pitch;
+    b->pitch.push_back(pitch);
+    b->plane.push_back(plane);
+    for (int p = 0; p < 2; p++) {
+      b->off_phi[p].push_back(off);
+      off += (size_t)gp_round_up(N * plane, 64);
+      b->off_mu[p].push_back(off);
+      off += (size_t)gp_round_up(K1 * plane, 64);
+    }
+  }
+  b->pool_floats = off;
+  bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaMalloc(&b->pool, off * sizeof(float)) == cudaSuccess &&
+            cudaMemset(b->pool, 0, off * sizeof(float)) == cudaSuccess &&
+            cudaMalloc(&b->partials, (size_t)b->red_blocks * 64 * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&b->reduced, 64 * sizeof(double)) == cudaSuccess &&
+            gp_f32_batch_create(models, n, &b->f32) == cudaSuccess;
+  if (ok) {
+    for (int i = 0; i < n; i++)
+      gp_f32_batch_bind(b->f32, i, b->pool + b->off_phi[0][i], b->pool + b->off_mu[0][i], b->pool + b->off_phi[1][i],
+                        b->pool + b->off_mu[1][i], b->pitch[i], b->plane[i]);
+    ok = gp_f32_batch_set_tiles(b->f32, b->tx, b->ty) == cudaSuccess;
+  }
+  if (!ok) {
+    gp_set_error("gp_batch_create: allocation failed: %s", cudaGetErrorString(cudaGetLastError()));
+    gp_batch_destroy(b);
+    return GP_E_NOMEM;
+  }
+  *out = b;
+  return GP_OK;
+}
+
+static int batch_copy(gp_batch* b, int i, const double* host, int nplanes, bool is_phi, bool up) {
+  const gp_model& m = b->models[i];
+  const int64_t mx = m.mesh_x, my = m.mesh_y;
+  float* dev = b->pool + (is_phi ? b->off_phi[b->parity][i] : b->off_mu[b->parity][i]);
+  double* stage = nullptr;
+  const size_t bytes = (size_t)nplanes * mx * my * sizeof(double);
+  GP_CUDA(cudaMallocAsync((void**)&stage, bytes, b->stream));
+  if (up) {
+    GP_CUDA(cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, b->stream));
+    k_pack<float><<<592, 256, 0, b->stream>>>(stage, dev, (int)mx, (int)my, b->pitch[i], b->plane[i], nplanes);
+  } else {
+    k_unpack<float><<<592, 256, 0, b->stream>>>(dev, stage, (int)mx, (int)my, b->pitch[i], b->plane[i], nplanes);
+    GP_CUDA(cudaMemcpyAsync((void*)host, stage, bytes, cudaMemcpyDeviceToHost, b->stream));
+  }
+  b->launches++;
+  GP_CUDA(cudaGetLastError());
+  GP_CUDA(cudaFreeAsync(stage, b->stream));
+  return GP_OK;
+}
+
+extern "C" int gp_batch_upload(gp_batch* b, int i, const double* phi, const double* mu) {
+  if (!b || i < 0 || i >= b->n || !phi || !mu) return GP_E_ARG;
+  int rc = batch_copy(b, i, phi, b->models[i].N, true, true);
+  if (rc == GP_OK) rc = batch_copy(b, i, mu, b->models[i].K1, false, true);
+  if (rc == GP_OK) GP_CUDA(cudaStreamSynchronize(b->stream));
+  b->have_prev = 0;
+  return rc;
+}
+
+extern "C" int gp_batch_download(gp_batch* b, int i, double* phi, double* mu) {
+  if (!b || i < 0 || i >= b->n || !phi || !mu) return GP_E_ARG;
+  int rc = batch_copy(b, i, phi, b->models[i].N, true, false);
+  if (rc == GP_OK) rc = batch_copy(b, i, mu, b->models[i].K1, false, false);
+  if (rc == GP_OK) GP_CUDA(cudaStreamSynchronize(b->stream));
+  return rc;
+}
+
+// Capture graph_steps launches starting at `parity` (an even count: the graph
+// ends on the parity it starts from).
+static int batch_capture(gp_batch* b, int parity) {
+  cudaGraph_t g = nullptr;
+  GP_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  for (int s = 0; s < b->graph_steps && e == cudaSuccess; s++) e = gp_f32_batch_launch(b->f32, parity ^ (s & 1), b->stream);
+  cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    gp_set_error("graph capture failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    return GP_E_CUDA;
+  }
+  e = cudaGraphInstantiate(&b->graph[parity], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    gp_set_error("graph instantiate failed: %s", cudaGetErrorString(e));
+    return GP_E_CUDA;
+  }
+  return GP_OK;
+}
+
+extern "C" int gp_batch_step(gp_batch* b, int64_t nsteps) {
+  if (!b || nsteps < 0) return GP_E_ARG;
+  while (nsteps >= b->graph_steps) {
+    if (!b->graph[b->parity]) {
+      int rc = batch_capture(b, b->parity);
+      if (rc != GP_OK) return rc;
+    }
+    GP_CUDA(cudaGraphLaunch(b->graph[b->parity], b->stream));
+    b->launches += b->graph_steps;
+    nsteps -= b->graph_steps;
+    b->have_prev = 1;
+  }
+  for (; nsteps > 0; nsteps--) {
+    GP_CUDA(gp_f32_batch_launch(b->f32, b->parity, b->stream));
+    b->launches++;
+    b->parity ^= 1;
+    b->have_prev = 1;
+  }
+  return GP_OK;
+}
+
+extern "C" int gp_batch_sync(gp_batch* b) {
+  if (!b) return GP_E_ARG;
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  return GP_OK;
+}
+
+extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
+  if (!b || i < 0 || i >= b->n || !out) return GP_E_ARG;
+  const gp_model& m = b->models[i];
+  const int cur = b->parity, prv = 1 - b->parity;
+  k_stats<float><<<b->red_blocks, 256, 0, b->stream>>>(
+      m, b->pool + b->off_phi[cur][i], b->pool + b->off_mu[cur][i], b->pool + b->off_phi[prv][i],
+      b->pool + b->off_mu[prv][i], b->have_prev, b->pitch[i], b->plane[i], b->partials);
+  GP_CUDA(cudaGetLastError());
+  k_stats_final<<<1, 64, 0, b->stream>>>(m.N, m.K1, b->partials, b->red_blocks, b->reduced);
+  GP_CUDA(cudaGetLastError());
+  b->launches += 2;
+  double v[64];
+  GP_CUDA(cudaMemcpyAsync(v, b->reduced, sizeof v, cudaMemcpyDeviceToHost, b->stream));
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  const StatLayout L{m.N, m.K1};
+  memset(out, 0, sizeof *out);
+  for (int a = 0; a < m.N; a++) {
+    out->phi_max[a] = v[L.phi_max(a)];
+    out->phi_min[a] = v[L.phi_min(a)];
+    out->rel_change_phi[a] = v[L.rel_phi(a)];
+    out->phase_fraction[a] = v[L.phase(a)];
+  }
+  for (int k = 0; k < m.K1; k++) {
+    out->mu_max[k] = v[L.mu_max(k)];
+    out->mu_min[k] = v[L.mu_min(k)];
+    out->rel_change_mu[k] = v[L.rel_mu(k)];
+    out->solute[k] = v[L.solute(k)];
+  }
+  out->nonfinite = (int64_t)v[L.nonfinite()];
+  return out->nonfinite ? GP_E_NONFINITE : GP_OK;
+}
+
+extern "C" int gp_batch_set_tile(gp_batch* b, int tx, int ty) {
+  if (!b) return GP_E_ARG;
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  if (gp_f32_batch_set_tiles(b->f32, tx, ty) != cudaSuccess) {
+    gp_set_error("tile shape %dx%d not available", tx, ty);
+    return GP_E_ARG;
+  }
+  batch_drop_graphs(b);
+  b->tx = tx;
+  b->ty = ty;
+  return GP_OK;
+}
+
+// Measured sweep over the tile shapes; the winner is cached in a small text
+// file (one line per batch signature: "N K1 aniso cells ninst tx ty ms").
+extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_out, int* ty_out) {
+  if (!b) return GP_E_ARG;
+  int64_t cells = 0;
+  for (const gp_model& m : b->models) cells += m.mesh_x * m.mesh_y;
+  const gp_model& m0 = b->models[0];
+  char key[128];
+  snprintf(key, sizeof key, "%d %d %d %lld %d", m0.N, m0.K1, m0.anisotropy, (long long)cells, b->n);
+  if (cache_path) {
+    FILE* f = fopen(cache_path, "r");
+    if (f) {
+      char line[256];
+      while (fgets(line, sizeof line, f)) {
+        int N, K1, an, n, tx, ty;
+        long long c;
+        double ms;
+        if (sscanf(line, "%d %d %d %lld %d %d %d %lf", &N, &K1, &an, &c, &n, &tx, &ty, &ms) == 8 && N == m0.N &&
+            K1 == m0.K1 && an == m0.anisotropy && c == cells && n == b->n) {
+          fclose(f);
+          if (tx_out) *tx_out = tx;
+          if (ty_out) *ty_out = ty;
+          return gp_batch_set_tile(b, tx, ty);
+        }
+      }
+      fclose(f);
+    }
+  }
+  // keep the state: time on a copy of the current buffers, restore afterwards
+  float* backup = nullptr;
+  GP_CUDA(cudaMallocAsync((void**)&backup, b->pool_floats * sizeof(float), b->stream));
+  GP_CUDA(cudaMemcpyAsync(backup, b->pool, b->pool_floats * sizeof(float), cudaMemcpyDeviceToDevice, b->stream));
+  const int saved_parity = b->parity, saved_prev = b->have_prev;
+  cudaEvent_t e0, e1;
+  GP_CUDA(cudaEventCreate(&e0));
+  GP_CUDA(cudaEventCreate(&e1));
+  int best_tx = b->tx, best_ty = b->ty;
+  float best = 1e30f;
+  for (int s = 0; s < gp_f32_tile_shape_count(); s++) {
+    int tx, ty;
+    gp_f32_tile_shape(s, &tx, &ty);
+    if (gp_batch_set_tile(b, tx, ty) != GP_OK) continue;
+    for (int w = 0; w < 3; w++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (w & 1), b->stream));
+    GP_CUDA(cudaEventRecord(e0, b->stream));
+    for (int r = 0; r < 10; r++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (r & 1), b->stream));
+    GP_CUDA(cudaEventRecord(e1, b->stream));
+    GP_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    GP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    b->launches += 13;
+    if (ms < best) {
+      best = ms;
+      best_tx = tx;
+      best_ty = ty;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  GP_CUDA(cudaMemcpyAsync(b->pool, backup, b->pool_floats * sizeof(float), cudaMemcpyDeviceToDevice, b->stream));
+  GP_CUDA(cudaFreeAsync(backup, b->stream));
+  b->parity = saved_parity;
+  b->have_prev = saved_prev;
+  int rc = gp_batch_set_tile(b, best_tx, best_ty);
+  if (rc != GP_OK) return rc;
+  if (cache_path) {
+    FILE* f = fopen(cache_path, "a");
+    if (f) {
+      fprintf(f, "%s %d %d %.6f\n", key, best_tx, best_ty, best / 10.0f);
+      fclose(f);
+    }
+  }
+  if (tx_out) *tx_out = best_tx;
+  if (ty_out) *ty_out = best_ty;
+  return GP_OK;
+}
+
+extern "C" void* gp_batch_stream(gp_batch* b) { return b ? (void*)b->stream : nullptr; }
+extern "C" int64_t gp_batch_launch_count(const gp_batch* b) { return b ? b->launches : 0; }
+extern "C" int64_t gp_batch_cells(const gp_batch* b) {
+  int64_t c = 0;
+  if (b)
+    for (const gp_model& m : b->models) c += m.mesh_x * m.mesh_y;
+  return c;
 }

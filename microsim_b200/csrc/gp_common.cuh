@@ -20,6 +20,14 @@ __host__ __device__ __forceinline__ int gp_map(int v, int M, int type) {
   return v;
 }
 
+// gp_map for coordinates that may lie anywhere beyond the grid (halo cells of
+// partial edge tiles, whose values no interior cell uses): clamped into
+// [-3, M+2] first so every load stays inside the interior.
+__host__ __device__ __forceinline__ int gp_map_any(int v, int M, int type) {
+  v = v < -3 ? -3 : (v > M + 2 ? M + 2 : v);
+  return gp_map(v, M, type);
+}
+
 // Per-field, per-axis copy types.  The reference forces both sides of an axis
 // to periodic when either is, and the kernels accept only types 1 and 3, so one
 // type per (field, axis) describes the copy.

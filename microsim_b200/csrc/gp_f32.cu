@@ -1,14 +1,899 @@
-// gp_f32.cu -- placeholder until the FP32 chosen form lands.
+// gp_f32.cu -- the chosen form of the step: FP32 storage and update, one
+// fused kernel per time step for a whole batch of independent instances.
+//
+// Same model as the plain form (gp_f64.cu, reference
+// Grand_potential_Finite_difference_2D_serial/solverloop/*), restructured for
+// the GPU instead of kept in the reference's evaluation order:
+//  * one launch per step covers every tile of every instance of a batch
+//    (instances may differ in size and parameters; they share N, K1 and the
+//    anisotropy switch, which are template parameters);
+//  * a block stages phi for its tile plus a 2-cell halo and mu plus a 1-cell
+//    halo in shared memory; ghost cells come from the boundary index map;
+//  * anisotropic gradient-energy terms are evaluated once per face and per
+//    phase pair and shared by the two cells of the face and by both phases of
+//    the pair (q_ba = -q_ab, a_c even, da_c/dq odd in q);
+//  * Delta-phi of the tile plus one ring stays in shared memory; the mu update
+//    then uses face fluxes (diffusion + antitrapping) computed once per face;
+//  * reciprocals of dx, dy, 2dy are folded; the (dc/dmu)^-1 solve of
+//    multicomponent cases and all statistics stay FP64.
+// The reference's j_at,y skip on row gidy == MESH_Y-2
+// (calculate_fluxes_concentration.h:65) is kept: it is part of the model the
+// reference integrates.
+
+#include <stdio.h>
+#include <string.h>
+
+#include <vector>
+
 #include "gp_common.cuh"
 
-int gp_f32_supported(const gp_model& m) {
-  (void)m;
-  return 0;
+extern "C" void gp_set_error(const char* fmt, ...);
+
+namespace gp32 {
+
+constexpr int MP = GP_MAX_PHASES;
+constexpr int MK = GP_MAX_K1;
+
+// FP32 model constants of one instance (built on the host from gp_model).
+struct Model {
+  float dx_inv, dy_inv, half_dy_inv, dt, eps, inv_eps, tau, w_obst, jscale, s_well;
+  int obstacle, mu_solver, skip_row, pad;
+  float Gamma[MP][MP];
+  float Gabc[MP][MP][MP];
+  float tau_ab[MP][MP];
+  float dab[MP][MP];
+  float R[MP][MP][2][2];
+  float Rinv[MP][MP][2][2];
+  float cmu[MP][MK][MK];
+  float A[MP][MK][MK];
+  float Beff[MP][MK];
+  float B[MP][MK];
+  float C[MP];
+  float DC[MP][MK][MK];  // sum_k Diff[b][i][k] * cmu[b][k][j]: D(phi) = sum_b DC_b phi_b
+  float atf[MP][MK];     // 1 - Diff[a][k][k] / Diff[N-1][k][k]
+  double cmu_d[MP][MK][MK];
+};
+
+// One instance of a batch: its buffers and geometry.
+struct Inst {
+  const float* phi;
+  const float* mu;
+  float* phi_out;
+  float* mu_out;
+  int64_t plane;
+  int mx, my, pitch;
+  int tiles_y;     // tiles along y
+  int tile_begin;  // first global tile index of this instance
+  int model;       // index into the model array
+  gp_bc bc;
+};
+
+template <int N>
+struct Pairs {
+  static constexpr int P = N * (N - 1) / 2;
+  static __host__ __device__ constexpr int index(int a, int b) {  // a < b
+    return a * N - a * (a + 1) / 2 + (b - a - 1);
+  }
+};
+
+// ---------------------------------------------------------------- device helpers
+
+template <int N>
+__device__ __forceinline__ float hphi(const float* p, int a) {
+  float s1 = 0.f;
+#pragma unroll
+  for (int b = 0; b < N; b++)
+#pragma unroll
+    for (int c = b + 1; c < N; c++)
+      if (b != a && c != a) s1 += p[b] * p[c];
+  return p[a] * p[a] * (3.f - 2.f * p[a]) + 2.f * p[a] * s1;
 }
 
-cudaError_t gp_f32_step(const gp_model& m, int pitch, int64_t plane, const float* phi, const float* mu,
-                        float* phi_out, float* mu_out, cudaStream_t s, int* launches) {
-  (void)m; (void)pitch; (void)plane; (void)phi; (void)mu; (void)phi_out; (void)mu_out; (void)s;
-  *launches = 0;
-  return cudaErrorNotSupported;
+// dh_b / dphi_a
+template <int N>
+__device__ __forceinline__ float dhphi(const float* p, int b, int a) {
+  float s = 0.f;
+  if (a == b) {
+#pragma unroll
+    for (int e = 0; e < N; e++)
+#pragma unroll
+      for (int f = e + 1; f < N; f++)
+        if (e != b && f != b) s += p[e] * p[f];
+    return 6.f * p[a] * (1.f - p[a]) + 2.f * s;
+  }
+#pragma unroll
+  for (int e = 0; e < N; e++)
+    if (e != b && e != a) s += p[e];
+  return 2.f * s * p[b];
+}
+
+template <int K1>
+__device__ __forceinline__ float c_mu(const Model& m, const float* mu, int a, int i) {
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < K1; k++) s += m.cmu[a][i][k] * (mu[k] - m.Beff[a][k]);
+  return s;
+}
+
+__device__ __forceinline__ float aniso_ac(float dab, float q0, float q1) {
+  const float q2 = q0 * q0 + q1 * q1;
+  if (q2 > 1.0e-15f) {
+    const float inv = __frcp_rn(q2);
+    const float x2 = q0 * q0 * inv, y2 = q1 * q1 * inv;
+    return 1.f - dab * (3.f - 4.f * (x2 * x2 + y2 * y2));
+  }
+  return 1.f;
+}
+
+// a_c and |q|^2 * d a_c / d q (the combination every caller uses)
+__device__ __forceinline__ void aniso_terms(float dab, float q0, float q1, float& ac, float& q2, float& e0,
+                                            float& e1) {
+  q2 = q0 * q0 + q1 * q1;
+  if (q2 > 1.0e-15f) {
+    const float inv = __frcp_rn(q2);
+    const float x2 = q0 * q0 * inv, y2 = q1 * q1 * inv;
+    const float s4 = x2 * x2 + y2 * y2;  // sum q_i^4 / |q|^4
+    ac = 1.f - dab * (3.f - 4.f * s4);
+    // |q|^2 * 16 dab (q_i^3/|q|^4 - q_i sum q^4/|q|^6) = 16 dab q_i (q_i^2/|q|^2 - s4)
+    e0 = 16.f * dab * q0 * (x2 - s4);
+    e1 = 16.f * dab * q1 * (y2 - s4);
+  } else {
+    ac = 1.f;
+    e0 = e1 = 0.f;
+  }
+}
+
+// ---------------------------------------------------------------- the fused step
+
+template <int N, int K1, bool ANISO, int TX, int TY>
+struct Tile {
+  static constexpr int P = Pairs<N>::P;
+  static constexpr int X2 = TX + 4, Y2 = TY + 4;  // phi region: tile +- 2
+  static constexpr int X1 = TX + 2, Y1 = TY + 2;  // mu / Delta-phi region: tile +- 1
+  // shared-memory layout (floats)
+  static constexpr int o_phi = 0;
+  static constexpr int o_mu = o_phi + N * X2 * Y2;
+  static constexpr int o_dphi = o_mu + K1 * X1 * Y1;
+  static constexpr int o_bx = o_dphi + N * X1 * Y1;                  // x-face brackets [P][TX+3][TY+2]
+  static constexpr int o_by = o_bx + (ANISO ? P : P) * (TX + 3) * (TY + 2);  // y-face brackets [P][TX+2][TY+3]
+  static constexpr int o_fx = o_by + P * (TX + 2) * (TY + 3);        // mu-update x-face fluxes [K1][TX+1][TY]
+  static constexpr int o_fy = o_fx + K1 * (TX + 1) * TY;             // mu-update y-face fluxes [K1][TX][TY+1]
+  static constexpr int total = o_fy + K1 * TX * (TY + 1);
+  static constexpr size_t bytes = total * sizeof(float);
+};
+
+template <int N, int K1, bool ANISO, int TX, int TY>
+__global__ void __launch_bounds__(256) k_step32(const Inst* __restrict__ insts, int ninst,
+                                                const Model* __restrict__ models) {
+  using T = Tile<N, K1, ANISO, TX, TY>;
+  constexpr int P = T::P, X2 = T::X2, Y2 = T::Y2, X1 = T::X1, Y1 = T::Y1;
+  constexpr int L = N - 1;
+  extern __shared__ float sm[];
+  float* sphi = sm + T::o_phi;
+  float* smu = sm + T::o_mu;
+  float* sdp = sm + T::o_dphi;
+  float* sbx = sm + T::o_bx;
+  float* sby = sm + T::o_by;
+  float* sfx = sm + T::o_fx;
+  float* sfy = sm + T::o_fy;
+  __shared__ int s_inst;
+
+  // which instance / tile (binary search on tile_begin)
+  const int tile = blockIdx.x;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (insts[mid].tile_begin <= tile) lo = mid;
+      else hi = mid - 1;
+    }
+    s_inst = lo;
+  }
+  __syncthreads();
+  const Inst& I = insts[s_inst];
+  const Model& m = models[I.model];
+  const int lt = tile - I.tile_begin;
+  const int x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
+  const int mx = I.mx, my = I.my;
+  const int nt = blockDim.x;
+
+  // ---- stage phi (tile +- 2) and mu (tile +- 1)
+  for (int e = threadIdx.x; e < X2 * Y2; e += nt) {
+    const int i = e / Y2, j = e % Y2;
+    const int gx = gp_map_any(x0 - 2 + i, mx, I.bc.phi_x), gy = gp_map_any(y0 - 2 + j, my, I.bc.phi_y);
+    const float* p = I.phi + (int64_t)gx * I.pitch + gy;
+#pragma unroll
+    for (int a = 0; a < N; a++) sphi[a * X2 * Y2 + e] = __ldg(p + a * I.plane);
+  }
+  for (int e = threadIdx.x; e < X1 * Y1; e += nt) {
+    const int i = e / Y1, j = e % Y1;
+    const int gx = gp_map_any(x0 - 1 + i, mx, I.bc.mu_x), gy = gp_map_any(y0 - 1 + j, my, I.bc.mu_y);
+    const float* p = I.mu + (int64_t)gx * I.pitch + gy;
+#pragma unroll
+    for (int k = 0; k < K1; k++) smu[k * X1 * Y1 + e] = __ldg(p + k * I.plane);
+  }
+  __syncthreads();
+
+  auto PH = [&](int a, int i, int j) -> float { return sphi[(a * X2 + i) * Y2 + j]; };
+
+  // ---- pure-tile test: when every staged cell is the same pure phase, Delta-phi
+  // is exactly zero on the ring (divphi = 0) and so is every antitrapping
+  // current (zero gradients), so those stages are skipped; the flux and update
+  // code below is shared, which keeps the results bit-identical to the full path.
+  int b0 = -1;
+#pragma unroll
+  for (int a = N - 1; a >= 0; a--)
+    if (sphi[a * X2 * Y2] == 1.f) b0 = a;
+  bool ok = b0 >= 0;
+  for (int e = threadIdx.x; ok && e < X2 * Y2; e += nt) {
+#pragma unroll
+    for (int a = 0; a < N; a++) ok &= (sphi[a * X2 * Y2 + e] == (a == b0 ? 1.f : 0.f));
+  }
+  const bool pure = __syncthreads_and(ok) != 0;
+  if (pure) {
+    for (int e = threadIdx.x; e < N * X1 * Y1; e += nt) sdp[e] = 0.f;
+  } else {
+  // ---- gradient-energy brackets per face and phase pair
+  // x-face between region-2 rows i and i+1 (i in [0, TX+2]), at region-2 columns j in [1, TY+2]
+  //   Bk = a_c^2 Qx + a_c |q|^2 (Rinv dadq)_x   (anisotropic),  Bk = Qx (isotropic)
+  //   with Qx = sx_a gx_b - sx_b gx_a, and the flux of phase a (pair b) through the
+  //   face  F_ab = -Bk sx_b,  F_ba = +Bk sx_a  (function_A_0x divdAdgradphi).
+  for (int e = threadIdx.x; e < (TX + 3) * (TY + 2); e += nt) {
+    const int i = e / (TY + 2), j = 1 + e % (TY + 2);
+    float sx[N], gxv[N], cy0[N], cy1[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      const float pc = PH(a, i, j), pf = PH(a, i + 1, j);
+      sx[a] = 0.5f * (pc + pf);
+      gxv[a] = (pf - pc) * m.dx_inv;
+      cy0[a] = (PH(a, i, j + 1) - PH(a, i, j - 1)) * m.half_dy_inv;
+      cy1[a] = (PH(a, i + 1, j + 1) - PH(a, i + 1, j - 1)) * m.half_dy_inv;
+    }
+#pragma unroll
+    for (int a = 0; a < N; a++)
+#pragma unroll
+      for (int b = a + 1; b < N; b++) {
+        const int p = Pairs<N>::index(a, b);
+        const float Qx = sx[a] * gxv[b] - sx[b] * gxv[a];
+        float bk = Qx;
+        if (ANISO) {
+          const float Qy = 0.5f * (sx[a] * (cy0[b] + cy1[b]) - sx[b] * (cy0[a] + cy1[a]));
+          const float q0 = m.R[a][b][0][0] * Qx + m.R[a][b][0][1] * Qy;
+          const float q1 = m.R[a][b][1][0] * Qx + m.R[a][b][1][1] * Qy;
+          float ac, q2, e0, e1;
+          aniso_terms(m.dab[a][b], q0, q1, ac, q2, e0, e1);
+          bk = ac * ac * Qx + ac * (m.Rinv[a][b][0][0] * e0 + m.Rinv[a][b][0][1] * e1);
+        }
+        sbx[(p * (TX + 3) + i) * (TY + 2) + (j - 1)] = bk;
+      }
+  }
+  // y-face between region-2 columns j and j+1 (j in [0, TY+2]), at rows i in [1, TX+2]
+  for (int e = threadIdx.x; e < (TX + 2) * (TY + 3); e += nt) {
+    const int i = 1 + e / (TY + 3), j = e % (TY + 3);
+    float sy[N], gyv[N], cx0[N], cx1[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      const float pc = PH(a, i, j), pr = PH(a, i, j + 1);
+      sy[a] = 0.5f * (pc + pr);
+      gyv[a] = (pr - pc) * m.dy_inv;
+      cx0[a] = 0.5f * (PH(a, i + 1, j) - PH(a, i - 1, j)) * m.dx_inv;
+      cx1[a] = 0.5f * (PH(a, i + 1, j + 1) - PH(a, i - 1, j + 1)) * m.dx_inv;
+    }
+#pragma unroll
+    for (int a = 0; a < N; a++)
+#pragma unroll
+      for (int b = a + 1; b < N; b++) {
+        const int p = Pairs<N>::index(a, b);
+        const float Qy = sy[a] * gyv[b] - sy[b] * gyv[a];
+        float bk = Qy;
+        if (ANISO) {
+          const float Qx = 0.5f * (sy[a] * (cx0[b] + cx1[b]) - sy[b] * (cx0[a] + cx1[a]));
+          const float q0 = m.R[a][b][0][0] * Qx + m.R[a][b][0][1] * Qy;
+          const float q1 = m.R[a][b][1][0] * Qx + m.R[a][b][1][1] * Qy;
+          float ac, q2, e0, e1;
+          aniso_terms(m.dab[a][b], q0, q1, ac, q2, e0, e1);
+          bk = ac * ac * Qy + ac * (m.Rinv[a][b][1][0] * e0 + m.Rinv[a][b][1][1] * e1);
+        }
+        sby[(p * (TX + 2) + (i - 1)) * (TY + 3) + j] = bk;
+      }
+  }
+  __syncthreads();
+
+  // ---- Delta-phi on the tile plus one ring (calculate_divergence_phasefield.h:4-62)
+  for (int e = threadIdx.x; e < X1 * Y1; e += nt) {
+    const int i1 = e / Y1, j1 = e % Y1;  // region-1 coordinates
+    const int i = i1 + 1, j = j1 + 1;    // region-2 coordinates
+    float ph[N], gf[N], gb[N], gr[N], gl[N], divphi[N];
+    bool any = false;
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      ph[a] = PH(a, i, j);
+      gf[a] = (PH(a, i + 1, j) - ph[a]) * m.dx_inv;
+      gb[a] = (ph[a] - PH(a, i - 1, j)) * m.dx_inv;
+      gr[a] = (PH(a, i, j + 1) - ph[a]) * m.dy_inv;
+      gl[a] = (ph[a] - PH(a, i, j - 1)) * m.dy_inv;
+      divphi[a] = (gf[a] - gb[a]) * m.dx_inv + (gr[a] - gl[a]) * m.dy_inv;
+      any |= (divphi[a] != 0.f);
+    }
+    float dp[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) dp[a] = 0.f;
+    if (any) {
+      float cx[N], cy[N];
+#pragma unroll
+      for (int a = 0; a < N; a++) {
+        cx[a] = 0.5f * (gf[a] + gb[a]);
+        cy[a] = (PH(a, i, j + 1) - PH(a, i, j - 1)) * m.half_dy_inv;
+      }
+      // -dA/dphi_a + div dA/dgrad phi_a, accumulated per phase over pairs
+      float gterm[N];
+#pragma unroll
+      for (int a = 0; a < N; a++) gterm[a] = 0.f;
+#pragma unroll
+      for (int a = 0; a < N; a++)
+#pragma unroll
+        for (int b = a + 1; b < N; b++) {
+          const int p = Pairs<N>::index(a, b);
+          const float g2 = 2.f * m.Gamma[a][b];
+          // divergence part from the four faces around (i, j)
+          const float bxf = sbx[(p * (TX + 3) + i) * (TY + 2) + (j - 1)];
+          const float bxb = sbx[(p * (TX + 3) + i - 1) * (TY + 2) + (j - 1)];
+          const float byr = sby[(p * (TX + 2) + (i - 1)) * (TY + 3) + j];
+          const float byl = sby[(p * (TX + 2) + (i - 1)) * (TY + 3) + j - 1];
+          const float sxa_f = 0.5f * (ph[a] + PH(a, i + 1, j)), sxb_f = 0.5f * (ph[b] + PH(b, i + 1, j));
+          const float sxa_b = 0.5f * (ph[a] + PH(a, i - 1, j)), sxb_b = 0.5f * (ph[b] + PH(b, i - 1, j));
+          const float sya_r = 0.5f * (ph[a] + PH(a, i, j + 1)), syb_r = 0.5f * (ph[b] + PH(b, i, j + 1));
+          const float sya_l = 0.5f * (ph[a] + PH(a, i, j - 1)), syb_l = 0.5f * (ph[b] + PH(b, i, j - 1));
+          const float div_ab = (-bxf * sxb_f + bxb * sxb_b) * m.dx_inv + (-byr * syb_r + byl * syb_l) * m.dy_inv;
+          const float div_ba = (bxf * sxa_f - bxb * sxa_b) * m.dx_inv + (byr * sya_r - byl * sya_l) * m.dy_inv;
+          // dA/dphi part at the centre
+          const float Qx = ph[a] * cx[b] - ph[b] * cx[a];
+          const float Qy = ph[a] * cy[b] - ph[b] * cy[a];
+          float dA_a, dA_b;
+          if (ANISO) {
+            const float q0 = m.R[a][b][0][0] * Qx + m.R[a][b][0][1] * Qy;
+            const float q1 = m.R[a][b][1][0] * Qx + m.R[a][b][1][1] * Qy;
+            float ac, q2, e0, e1;
+            aniso_terms(m.dab[a][b], q0, q1, ac, q2, e0, e1);
+            const float rb0 = m.R[a][b][0][0] * cx[b] + m.R[a][b][0][1] * cy[b];
+            const float rb1 = m.R[a][b][1][0] * cx[b] + m.R[a][b][1][1] * cy[b];
+            const float ra0 = m.R[a][b][0][0] * cx[a] + m.R[a][b][0][1] * cy[a];
+            const float ra1 = m.R[a][b][1][0] * cx[a] + m.R[a][b][1][1] * cy[a];
+            const float ac2 = ac * ac;
+            dA_a = ac2 * (q0 * rb0 + q1 * rb1) + ac * (e0 * rb0 + e1 * rb1);
+            dA_b = -(ac2 * (q0 * ra0 + q1 * ra1) + ac * (e0 * ra0 + e1 * ra1));
+          } else {
+            dA_a = Qx * cx[b] + Qy * cy[b];
+            dA_b = -(Qx * cx[a] + Qy * cy[a]);
+          }
+          gterm[a] += g2 * (div_ab - dA_a);
+          gterm[b] += g2 * (div_ba - dA_b);
+        }
+      // grand potentials of the phases at this cell's mu
+      float mu[K1];
+#pragma unroll
+      for (int k = 0; k < K1; k++) mu[k] = smu[(k * X1 + i1) * Y1 + j1];
+      float psi[N];
+#pragma unroll
+      for (int b = 0; b < N; b++) {
+        float c[K1], s = 0.f;
+#pragma unroll
+        for (int k = 0; k < K1; k++) c[k] = c_mu<K1>(m, mu, b, k);
+#pragma unroll
+        for (int k = 0; k < K1; k++) {
+#pragma unroll
+          for (int l = k; l < K1; l++) s += m.A[b][k][l] * c[k] * c[l];
+          s += (m.B[b][k] - mu[k]) * c[k];
+        }
+        psi[b] = s + m.C[b];
+      }
+      float lambda[N], sum_l = 0.f;
+      int active = 0;
+#pragma unroll
+      for (int a = 0; a < N; a++) {
+        lambda[a] = 0.f;
+        if (divphi[a] != 0.f) {
+          // obstacle / well potential (functionW_01.h, functionW_02.h)
+          float w = 0.f;
+#pragma unroll
+          for (int b = 0; b < N; b++) {
+            if (b == a || divphi[b] == 0.f) continue;
+            if (m.obstacle) w += (ph[a] * ph[b] >= 0.f ? m.Gamma[a][b] : -m.Gamma[a][b]) * ph[b];
+            else w += 2.f * m.Gamma[a][b] * ph[b] * ph[b] * ph[a];
+          }
+          w *= m.obstacle ? m.w_obst : 9.f;
+#pragma unroll
+          for (int b = 0; b < N; b++)
+#pragma unroll
+            for (int c = b + 1; c < N; c++) {
+              if (b == a || c == a || divphi[b] == 0.f || divphi[c] == 0.f) continue;
+              const float pbc = ph[b] * ph[c];
+              w += (ph[a] * pbc >= 0.f ? m.Gabc[a][b][c] : -m.Gabc[a][b][c]) * pbc;
+            }
+          float dpsi = 0.f;
+#pragma unroll
+          for (int b = 0; b < N; b++) dpsi += psi[b] * dhphi<N>(ph, b, a);
+          lambda[a] = m.eps * gterm[a] - m.inv_eps * w - dpsi;
+          sum_l += lambda[a];
+          active++;
+        }
+      }
+      sum_l /= (float)active;
+      float st = 0.f, st1 = 0.f;
+#pragma unroll
+      for (int a = 0; a < N; a++)
+#pragma unroll
+        for (int b = a + 1; b < N; b++) {
+          const float pp = ph[a] * ph[b];
+          st += m.tau_ab[a][b] * pp;
+          st1 += pp;
+        }
+      const float tphi = st1 != 0.f ? st / st1 : m.tau;
+      const float f = m.dt / (tphi * m.eps);
+#pragma unroll
+      for (int a = 0; a < N; a++)
+        if (divphi[a] != 0.f) dp[a] = f * (lambda[a] - sum_l);
+      // projection onto the Gibbs simplex (simplex_projection.h:1-49)
+      float over = 0.f, sum_in = 0.f;
+      int count = 0;
+#pragma unroll
+      for (int a = 0; a < N; a++) {
+        const float v = ph[a] + dp[a];
+        if (divphi[a] != 0.f && v > 0.f && v < 1.f) {
+          count++;
+          sum_in += ph[a];
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < N; a++) {
+        const float v = ph[a] + dp[a];
+        if (v < 0.f) {
+          dp[a] -= v;
+          over -= v;
+        }
+      }
+      if (over > 0.f) {
+#pragma unroll
+        for (int b = 0; b < N; b++) {
+          const float v = ph[b] + dp[b];
+          if (divphi[b] != 0.f && v > 0.f && v < 1.f)
+            dp[b] -= sum_in != 0.f ? over * ph[b] / sum_in : over / (float)count;
+        }
+      }
+      int hit = -1;
+#pragma unroll
+      for (int a = 0; a < N; a++)
+        if (hit < 0 && divphi[a] != 0.f && ph[a] + dp[a] > 1.f) hit = a;
+      if (hit >= 0) {
+#pragma unroll
+        for (int a = 0; a < N; a++)
+          if (divphi[a] != 0.f) dp[a] = (a == hit) ? 1.f - ph[a] : -ph[a];
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < N; a++) sdp[(a * X1 + i1) * Y1 + j1] = dp[a];
+  }
+  }  // !pure
+  __syncthreads();
+
+  // ---- face fluxes of the mu update: dt * D grad mu - jscale * j_at
+  // (calculate_gradients.h:132-185, calculate_fluxes_concentration.h:4-145)
+  auto face_flux = [&](int ic, int jc, int in, int jn, bool xface, bool skip_at, float* out) {
+    // ic, jc / in, jn: region-1 coordinates of the two cells (n = +x or +y neighbour)
+    float pc[N], pn[N], tc[N], tn[N], gn[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      pc[a] = PH(a, ic + 1, jc + 1);
+      pn[a] = PH(a, in + 1, jn + 1);
+      gn[a] = (pn[a] - pc[a]) * (xface ? m.dx_inv : m.dy_inv);
+      if (xface) {  // tangential: centred y gradient of each cell
+        tc[a] = (PH(a, ic + 1, jc + 2) - PH(a, ic + 1, jc)) * m.half_dy_inv;
+        tn[a] = (PH(a, in + 1, jn + 2) - PH(a, in + 1, jn)) * m.half_dy_inv;
+      } else {  // centred x gradient (average of the two one-sided ones)
+        tc[a] = 0.5f * (PH(a, ic + 2, jc + 1) - PH(a, ic, jc + 1)) * m.dx_inv;
+        tn[a] = 0.5f * (PH(a, in + 2, jn + 1) - PH(a, in, jn + 1)) * m.dx_inv;
+      }
+    }
+    float muc[K1], mun[K1];
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      muc[k] = smu[(k * X1 + ic) * Y1 + jc];
+      mun[k] = smu[(k * X1 + in) * Y1 + jn];
+    }
+    // diffusion: face mobility (D(c) + D(n))/2 with D = sum_b DC_b phi_b (functionD.h)
+    const float h = xface ? m.dx_inv : m.dy_inv;
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      float jd = 0.f;
+#pragma unroll
+      for (int l = 0; l < K1; l++) {
+        float dcs = 0.f, dns = 0.f;
+#pragma unroll
+        for (int b = 0; b < N; b++) {
+          dcs += m.DC[b][k][l] * pc[b];
+          dns += m.DC[b][k][l] * pn[b];
+        }
+        jd += 0.5f * (dcs + dns) * (mun[l] - muc[l]) * h;
+      }
+      out[k] = m.dt * jd;
+    }
+    // antitrapping current
+    if (!skip_at && !pure) {
+      const float tl = 0.5f * (tc[L] + tn[L]);
+      const float norm_l = sqrtf(tl * tl + gn[L] * gn[L]);
+#pragma unroll
+      for (int a = 0; a < N - 1; a++) {
+        const float ta = 0.5f * (tc[a] + tn[a]);
+        const float n2 = ta * ta + gn[a] * gn[a];
+        if (n2 == 0.f) continue;
+        const float rn = rsqrtf(n2);
+        float sp = gn[a] * gn[L] + ta * tl;
+        if (norm_l > 0.f) sp *= rn / norm_l;
+        float sc = 1.f, sn = 1.f;
+        if (m.obstacle) {
+          const float uc = pc[a] * (1.f - pc[a]), un = pn[a] * (1.f - pn[a]);
+          sc = uc > 0.f ? pc[a] * (1.f - hphi<N>(pc, a)) * rsqrtf(uc) : 0.f;
+          sn = un > 0.f ? pn[a] * (1.f - hphi<N>(pn, a)) * rsqrtf(un) : 0.f;
+        }
+        const float dpc = sdp[(a * X1 + ic) * Y1 + jc], dpn = sdp[(a * X1 + in) * Y1 + jn];
+        const float pref = fabsf(sp) * (m.obstacle ? 0.5f : m.s_well) * gn[a] * rn;
+#pragma unroll
+        for (int k = 0; k < K1; k++) {
+          const float dcn = c_mu<K1>(m, mun, L, k) - c_mu<K1>(m, mun, a, k);
+          const float dcc = c_mu<K1>(m, muc, L, k) - c_mu<K1>(m, muc, a, k);
+          const float j = m.atf[a][k] * pref * (sn * dcn * dpn + sc * dcc * dpc);
+          out[k] -= m.jscale * j;
+        }
+      }
+    }
+  };
+  // x-faces between region-1 rows i and i+1, i in [0, TX], tile columns
+  for (int e = threadIdx.x; e < (TX + 1) * TY; e += nt) {
+    const int i = e / TY, j = 1 + e % TY;
+    float f[K1];
+    face_flux(i, j, i + 1, j, true, false, f);
+#pragma unroll
+    for (int k = 0; k < K1; k++) sfx[(k * (TX + 1) + i) * TY + (j - 1)] = f[k];
+  }
+  // y-faces between region-1 columns j and j+1, j in [0, TY], tile rows; the face whose
+  // lower cell sits on interior row mesh_y-5 (gidy == MESH_Y-2) carries no antitrapping
+  for (int e = threadIdx.x; e < TX * (TY + 1); e += nt) {
+    const int i = 1 + e / (TY + 1), j = e % (TY + 1);
+    const int gy = y0 - 1 + j;  // interior row of the lower cell
+    float f[K1];
+    face_flux(i, j, i, j + 1, false, gy == m.skip_row, f);
+#pragma unroll
+    for (int k = 0; k < K1; k++) sfy[(k * TX + (i - 1)) * (TY + 1) + j] = f[k];
+  }
+  __syncthreads();
+
+  // ---- mu and phi update of the tile (calculate_divergence_concentration.h:4-153)
+  for (int e = threadIdx.x; e < TX * TY; e += nt) {
+    const int ti = e / TY, tj = e % TY;
+    const int x = x0 + ti, y = y0 + tj;
+    if (x >= mx || y >= my) continue;
+    const int i1 = ti + 1, j1 = tj + 1;
+    float ph[N], dp[N], mu[K1], dc[K1];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      ph[a] = PH(a, i1 + 1, j1 + 1);
+      dp[a] = sdp[(a * X1 + i1) * Y1 + j1];
+    }
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      mu[k] = smu[(k * X1 + i1) * Y1 + j1];
+      dc[k] = (sfx[(k * (TX + 1) + ti + 1) * TY + tj] - sfx[(k * (TX + 1) + ti) * TY + tj]) * m.dx_inv +
+              (sfy[(k * TX + ti) * (TY + 1) + tj + 1] - sfy[(k * TX + ti) * (TY + 1) + tj]) * m.dy_inv;
+    }
+    int bulk = -1;
+#pragma unroll
+    for (int a = 0; a < N; a++)
+      if (bulk < 0 && ph[a] == 1.f) bulk = a;
+    float mnew[K1];
+    if (bulk >= 0) {
+      // c -> c + dc in the bulk phase, mu = dF/dc there (functionF_01.h:19-29)
+      float c[K1];
+#pragma unroll
+      for (int a = 0; a < N; a++)
+        if (a == bulk) {
+#pragma unroll
+          for (int k = 0; k < K1; k++) c[k] = c_mu<K1>(m, mu, a, k) + dc[k];
+#pragma unroll
+          for (int k = 0; k < K1; k++) {
+            float s = 2.f * m.A[a][k][k] * c[k] + m.Beff[a][k];
+#pragma unroll
+            for (int l = 0; l < K1; l++)
+              if (l != k) s += m.A[a][k][l] * c[l];
+            mnew[k] = s;
+          }
+        }
+    } else {
+      float hh[N];
+#pragma unroll
+      for (int a = 0; a < N; a++) hh[a] = hphi<N>(ph, a);
+      // dc -= sum_a c_a(mu) * dh_a/dt
+#pragma unroll
+      for (int a = 0; a < N; a++) {
+        float sdh = 0.f;
+#pragma unroll
+        for (int b = 0; b < N; b++) sdh += dhphi<N>(ph, a, b) * dp[b];
+#pragma unroll
+        for (int k = 0; k < K1; k++) dc[k] -= c_mu<K1>(m, mu, a, k) * sdh;
+      }
+      if (K1 == 1) {
+        float d = 0.f;
+#pragma unroll
+        for (int a = 0; a < N; a++) d += m.cmu[a][0][0] * hh[a];
+        mnew[0] = mu[0] + dc[0] / d;
+      } else {
+        // (dc/dmu) = sum_a cmu_a h_a, inverted in FP64
+        double D[MK][MK];
+#pragma unroll
+        for (int k = 0; k < K1; k++)
+#pragma unroll
+          for (int l = 0; l < K1; l++) {
+            double s = 0.0;
+#pragma unroll
+            for (int a = 0; a < N; a++) s += m.cmu_d[a][k][l] * (double)hh[a];
+            D[k][l] = s;
+          }
+        double dm[K1];
+        if (m.mu_solver == GP_MU_BINARY) {  // BINARY = 1 updates the first potential only
+#pragma unroll
+          for (int k = 0; k < K1; k++) dm[k] = k == 0 ? (double)dc[0] / D[0][0] : 0.0;
+        } else if (m.mu_solver == GP_MU_DILUTE) {
+#pragma unroll
+          for (int k = 0; k < K1; k++) dm[k] = (double)dc[k] / D[k][k];
+        } else if (K1 == 2) {
+          const double det = D[0][0] * D[K1 - 1][K1 - 1] - D[0][K1 - 1] * D[K1 - 1][0];
+          dm[0] = (D[K1 - 1][K1 - 1] * dc[0] - D[0][K1 - 1] * dc[K1 - 1]) / det;
+          dm[K1 - 1] = (D[0][0] * dc[K1 - 1] - D[K1 - 1][0] * dc[0]) / det;
+        } else {
+          // Gauss-Jordan with partial pivoting, K1 <= 3
+          double Aug[MK][MK + 1];
+#pragma unroll
+          for (int k = 0; k < K1; k++) {
+#pragma unroll
+            for (int l = 0; l < K1; l++) Aug[k][l] = D[k][l];
+            Aug[k][K1] = dc[k];
+          }
+#pragma unroll
+          for (int c = 0; c < K1; c++) {
+            int piv = c;
+#pragma unroll
+            for (int r = c + 1; r < K1; r++)
+              if (fabs(Aug[r][c]) > fabs(Aug[piv][c])) piv = r;
+#pragma unroll
+            for (int r = 0; r < K1; r++)
+              if (r == piv && piv != c) {
+#pragma unroll
+                for (int l = 0; l <= K1; l++) {
+                  const double t = Aug[c][l];
+                  Aug[c][l] = Aug[r][l];
+                  Aug[r][l] = t;
+                }
+              }
+            const double inv = 1.0 / Aug[c][c];
+#pragma unroll
+            for (int r = 0; r < K1; r++) {
+              if (r == c) continue;
+              const double f = Aug[r][c] * inv;
+#pragma unroll
+              for (int l = 0; l <= K1; l++) Aug[r][l] -= f * Aug[c][l];
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < K1; k++) dm[k] = Aug[k][K1] / Aug[k][k];
+        }
+#pragma unroll
+        for (int k = 0; k < K1; k++) mnew[k] = mu[k] + (float)dm[k];
+      }
+    }
+    const int64_t o = (int64_t)x * I.pitch + y;
+#pragma unroll
+    for (int k = 0; k < K1; k++) I.mu_out[o + k * I.plane] = mnew[k];
+#pragma unroll
+    for (int a = 0; a < N; a++) I.phi_out[o + a * I.plane] = ph[a] + dp[a];
+  }
+}
+
+// ---------------------------------------------------------------- host side
+
+Model make_model(const gp_model& g) {
+  Model m;
+  memset(&m, 0, sizeof m);
+  m.dx_inv = (float)(1.0 / g.dx);
+  m.dy_inv = (float)(1.0 / g.dy);
+  m.half_dy_inv = (float)(0.5 / g.dy);
+  m.dt = (float)g.dt;
+  m.eps = (float)g.epsilon;
+  m.inv_eps = (float)(1.0 / g.epsilon);
+  m.tau = (float)g.tau;
+  m.w_obst = (float)g.w_obstacle;
+  m.jscale = (float)(g.obstacle ? g.jat_obst : g.jat_well);
+  m.s_well = (float)g.s_well;
+  m.obstacle = g.obstacle;
+  m.mu_solver = g.mu_solver;
+  m.skip_row = (int)g.mesh_y - 5;
+  const int N = g.N, K1 = g.K1;
+  for (int a = 0; a < MP; a++)
+    for (int b = 0; b < MP; b++) {
+      m.Gamma[a][b] = (float)g.Gamma[a][b];
+      m.tau_ab[a][b] = (float)g.tau_ab[a][b];
+      m.dab[a][b] = (float)g.dab[a][b];
+      for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+          m.R[a][b][i][j] = (float)g.R[a][b][i][j];
+          m.Rinv[a][b][i][j] = (float)g.Rinv[a][b][i][j];
+        }
+      for (int c = 0; c < MP; c++) m.Gabc[a][b][c] = (float)g.Gamma_abc[a][b][c];
+    }
+  for (int a = 0; a < N; a++) {
+    m.C[a] = (float)g.C[a];
+    for (int i = 0; i < K1; i++) {
+      m.Beff[a][i] = (float)g.Beff[a][i];
+      m.B[a][i] = (float)g.B[a][i];
+      m.atf[a][i] = (float)(1.0 - g.Diff[a][i][i] / g.Diff[N - 1][i][i]);
+      for (int j = 0; j < K1; j++) {
+        m.cmu[a][i][j] = (float)g.cmu[a][i][j];
+        m.cmu_d[a][i][j] = g.cmu[a][i][j];
+        m.A[a][i][j] = (float)g.A[a][i][j];
+        double s = 0.0;
+        for (int k = 0; k < K1; k++) s += g.Diff[a][i][k] * g.cmu[a][k][j];
+        m.DC[a][i][j] = (float)s;
+      }
+    }
+  }
+  return m;
+}
+
+}  // namespace gp32
+
+using namespace gp32;
+
+// A batch of FP32 instances on the current device.
+struct gp_f32_batch {
+  int n = 0, N = 0, K1 = 0, aniso = 0;
+  int tx = 16, ty = 32;  // tile shape (autotuned)
+  std::vector<gp_model> gm;
+  std::vector<Inst> hinst[2];  // [buffer parity]
+  Inst* dinst[2] = {nullptr, nullptr};
+  Model* dmodel = nullptr;
+  int total_tiles = 0;
+};
+
+typedef void (*launch_fn)(const Inst*, int, const Model*, int, cudaStream_t);
+
+template <int N, int K1, bool AN, int TX, int TY>
+static void launch_tile(const Inst* inst, int ninst, const Model* models, int tiles, cudaStream_t s) {
+  using T = Tile<N, K1, AN, TX, TY>;
+  static unsigned long long configured = 0;  // one bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(configured & (1ull << dev))) {
+    cudaFuncSetAttribute(k_step32<N, K1, AN, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes);
+    configured |= 1ull << dev;
+  }
+  k_step32<N, K1, AN, TX, TY><<<tiles, 256, T::bytes, s>>>(inst, ninst, models);
+}
+
+template <int N, int K1, bool AN>
+static launch_fn pick_tile(int tx, int ty) {
+  if (tx == 16 && ty == 32) return launch_tile<N, K1, AN, 16, 32>;
+  if (tx == 8 && ty == 32) return launch_tile<N, K1, AN, 8, 32>;
+  if (tx == 32 && ty == 32) return launch_tile<N, K1, AN, 32, 32>;
+  if (tx == 16 && ty == 64) return launch_tile<N, K1, AN, 16, 64>;
+  return nullptr;
+}
+
+static launch_fn pick(int N, int K1, int an, int tx, int ty) {
+#define GP_PICK(NN, KK)                                                                 \
+  if (N == NN && K1 == KK) return an ? pick_tile<NN, KK, true>(tx, ty) : pick_tile<NN, KK, false>(tx, ty);
+  GP_PICK(2, 1) GP_PICK(2, 2) GP_PICK(3, 1) GP_PICK(3, 2) GP_PICK(4, 1) GP_PICK(4, 2)
+  GP_PICK(2, 3) GP_PICK(3, 3) GP_PICK(4, 3)
+#undef GP_PICK
+  return nullptr;
+}
+
+int gp_f32_supported(const gp_model& m) { return pick(m.N, m.K1, m.anisotropy, 16, 32) != nullptr; }
+
+// tile shapes offered to the autotuner
+static const int kTileShapes[][2] = {{16, 32}, {8, 32}, {32, 32}, {16, 64}};
+static const int kNumTileShapes = 4;
+
+int gp_f32_tile_shape_count() { return kNumTileShapes; }
+void gp_f32_tile_shape(int i, int* tx, int* ty) {
+  *tx = kTileShapes[i][0];
+  *ty = kTileShapes[i][1];
+}
+
+// Create a batch from n models (same N, K1, anisotropy switch); state buffers
+// are owned by the caller of gp_f32_batch_bind.
+cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** out) {
+  if (n < 1) return cudaErrorInvalidValue;
+  for (int i = 1; i < n; i++)
+    if (models[i].N != models[0].N || models[i].K1 != models[0].K1 || models[i].anisotropy != models[0].anisotropy)
+      return cudaErrorInvalidValue;
+  if (!pick(models[0].N, models[0].K1, models[0].anisotropy, 16, 32)) return cudaErrorNotSupported;
+  gp_f32_batch* b = new gp_f32_batch();
+  b->n = n;
+  b->N = models[0].N;
+  b->K1 = models[0].K1;
+  b->aniso = models[0].anisotropy;
+  b->gm.assign(models, models + n);
+  std::vector<Model> hm(n);
+  for (int i = 0; i < n; i++) hm[i] = make_model(models[i]);
+  cudaError_t e = cudaMalloc(&b->dmodel, sizeof(Model) * n);
+  if (e == cudaSuccess) e = cudaMemcpy(b->dmodel, hm.data(), sizeof(Model) * n, cudaMemcpyHostToDevice);
+  for (int p = 0; e == cudaSuccess && p < 2; p++) {
+    b->hinst[p].resize(n);
+    e = cudaMalloc(&b->dinst[p], sizeof(Inst) * n);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(b->dmodel);
+    cudaFree(b->dinst[0]);
+    cudaFree(b->dinst[1]);
+    delete b;
+    return e;
+  }
+  *out = b;
+  return cudaSuccess;
+}
+
+void gp_f32_batch_destroy(gp_f32_batch* b) {
+  if (!b) return;
+  cudaFree(b->dmodel);
+  cudaFree(b->dinst[0]);
+  cudaFree(b->dinst[1]);
+  delete b;
+}
+
+// Bind the two state buffers of instance i (parity 0 reads buffer A, writes B).
+void gp_f32_batch_bind(gp_f32_batch* b, int i, float* phiA, float* muA, float* phiB, float* muB, int pitch,
+                       int64_t plane) {
+  for (int p = 0; p < 2; p++) {
+    Inst& I = b->hinst[p][i];
+    I.phi = p ? phiB : phiA;
+    I.mu = p ? muB : muA;
+    I.phi_out = p ? phiA : phiB;
+    I.mu_out = p ? muA : muB;
+    I.plane = plane;
+    I.pitch = pitch;
+    I.mx = (int)b->gm[i].mesh_x;
+    I.my = (int)b->gm[i].mesh_y;
+    I.model = i;
+    I.bc = gp_bc_of(b->gm[i]);
+  }
+}
+
+// Recompute the tile decomposition for shape (tx, ty) and upload the instance tables.
+cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
+  if (!pick(b->N, b->K1, b->aniso, tx, ty)) return cudaErrorInvalidValue;
+  b->tx = tx;
+  b->ty = ty;
+  int t = 0;
+  for (int i = 0; i < b->n; i++) {
+    const int txs = (int)((b->gm[i].mesh_x + tx - 1) / tx), tys = (int)((b->gm[i].mesh_y + ty - 1) / ty);
+    for (int p = 0; p < 2; p++) {
+      b->hinst[p][i].tiles_y = tys;
+      b->hinst[p][i].tile_begin = t;
+    }
+    t += txs * tys;
+  }
+  b->total_tiles = t;
+  for (int p = 0; p < 2; p++) {
+    cudaError_t e = cudaMemcpy(b->dinst[p], b->hinst[p].data(), sizeof(Inst) * b->n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+int gp_f32_batch_tiles(const gp_f32_batch* b) { return b->total_tiles; }
+
+// One step of every instance, reading buffer parity `parity`.
+cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
+  launch_fn f = pick(b->N, b->K1, b->aniso, b->tx, b->ty);
+  if (!f) return cudaErrorInvalidValue;
+  f(b->dinst[parity & 1], b->n, b->dmodel, b->total_tiles, s);
+  return cudaGetLastError();
 }
