@@ -243,6 +243,7 @@ def run_ours(args, world, rank, local):
     N, K1 = models[0].N, models[0].K1
     peak, peak_kind = measured_peaks()
     fp64 = None
+    tile = None
     barrier(world)
     if len(models) == 1:
         m = models[0]
@@ -268,8 +269,7 @@ def run_ours(args, world, rank, local):
         ctx = mb.Batch(models)
         for i, f in enumerate(fields):
             ctx.upload(i, *f)
-        if args.autotune:
-            ctx.autotune(os.path.join(ROOT, "microsim_b200", "tile_cache.txt"))
+        tile = ctx.autotune(None) if not args.no_autotune else None
         stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
         ctx.step(args.warmup)
         ctx.sync()
@@ -343,7 +343,8 @@ def run_ours(args, world, rank, local):
             "vs_baseline": None, "dtype": "f32" if prec == mb.GP_FP32 else "f64", "data": "synthetic",
             "config": {"workload": wname, "precision": args.precision if len(models) == 1 else "fp32",
                        "instances": len(models), "cells_per_gpu": cells, "state_prepared_steps": prep,
-                       "parallelism": f"replicas{world}" if world > 1 else "single", "l2": l2},
+                       "parallelism": f"replicas{world}" if world > 1 else "single", "l2": l2,
+                       "tile": list(tile) if len(models) > 1 and tile else [16, 32]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
                          "note": f"algorithmic {alg_bytes} B/cell-update (read+write phi, mu once) per "
@@ -373,7 +374,7 @@ def main():
                     help="steps of the FP32 form run before timing to reach a mid-run state (-1: half the run)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

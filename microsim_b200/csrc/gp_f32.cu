@@ -35,7 +35,7 @@ constexpr int MP = GP_MAX_PHASES;
 constexpr int MK = GP_MAX_K1;
 
 // FP32 model constants of one instance (built on the host from gp_model).
-struct Model {
+struct alignas(16) Model {
   float dx_inv, dy_inv, half_dy_inv, dt, eps, inv_eps, tau, w_obst, jscale, s_well;
   int obstacle, mu_solver, skip_row, pad;
   float Gamma[MP][MP];
@@ -53,9 +53,10 @@ struct Model {
   float atf[MP][MK];     // 1 - Diff[a][k][k] / Diff[N-1][k][k]
   double cmu_d[MP][MK][MK];
 };
+static_assert(sizeof(Model) % 16 == 0, "Model is copied to shared memory as float4");
 
 // One instance of a batch: its buffers and geometry.
-struct Inst {
+struct alignas(16) Inst {
   const float* phi;
   const float* mu;
   float* phi_out;
@@ -143,22 +144,95 @@ __device__ __forceinline__ void aniso_terms(float dab, float q0, float q1, float
   }
 }
 
+// ---------------------------------------------------------------- shared pieces of the update
+
+// The pieces below are shared by the pure-tile path and the full path.  They
+// are written with explicit round-to-nearest intrinsics (never contracted or
+// re-associated by the compiler), so a cell gets the same bits whichever path
+// its tile takes -- the result does not depend on the tile shape.
+
+// Diffusion flux of every component through one face, dt * sum_l (D_c + D_n)/2
+// (mu_n - mu_c) * h (calculate_gradients.h:132-185 with functionD.h).
+template <int K1>
+__device__ __forceinline__ void diff_flux(const Model& m, const float (&Dc)[MK][MK], const float (&Dn)[MK][MK],
+                                          const float* muc, const float* mun, float h, float* out) {
+#pragma unroll
+  for (int k = 0; k < K1; k++) {
+    float jd = 0.f;
+#pragma unroll
+    for (int l = 0; l < K1; l++) {
+      const float dm = __fmul_rn(__fmul_rn(0.5f, __fadd_rn(Dc[k][l], Dn[k][l])), __fsub_rn(mun[l], muc[l]));
+      jd = __fadd_rn(jd, __fmul_rn(dm, h));
+    }
+    out[k] = __fmul_rn(m.dt, jd);
+  }
+}
+
+// phi-weighted mobility D = sum_b DC_b phi_b (functionD.h:1-16)
+template <int N, int K1>
+__device__ __forceinline__ void mobility(const Model& m, const float* ph, float (&D)[MK][MK]) {
+#pragma unroll
+  for (int k = 0; k < K1; k++)
+#pragma unroll
+    for (int l = 0; l < K1; l++) {
+      float s = 0.f;
+#pragma unroll
+      for (int b = 0; b < N; b++) s = __fmaf_rn(m.DC[b][k][l], ph[b], s);
+      D[k][l] = s;
+    }
+}
+
+// net face flux into a cell: (F(+x) - F(-x))/dx + (F(+y) - F(-y))/dy
+__device__ __forceinline__ float flux_div(const Model& m, float fxp, float fxm, float fyp, float fym) {
+  return __fadd_rn(__fmul_rn(__fsub_rn(fxp, fxm), m.dx_inv), __fmul_rn(__fsub_rn(fyp, fym), m.dy_inv));
+}
+
+// bulk cell of phase `bulk`: c -> c + dc, mu = dF/dc (calculate_divergence_concentration.h:216-224)
+template <int N, int K1>
+__device__ __forceinline__ void bulk_update(const Model& m, int bulk, const float* mu, const float* dc, float* mnew) {
+#pragma unroll
+  for (int a = 0; a < N; a++)
+    if (a == bulk) {
+      float c[K1];
+#pragma unroll
+      for (int k = 0; k < K1; k++) {
+        float s = 0.f;
+#pragma unroll
+        for (int l = 0; l < K1; l++) s = __fmaf_rn(m.cmu[a][k][l], __fsub_rn(mu[l], m.Beff[a][l]), s);
+        c[k] = __fadd_rn(s, dc[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < K1; k++) {
+        float s = __fmaf_rn(__fmul_rn(2.f, m.A[a][k][k]), c[k], m.Beff[a][k]);
+#pragma unroll
+        for (int l = 0; l < K1; l++)
+          if (l != k) s = __fmaf_rn(m.A[a][k][l], c[l], s);
+        mnew[k] = s;
+      }
+    }
+}
+
 // ---------------------------------------------------------------- the fused step
 
 template <int N, int K1, bool ANISO, int TX, int TY>
 struct Tile {
+  static_assert(TY % 32 == 0, "a tile row is a whole number of warps");
   static constexpr int P = Pairs<N>::P;
   static constexpr int X2 = TX + 4, Y2 = TY + 4;  // phi region: tile +- 2
   static constexpr int X1 = TX + 2, Y1 = TY + 2;  // mu / Delta-phi region: tile +- 1
+  static constexpr int W = TY + 8;                 // staged row: y0-4 .. y0+TY+3 (16-byte aligned)
+  static constexpr int Q = W / 4;                  // float4 per staged row
   // shared-memory layout (floats)
-  static constexpr int o_phi = 0;
-  static constexpr int o_mu = o_phi + N * X2 * Y2;
-  static constexpr int o_dphi = o_mu + K1 * X1 * Y1;
-  static constexpr int o_bx = o_dphi + N * X1 * Y1;                  // x-face brackets [P][TX+3][TY+2]
-  static constexpr int o_by = o_bx + (ANISO ? P : P) * (TX + 3) * (TY + 2);  // y-face brackets [P][TX+2][TY+3]
-  static constexpr int o_fx = o_by + P * (TX + 2) * (TY + 3);        // mu-update x-face fluxes [K1][TX+1][TY]
-  static constexpr int o_fy = o_fx + K1 * (TX + 1) * TY;             // mu-update y-face fluxes [K1][TX][TY+1]
-  static constexpr int total = o_fy + K1 * TX * (TY + 1);
+  static constexpr int o_phi = 0;                                 // [N][X2][W]
+  static constexpr int o_mu = o_phi + N * X2 * W;                 // [K1][X1][W]
+  static constexpr int o_dphi = o_mu + K1 * X1 * W;               // [N][X1][Y1]
+  static constexpr int o_bx = o_dphi + N * X1 * Y1;               // x-face brackets [P][TX+3][TY+2]
+  static constexpr int o_by = o_bx + P * (TX + 3) * (TY + 2);     // y-face brackets [P][TX+2][TY+3]
+  static constexpr int o_fx = o_by + P * (TX + 2) * (TY + 3);     // mu-update x-face fluxes [K1][TX+1][TY]
+  static constexpr int o_fy = o_fx + K1 * (TX + 1) * TY;          // mu-update y-face fluxes [K1][TX][TY+1]
+  static constexpr int o_list = o_fy + K1 * TX * (TY + 1);        // active ring cells (ints) [X1*Y1]
+  static constexpr int o_act = o_list + X1 * Y1;                  // active flags (ints) [X1*Y1]
+  static constexpr int total = o_act + X1 * Y1;
   static constexpr size_t bytes = total * sizeof(float);
 };
 
@@ -166,17 +240,16 @@ template <int N, int K1, bool ANISO, int TX, int TY>
 __global__ void __launch_bounds__(256) k_step32(const Inst* __restrict__ insts, int ninst,
                                                 const Model* __restrict__ models) {
   using T = Tile<N, K1, ANISO, TX, TY>;
-  constexpr int P = T::P, X2 = T::X2, Y2 = T::Y2, X1 = T::X1, Y1 = T::Y1;
+  constexpr int X2 = T::X2, Y2 = T::Y2, X1 = T::X1, Y1 = T::Y1, W = T::W, Q = T::Q;
   constexpr int L = N - 1;
-  extern __shared__ float sm[];
+  extern __shared__ __align__(16) float sm[];
   float* sphi = sm + T::o_phi;
   float* smu = sm + T::o_mu;
   float* sdp = sm + T::o_dphi;
-  float* sbx = sm + T::o_bx;
-  float* sby = sm + T::o_by;
-  float* sfx = sm + T::o_fx;
-  float* sfy = sm + T::o_fy;
+  __shared__ __align__(16) Model sModel;
+  __shared__ __align__(16) Inst sInst;
   __shared__ int s_inst;
+  const int nt = blockDim.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = nt >> 5;
 
   // which instance / tile (binary search on tile_begin)
   const int tile = blockIdx.x;
@@ -188,303 +261,423 @@ __global__ void __launch_bounds__(256) k_step32(const Inst* __restrict__ insts, 
       else hi = mid - 1;
     }
     s_inst = lo;
+    sInst = insts[lo];
   }
   __syncthreads();
-  const Inst& I = insts[s_inst];
-  const Model& m = models[I.model];
+  {  // the instance's model constants into shared memory
+    const float4* src = reinterpret_cast<const float4*>(models + sInst.model);
+    float4* dst = reinterpret_cast<float4*>(&sModel);
+    for (int e = threadIdx.x; e < (int)(sizeof(Model) / 16); e += nt) dst[e] = __ldg(src + e);
+  }
+  const Inst& I = sInst;
+  const Model& m = sModel;
   const int lt = tile - I.tile_begin;
   const int x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
   const int mx = I.mx, my = I.my;
-  const int nt = blockDim.x;
+
+  auto PH = [&](int a, int i, int j) -> float { return sphi[(a * X2 + i) * W + j + 2]; };  // region-2 coords
+  auto MU = [&](int k, int i, int j) -> float { return smu[(k * X1 + i) * W + j + 3]; };   // region-1 coords
 
   // ---- stage phi (tile +- 2) and mu (tile +- 1)
-  for (int e = threadIdx.x; e < X2 * Y2; e += nt) {
-    const int i = e / Y2, j = e % Y2;
-    const int gx = gp_map_any(x0 - 2 + i, mx, I.bc.phi_x), gy = gp_map_any(y0 - 2 + j, my, I.bc.phi_y);
-    const float* p = I.phi + (int64_t)gx * I.pitch + gy;
+  const bool inner = x0 >= 2 && x0 + TX + 2 <= mx && y0 >= 4 && y0 + TY + 4 <= my;
+  if (inner) {
+    // whole 16-byte aligned rows y0-4 .. y0+TY+3, no boundary maps needed
+    for (int e = threadIdx.x; e < N * X2 * Q; e += nt) {
+      const int a = e / (X2 * Q), r = (e / Q) % X2, q = e % Q;
+      const float4 v = __ldg(reinterpret_cast<const float4*>(I.phi + a * I.plane + (int64_t)(x0 - 2 + r) * I.pitch +
+                                                             (y0 - 4)) + q);
+      reinterpret_cast<float4*>(sphi + (a * X2 + r) * W)[q] = v;
+    }
+    for (int e = threadIdx.x; e < K1 * X1 * Q; e += nt) {
+      const int k = e / (X1 * Q), r = (e / Q) % X1, q = e % Q;
+      const float4 v = __ldg(reinterpret_cast<const float4*>(I.mu + k * I.plane + (int64_t)(x0 - 1 + r) * I.pitch +
+                                                             (y0 - 4)) + q);
+      reinterpret_cast<float4*>(smu + (k * X1 + r) * W)[q] = v;
+    }
+  } else {
+    for (int e = threadIdx.x; e < X2 * Y2; e += nt) {
+      const int i = e / Y2, j = e % Y2;
+      const int gx = gp_map_any(x0 - 2 + i, mx, I.bc.phi_x), gy = gp_map_any(y0 - 2 + j, my, I.bc.phi_y);
+      const float* p = I.phi + (int64_t)gx * I.pitch + gy;
 #pragma unroll
-    for (int a = 0; a < N; a++) sphi[a * X2 * Y2 + e] = __ldg(p + a * I.plane);
-  }
-  for (int e = threadIdx.x; e < X1 * Y1; e += nt) {
-    const int i = e / Y1, j = e % Y1;
-    const int gx = gp_map_any(x0 - 1 + i, mx, I.bc.mu_x), gy = gp_map_any(y0 - 1 + j, my, I.bc.mu_y);
-    const float* p = I.mu + (int64_t)gx * I.pitch + gy;
+      for (int a = 0; a < N; a++) sphi[(a * X2 + i) * W + j + 2] = __ldg(p + a * I.plane);
+    }
+    for (int e = threadIdx.x; e < X1 * Y1; e += nt) {
+      const int i = e / Y1, j = e % Y1;
+      const int gx = gp_map_any(x0 - 1 + i, mx, I.bc.mu_x), gy = gp_map_any(y0 - 1 + j, my, I.bc.mu_y);
+      const float* p = I.mu + (int64_t)gx * I.pitch + gy;
 #pragma unroll
-    for (int k = 0; k < K1; k++) smu[k * X1 * Y1 + e] = __ldg(p + k * I.plane);
+      for (int k = 0; k < K1; k++) smu[(k * X1 + i) * W + j + 3] = __ldg(p + k * I.plane);
+    }
   }
   __syncthreads();
-
-  auto PH = [&](int a, int i, int j) -> float { return sphi[(a * X2 + i) * Y2 + j]; };
 
   // ---- pure-tile test: when every staged cell is the same pure phase, Delta-phi
   // is exactly zero on the ring (divphi = 0) and so is every antitrapping
-  // current (zero gradients), so those stages are skipped; the flux and update
-  // code below is shared, which keeps the results bit-identical to the full path.
+  // current (zero gradients): the tile's update is diffusion in one phase.
   int b0 = -1;
 #pragma unroll
   for (int a = N - 1; a >= 0; a--)
-    if (sphi[a * X2 * Y2] == 1.f) b0 = a;
+    if (PH(a, 0, 0) == 1.f) b0 = a;
   bool ok = b0 >= 0;
   for (int e = threadIdx.x; ok && e < X2 * Y2; e += nt) {
+    const int i = e / Y2, j = e % Y2;
 #pragma unroll
-    for (int a = 0; a < N; a++) ok &= (sphi[a * X2 * Y2 + e] == (a == b0 ? 1.f : 0.f));
+    for (int a = 0; a < N; a++) ok &= (PH(a, i, j) == (a == b0 ? 1.f : 0.f));
   }
   const bool pure = __syncthreads_and(ok) != 0;
+
   if (pure) {
-    for (int e = threadIdx.x; e < N * X1 * Y1; e += nt) sdp[e] = 0.f;
-  } else {
-  // ---- gradient-energy brackets per face and phase pair
-  // x-face between region-2 rows i and i+1 (i in [0, TX+2]), at region-2 columns j in [1, TY+2]
-  //   Bk = a_c^2 Qx + a_c |q|^2 (Rinv dadq)_x   (anisotropic),  Bk = Qx (isotropic)
-  //   with Qx = sx_a gx_b - sx_b gx_a, and the flux of phase a (pair b) through the
-  //   face  F_ab = -Bk sx_b,  F_ba = +Bk sx_a  (function_A_0x divdAdgradphi).
-  for (int e = threadIdx.x; e < (TX + 3) * (TY + 2); e += nt) {
-    const int i = e / (TY + 2), j = 1 + e % (TY + 2);
-    float sx[N], gxv[N], cy0[N], cy1[N];
-#pragma unroll
-    for (int a = 0; a < N; a++) {
-      const float pc = PH(a, i, j), pf = PH(a, i + 1, j);
-      sx[a] = 0.5f * (pc + pf);
-      gxv[a] = (pf - pc) * m.dx_inv;
-      cy0[a] = (PH(a, i, j + 1) - PH(a, i, j - 1)) * m.half_dy_inv;
-      cy1[a] = (PH(a, i + 1, j + 1) - PH(a, i + 1, j - 1)) * m.half_dy_inv;
-    }
+    float Db[MK][MK];
 #pragma unroll
     for (int a = 0; a < N; a++)
+      if (a == b0) {
 #pragma unroll
-      for (int b = a + 1; b < N; b++) {
-        const int p = Pairs<N>::index(a, b);
-        const float Qx = sx[a] * gxv[b] - sx[b] * gxv[a];
-        float bk = Qx;
-        if (ANISO) {
-          const float Qy = 0.5f * (sx[a] * (cy0[b] + cy1[b]) - sx[b] * (cy0[a] + cy1[a]));
-          const float q0 = m.R[a][b][0][0] * Qx + m.R[a][b][0][1] * Qy;
-          const float q1 = m.R[a][b][1][0] * Qx + m.R[a][b][1][1] * Qy;
-          float ac, q2, e0, e1;
-          aniso_terms(m.dab[a][b], q0, q1, ac, q2, e0, e1);
-          bk = ac * ac * Qx + ac * (m.Rinv[a][b][0][0] * e0 + m.Rinv[a][b][0][1] * e1);
-        }
-        sbx[(p * (TX + 3) + i) * (TY + 2) + (j - 1)] = bk;
+        for (int k = 0; k < K1; k++)
+#pragma unroll
+          for (int l = 0; l < K1; l++) Db[k][l] = m.DC[a][k][l];
       }
+    for (int r = warp; r < TX; r += nw) {
+      const int x = x0 + r;
+      if (x >= mx) break;
+#pragma unroll
+      for (int c0 = 0; c0 < TY; c0 += 32) {
+        const int c = c0 + lane, y = y0 + c;
+        if (y >= my) continue;
+        const int i1 = r + 1, j1 = c + 1;
+        float mc[K1], mb[K1], mf[K1], ml[K1], mr[K1];
+#pragma unroll
+        for (int k = 0; k < K1; k++) {
+          mc[k] = MU(k, i1, j1);
+          mb[k] = MU(k, i1 - 1, j1);
+          mf[k] = MU(k, i1 + 1, j1);
+          ml[k] = MU(k, i1, j1 - 1);
+          mr[k] = MU(k, i1, j1 + 1);
+        }
+        float fxp[K1], fxm[K1], fyp[K1], fym[K1], dc[K1], mnew[K1];
+        diff_flux<K1>(m, Db, Db, mc, mf, m.dx_inv, fxp);
+        diff_flux<K1>(m, Db, Db, mb, mc, m.dx_inv, fxm);
+        diff_flux<K1>(m, Db, Db, mc, mr, m.dy_inv, fyp);
+        diff_flux<K1>(m, Db, Db, ml, mc, m.dy_inv, fym);
+#pragma unroll
+        for (int k = 0; k < K1; k++) dc[k] = flux_div(m, fxp[k], fxm[k], fyp[k], fym[k]);
+        bulk_update<N, K1>(m, b0, mc, dc, mnew);
+        const int64_t o = (int64_t)x * I.pitch + y;
+#pragma unroll
+        for (int k = 0; k < K1; k++) I.mu_out[o + k * I.plane] = mnew[k];
+#pragma unroll
+        for (int a = 0; a < N; a++) I.phi_out[o + a * I.plane] = (a == b0) ? 1.f : 0.f;
+      }
+    }
+    return;
   }
-  // y-face between region-2 columns j and j+1 (j in [0, TY+2]), at rows i in [1, TX+2]
-  for (int e = threadIdx.x; e < (TX + 2) * (TY + 3); e += nt) {
-    const int i = 1 + e / (TY + 3), j = e % (TY + 3);
-    float sy[N], gyv[N], cx0[N], cx1[N];
+
+  // ---- tile touches an interface.  Active ring cells (some divphi != 0) are
+  // flagged and compacted into a list; gradient-energy brackets are evaluated
+  // only on faces next to an active cell; Delta-phi is computed for the listed
+  // cells (calculate_divergence_phasefield.h:4-62).
+  int* s_list = reinterpret_cast<int*>(sm + T::o_list);
+  int* s_act = reinterpret_cast<int*>(sm + T::o_act);
+  float* sbx = sm + T::o_bx;
+  float* sby = sm + T::o_by;
+  float* sfx = sm + T::o_fx;
+  float* sfy = sm + T::o_fy;
+  __shared__ int s_nact;
+  if (threadIdx.x == 0) s_nact = 0;
+  __syncthreads();
+  for (int e0 = 0; e0 < X1 * Y1; e0 += nt) {
+    const int e = e0 + threadIdx.x;
+    bool act = false;
+    if (e < X1 * Y1) {
+      const int i1 = e / Y1, j1 = e % Y1;
+      const int i = i1 + 1, j = j1 + 1;
 #pragma unroll
-    for (int a = 0; a < N; a++) {
-      const float pc = PH(a, i, j), pr = PH(a, i, j + 1);
-      sy[a] = 0.5f * (pc + pr);
-      gyv[a] = (pr - pc) * m.dy_inv;
-      cx0[a] = 0.5f * (PH(a, i + 1, j) - PH(a, i - 1, j)) * m.dx_inv;
-      cx1[a] = 0.5f * (PH(a, i + 1, j + 1) - PH(a, i - 1, j + 1)) * m.dx_inv;
-    }
-#pragma unroll
-    for (int a = 0; a < N; a++)
-#pragma unroll
-      for (int b = a + 1; b < N; b++) {
-        const int p = Pairs<N>::index(a, b);
-        const float Qy = sy[a] * gyv[b] - sy[b] * gyv[a];
-        float bk = Qy;
-        if (ANISO) {
-          const float Qx = 0.5f * (sy[a] * (cx0[b] + cx1[b]) - sy[b] * (cx0[a] + cx1[a]));
-          const float q0 = m.R[a][b][0][0] * Qx + m.R[a][b][0][1] * Qy;
-          const float q1 = m.R[a][b][1][0] * Qx + m.R[a][b][1][1] * Qy;
-          float ac, q2, e0, e1;
-          aniso_terms(m.dab[a][b], q0, q1, ac, q2, e0, e1);
-          bk = ac * ac * Qy + ac * (m.Rinv[a][b][1][0] * e0 + m.Rinv[a][b][1][1] * e1);
-        }
-        sby[(p * (TX + 2) + (i - 1)) * (TY + 3) + j] = bk;
+      for (int a = 0; a < N; a++) {
+        const float pc = PH(a, i, j);
+        const float gf = (PH(a, i + 1, j) - pc) * m.dx_inv, gb = (pc - PH(a, i - 1, j)) * m.dx_inv;
+        const float gr = (PH(a, i, j + 1) - pc) * m.dy_inv, gl = (pc - PH(a, i, j - 1)) * m.dy_inv;
+        act |= ((gf - gb) * m.dx_inv + (gr - gl) * m.dy_inv) != 0.f;
+        sdp[a * X1 * Y1 + e] = 0.f;
       }
+      s_act[e] = act;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, act);
+    int base = 0;
+    if (lane == 0 && bal) base = atomicAdd(&s_nact, __popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (act) s_list[base + __popc(bal & ((1u << lane) - 1u))] = e;
   }
   __syncthreads();
 
-  // ---- Delta-phi on the tile plus one ring (calculate_divergence_phasefield.h:4-62)
-  for (int e = threadIdx.x; e < X1 * Y1; e += nt) {
+  // gradient-energy bracket of pair (a, b) on the x-face between region-2 rows
+  // i and i+1 at column j (and on the y-face between columns j and j+1 at row i):
+  //   Bk = a_c^2 Q_n + a_c |q|^2 (Rinv dadq)_n (anisotropic), Bk = Q_n (isotropic),
+  //   Q_n = s_a g_b - s_b g_a; the flux of phase a (pair b) through the face is
+  //   -Bk s_b, that of b (pair a) +Bk s_a (function_A_0x divdAdgradphi).
+  auto bk_x = [&](int i, int j, int a, int b) -> float {
+    const float pa = PH(a, i, j), pfa = PH(a, i + 1, j), pb = PH(b, i, j), pfb = PH(b, i + 1, j);
+    const float sa = 0.5f * (pa + pfa), sb = 0.5f * (pb + pfb);
+    const float Qx = sa * ((pfb - pb) * m.dx_inv) - sb * ((pfa - pa) * m.dx_inv);
+    if (!ANISO) return Qx;
+    const float cya = (PH(a, i, j + 1) - PH(a, i, j - 1)) * m.half_dy_inv +
+                      (PH(a, i + 1, j + 1) - PH(a, i + 1, j - 1)) * m.half_dy_inv;
+    const float cyb = (PH(b, i, j + 1) - PH(b, i, j - 1)) * m.half_dy_inv +
+                      (PH(b, i + 1, j + 1) - PH(b, i + 1, j - 1)) * m.half_dy_inv;
+    const float Qy = 0.5f * (sa * cyb - sb * cya);
+    const float q0 = m.R[a][b][0][0] * Qx + m.R[a][b][0][1] * Qy;
+    const float q1 = m.R[a][b][1][0] * Qx + m.R[a][b][1][1] * Qy;
+    float ac, q2, e0, e1;
+    aniso_terms(m.dab[a][b], q0, q1, ac, q2, e0, e1);
+    return ac * ac * Qx + ac * (m.Rinv[a][b][0][0] * e0 + m.Rinv[a][b][0][1] * e1);
+  };
+  auto bk_y = [&](int i, int j, int a, int b) -> float {
+    const float pa = PH(a, i, j), pra = PH(a, i, j + 1), pb = PH(b, i, j), prb = PH(b, i, j + 1);
+    const float sa = 0.5f * (pa + pra), sb = 0.5f * (pb + prb);
+    const float Qy = sa * ((prb - pb) * m.dy_inv) - sb * ((pra - pa) * m.dy_inv);
+    if (!ANISO) return Qy;
+    const float cxa = 0.5f * (PH(a, i + 1, j) - PH(a, i - 1, j)) * m.dx_inv +
+                      0.5f * (PH(a, i + 1, j + 1) - PH(a, i - 1, j + 1)) * m.dx_inv;
+    const float cxb = 0.5f * (PH(b, i + 1, j) - PH(b, i - 1, j)) * m.dx_inv +
+                      0.5f * (PH(b, i + 1, j + 1) - PH(b, i - 1, j + 1)) * m.dx_inv;
+    const float Qx = 0.5f * (sa * cxb - sb * cxa);
+    const float q0 = m.R[a][b][0][0] * Qx + m.R[a][b][0][1] * Qy;
+    const float q1 = m.R[a][b][1][0] * Qx + m.R[a][b][1][1] * Qy;
+    float ac, q2, e0, e1;
+    aniso_terms(m.dab[a][b], q0, q1, ac, q2, e0, e1);
+    return ac * ac * Qy + ac * (m.Rinv[a][b][1][0] * e0 + m.Rinv[a][b][1][1] * e1);
+  };
+
+  // x-face between region-2 rows i and i+1 (i in [0, TX+2]) at region-2 columns
+  // j in [1, TY+2]; read by ring cell (i-1, j-1) as its +x face and by ring cell
+  // (i, j-1) as its -x face (region-1 coordinates)
+  for (int e = threadIdx.x; e < (TX + 3) * (TY + 2); e += nt) {
+    const int i = e / (TY + 2), j = 1 + e % (TY + 2);
+    const bool need = (i >= 1 && s_act[(i - 1) * Y1 + (j - 1)]) || (i <= TX + 1 && s_act[i * Y1 + (j - 1)]);
+    if (!need) continue;
+#pragma unroll
+    for (int a = 0; a < N; a++)
+#pragma unroll
+      for (int b = a + 1; b < N; b++)
+        sbx[(Pairs<N>::index(a, b) * (TX + 3) + i) * (TY + 2) + (j - 1)] = bk_x(i, j, a, b);
+  }
+  // y-face between region-2 columns j and j+1 (j in [0, TY+2]) at rows i in [1, TX+2]
+  for (int e = threadIdx.x; e < (TX + 2) * (TY + 3); e += nt) {
+    const int i = 1 + e / (TY + 3), j = e % (TY + 3);
+    const bool need = (j >= 1 && s_act[(i - 1) * Y1 + (j - 1)]) || (j <= TY + 1 && s_act[(i - 1) * Y1 + j]);
+    if (!need) continue;
+#pragma unroll
+    for (int a = 0; a < N; a++)
+#pragma unroll
+      for (int b = a + 1; b < N; b++)
+        sby[(Pairs<N>::index(a, b) * (TX + 2) + (i - 1)) * (TY + 3) + j] = bk_y(i, j, a, b);
+  }
+  __syncthreads();
+
+  const int nact = s_nact;
+  for (int idx = threadIdx.x; idx < nact; idx += nt) {
+    const int e = s_list[idx];
     const int i1 = e / Y1, j1 = e % Y1;  // region-1 coordinates
     const int i = i1 + 1, j = j1 + 1;    // region-2 coordinates
-    float ph[N], gf[N], gb[N], gr[N], gl[N], divphi[N];
-    bool any = false;
+    float ph[N], cx[N], cy[N], divphi[N];
 #pragma unroll
     for (int a = 0; a < N; a++) {
       ph[a] = PH(a, i, j);
-      gf[a] = (PH(a, i + 1, j) - ph[a]) * m.dx_inv;
-      gb[a] = (ph[a] - PH(a, i - 1, j)) * m.dx_inv;
-      gr[a] = (PH(a, i, j + 1) - ph[a]) * m.dy_inv;
-      gl[a] = (ph[a] - PH(a, i, j - 1)) * m.dy_inv;
-      divphi[a] = (gf[a] - gb[a]) * m.dx_inv + (gr[a] - gl[a]) * m.dy_inv;
-      any |= (divphi[a] != 0.f);
+      const float gf = (PH(a, i + 1, j) - ph[a]) * m.dx_inv, gb = (ph[a] - PH(a, i - 1, j)) * m.dx_inv;
+      const float gr = (PH(a, i, j + 1) - ph[a]) * m.dy_inv, gl = (ph[a] - PH(a, i, j - 1)) * m.dy_inv;
+      divphi[a] = (gf - gb) * m.dx_inv + (gr - gl) * m.dy_inv;
+      cx[a] = 0.5f * (gf + gb);
+      cy[a] = (PH(a, i, j + 1) - PH(a, i, j - 1)) * m.half_dy_inv;
     }
-    float dp[N];
+    // -dA/dphi_a + div dA/dgrad phi_a, accumulated per phase over pairs (one
+    // copy of the pair code: the loops below are not unrolled, keeping the
+    // register count of the fused kernel low)
+    float gterm[N];
 #pragma unroll
-    for (int a = 0; a < N; a++) dp[a] = 0.f;
-    if (any) {
-      float cx[N], cy[N];
+    for (int a = 0; a < N; a++) gterm[a] = 0.f;
+#pragma unroll 1
+    for (int p = 0; p < Pairs<N>::P; p++) {
+      int a = 0, b = 1;
 #pragma unroll
-      for (int a = 0; a < N; a++) {
-        cx[a] = 0.5f * (gf[a] + gb[a]);
-        cy[a] = (PH(a, i, j + 1) - PH(a, i, j - 1)) * m.half_dy_inv;
+      for (int aa = 0; aa < N; aa++)
+#pragma unroll
+        for (int bb = aa + 1; bb < N; bb++)
+          if (Pairs<N>::index(aa, bb) == p) { a = aa; b = bb; }
+      float pha = 0.f, phb = 0.f, cxa = 0.f, cxb = 0.f, cya = 0.f, cyb = 0.f;
+#pragma unroll
+      for (int aa = 0; aa < N; aa++) {
+        if (aa == a) { pha = ph[aa]; cxa = cx[aa]; cya = cy[aa]; }
+        if (aa == b) { phb = ph[aa]; cxb = cx[aa]; cyb = cy[aa]; }
       }
-      // -dA/dphi_a + div dA/dgrad phi_a, accumulated per phase over pairs
-      float gterm[N];
-#pragma unroll
-      for (int a = 0; a < N; a++) gterm[a] = 0.f;
-#pragma unroll
-      for (int a = 0; a < N; a++)
-#pragma unroll
-        for (int b = a + 1; b < N; b++) {
-          const int p = Pairs<N>::index(a, b);
-          const float g2 = 2.f * m.Gamma[a][b];
-          // divergence part from the four faces around (i, j)
-          const float bxf = sbx[(p * (TX + 3) + i) * (TY + 2) + (j - 1)];
-          const float bxb = sbx[(p * (TX + 3) + i - 1) * (TY + 2) + (j - 1)];
-          const float byr = sby[(p * (TX + 2) + (i - 1)) * (TY + 3) + j];
-          const float byl = sby[(p * (TX + 2) + (i - 1)) * (TY + 3) + j - 1];
-          const float sxa_f = 0.5f * (ph[a] + PH(a, i + 1, j)), sxb_f = 0.5f * (ph[b] + PH(b, i + 1, j));
-          const float sxa_b = 0.5f * (ph[a] + PH(a, i - 1, j)), sxb_b = 0.5f * (ph[b] + PH(b, i - 1, j));
-          const float sya_r = 0.5f * (ph[a] + PH(a, i, j + 1)), syb_r = 0.5f * (ph[b] + PH(b, i, j + 1));
-          const float sya_l = 0.5f * (ph[a] + PH(a, i, j - 1)), syb_l = 0.5f * (ph[b] + PH(b, i, j - 1));
-          const float div_ab = (-bxf * sxb_f + bxb * sxb_b) * m.dx_inv + (-byr * syb_r + byl * syb_l) * m.dy_inv;
-          const float div_ba = (bxf * sxa_f - bxb * sxa_b) * m.dx_inv + (byr * sya_r - byl * sya_l) * m.dy_inv;
-          // dA/dphi part at the centre
-          const float Qx = ph[a] * cx[b] - ph[b] * cx[a];
-          const float Qy = ph[a] * cy[b] - ph[b] * cy[a];
-          float dA_a, dA_b;
-          if (ANISO) {
-            const float q0 = m.R[a][b][0][0] * Qx + m.R[a][b][0][1] * Qy;
-            const float q1 = m.R[a][b][1][0] * Qx + m.R[a][b][1][1] * Qy;
-            float ac, q2, e0, e1;
-            aniso_terms(m.dab[a][b], q0, q1, ac, q2, e0, e1);
-            const float rb0 = m.R[a][b][0][0] * cx[b] + m.R[a][b][0][1] * cy[b];
-            const float rb1 = m.R[a][b][1][0] * cx[b] + m.R[a][b][1][1] * cy[b];
-            const float ra0 = m.R[a][b][0][0] * cx[a] + m.R[a][b][0][1] * cy[a];
-            const float ra1 = m.R[a][b][1][0] * cx[a] + m.R[a][b][1][1] * cy[a];
-            const float ac2 = ac * ac;
-            dA_a = ac2 * (q0 * rb0 + q1 * rb1) + ac * (e0 * rb0 + e1 * rb1);
-            dA_b = -(ac2 * (q0 * ra0 + q1 * ra1) + ac * (e0 * ra0 + e1 * ra1));
-          } else {
-            dA_a = Qx * cx[b] + Qy * cy[b];
-            dA_b = -(Qx * cx[a] + Qy * cy[a]);
-          }
-          gterm[a] += g2 * (div_ab - dA_a);
-          gterm[b] += g2 * (div_ba - dA_b);
-        }
-      // grand potentials of the phases at this cell's mu
-      float mu[K1];
-#pragma unroll
-      for (int k = 0; k < K1; k++) mu[k] = smu[(k * X1 + i1) * Y1 + j1];
-      float psi[N];
-#pragma unroll
-      for (int b = 0; b < N; b++) {
-        float c[K1], s = 0.f;
-#pragma unroll
-        for (int k = 0; k < K1; k++) c[k] = c_mu<K1>(m, mu, b, k);
-#pragma unroll
-        for (int k = 0; k < K1; k++) {
-#pragma unroll
-          for (int l = k; l < K1; l++) s += m.A[b][k][l] * c[k] * c[l];
-          s += (m.B[b][k] - mu[k]) * c[k];
-        }
-        psi[b] = s + m.C[b];
+      const float g2 = 2.f * m.Gamma[a][b];
+      const float bxf = sbx[(p * (TX + 3) + i) * (TY + 2) + (j - 1)];
+      const float bxb = sbx[(p * (TX + 3) + i - 1) * (TY + 2) + (j - 1)];
+      const float byr = sby[(p * (TX + 2) + (i - 1)) * (TY + 3) + j];
+      const float byl = sby[(p * (TX + 2) + (i - 1)) * (TY + 3) + j - 1];
+      const float sxa_f = 0.5f * (pha + PH(a, i + 1, j)), sxb_f = 0.5f * (phb + PH(b, i + 1, j));
+      const float sxa_b = 0.5f * (pha + PH(a, i - 1, j)), sxb_b = 0.5f * (phb + PH(b, i - 1, j));
+      const float sya_r = 0.5f * (pha + PH(a, i, j + 1)), syb_r = 0.5f * (phb + PH(b, i, j + 1));
+      const float sya_l = 0.5f * (pha + PH(a, i, j - 1)), syb_l = 0.5f * (phb + PH(b, i, j - 1));
+      const float div_ab = (-bxf * sxb_f + bxb * sxb_b) * m.dx_inv + (-byr * syb_r + byl * syb_l) * m.dy_inv;
+      const float div_ba = (bxf * sxa_f - bxb * sxa_b) * m.dx_inv + (byr * sya_r - byl * sya_l) * m.dy_inv;
+      // dA/dphi part at the centre
+      const float Qx = pha * cxb - phb * cxa;
+      const float Qy = pha * cyb - phb * cya;
+      float dA_a, dA_b;
+      if (ANISO) {
+        const float q0 = m.R[a][b][0][0] * Qx + m.R[a][b][0][1] * Qy;
+        const float q1 = m.R[a][b][1][0] * Qx + m.R[a][b][1][1] * Qy;
+        float ac, q2, e0, e1;
+        aniso_terms(m.dab[a][b], q0, q1, ac, q2, e0, e1);
+        const float rb0 = m.R[a][b][0][0] * cxb + m.R[a][b][0][1] * cyb;
+        const float rb1 = m.R[a][b][1][0] * cxb + m.R[a][b][1][1] * cyb;
+        const float ra0 = m.R[a][b][0][0] * cxa + m.R[a][b][0][1] * cya;
+        const float ra1 = m.R[a][b][1][0] * cxa + m.R[a][b][1][1] * cya;
+        const float ac2 = ac * ac;
+        dA_a = ac2 * (q0 * rb0 + q1 * rb1) + ac * (e0 * rb0 + e1 * rb1);
+        dA_b = -(ac2 * (q0 * ra0 + q1 * ra1) + ac * (e0 * ra0 + e1 * ra1));
+      } else {
+        dA_a = Qx * cxb + Qy * cyb;
+        dA_b = -(Qx * cxa + Qy * cya);
       }
-      float lambda[N], sum_l = 0.f;
-      int active = 0;
+      const float ta = g2 * (div_ab - dA_a), tb = g2 * (div_ba - dA_b);
 #pragma unroll
-      for (int a = 0; a < N; a++) {
-        lambda[a] = 0.f;
-        if (divphi[a] != 0.f) {
-          // obstacle / well potential (functionW_01.h, functionW_02.h)
-          float w = 0.f;
-#pragma unroll
-          for (int b = 0; b < N; b++) {
-            if (b == a || divphi[b] == 0.f) continue;
-            if (m.obstacle) w += (ph[a] * ph[b] >= 0.f ? m.Gamma[a][b] : -m.Gamma[a][b]) * ph[b];
-            else w += 2.f * m.Gamma[a][b] * ph[b] * ph[b] * ph[a];
-          }
-          w *= m.obstacle ? m.w_obst : 9.f;
-#pragma unroll
-          for (int b = 0; b < N; b++)
-#pragma unroll
-            for (int c = b + 1; c < N; c++) {
-              if (b == a || c == a || divphi[b] == 0.f || divphi[c] == 0.f) continue;
-              const float pbc = ph[b] * ph[c];
-              w += (ph[a] * pbc >= 0.f ? m.Gabc[a][b][c] : -m.Gabc[a][b][c]) * pbc;
-            }
-          float dpsi = 0.f;
-#pragma unroll
-          for (int b = 0; b < N; b++) dpsi += psi[b] * dhphi<N>(ph, b, a);
-          lambda[a] = m.eps * gterm[a] - m.inv_eps * w - dpsi;
-          sum_l += lambda[a];
-          active++;
-        }
+      for (int aa = 0; aa < N; aa++) {
+        if (aa == a) gterm[aa] += ta;
+        if (aa == b) gterm[aa] += tb;
       }
-      sum_l /= (float)active;
-      float st = 0.f, st1 = 0.f;
+    }
+    // grand potentials of the phases at this cell's mu
+    float mu[K1];
 #pragma unroll
-      for (int a = 0; a < N; a++)
+    for (int k = 0; k < K1; k++) mu[k] = MU(k, i1, j1);
+    float psi[N];
 #pragma unroll
-        for (int b = a + 1; b < N; b++) {
-          const float pp = ph[a] * ph[b];
-          st += m.tau_ab[a][b] * pp;
-          st1 += pp;
-        }
-      const float tphi = st1 != 0.f ? st / st1 : m.tau;
-      const float f = m.dt / (tphi * m.eps);
+    for (int b = 0; b < N; b++) {
+      float c[K1], sv = 0.f;
 #pragma unroll
-      for (int a = 0; a < N; a++)
-        if (divphi[a] != 0.f) dp[a] = f * (lambda[a] - sum_l);
-      // projection onto the Gibbs simplex (simplex_projection.h:1-49)
-      float over = 0.f, sum_in = 0.f;
-      int count = 0;
+      for (int k = 0; k < K1; k++) c[k] = c_mu<K1>(m, mu, b, k);
 #pragma unroll
-      for (int a = 0; a < N; a++) {
-        const float v = ph[a] + dp[a];
-        if (divphi[a] != 0.f && v > 0.f && v < 1.f) {
-          count++;
-          sum_in += ph[a];
-        }
+      for (int k = 0; k < K1; k++) {
+#pragma unroll
+        for (int l = k; l < K1; l++) sv += m.A[b][k][l] * c[k] * c[l];
+        sv += (m.B[b][k] - mu[k]) * c[k];
       }
+      psi[b] = sv + m.C[b];
+    }
+    float lambda[N], dp[N], sum_l = 0.f;
+    int active = 0;
 #pragma unroll
-      for (int a = 0; a < N; a++) {
-        const float v = ph[a] + dp[a];
-        if (v < 0.f) {
-          dp[a] -= v;
-          over -= v;
-        }
-      }
-      if (over > 0.f) {
+    for (int a = 0; a < N; a++) {
+      lambda[a] = 0.f;
+      dp[a] = 0.f;
+      if (divphi[a] != 0.f) {
+        // obstacle / well potential (functionW_01.h, functionW_02.h)
+        float w = 0.f;
 #pragma unroll
         for (int b = 0; b < N; b++) {
-          const float v = ph[b] + dp[b];
-          if (divphi[b] != 0.f && v > 0.f && v < 1.f)
-            dp[b] -= sum_in != 0.f ? over * ph[b] / sum_in : over / (float)count;
+          if (b == a || divphi[b] == 0.f) continue;
+          if (m.obstacle) w += (ph[a] * ph[b] >= 0.f ? m.Gamma[a][b] : -m.Gamma[a][b]) * ph[b];
+          else w += 2.f * m.Gamma[a][b] * ph[b] * ph[b] * ph[a];
         }
+        w *= m.obstacle ? m.w_obst : 9.f;
+#pragma unroll
+        for (int b = 0; b < N; b++)
+#pragma unroll
+          for (int c = b + 1; c < N; c++) {
+            if (b == a || c == a || divphi[b] == 0.f || divphi[c] == 0.f) continue;
+            const float pbc = ph[b] * ph[c];
+            w += (ph[a] * pbc >= 0.f ? m.Gabc[a][b][c] : -m.Gabc[a][b][c]) * pbc;
+          }
+        float dpsi = 0.f;
+#pragma unroll
+        for (int b = 0; b < N; b++) dpsi += psi[b] * dhphi<N>(ph, b, a);
+        lambda[a] = m.eps * gterm[a] - m.inv_eps * w - dpsi;
+        sum_l += lambda[a];
+        active++;
       }
-      int hit = -1;
+    }
+    sum_l /= (float)active;
+    float st = 0.f, st1 = 0.f;
+#pragma unroll
+    for (int a = 0; a < N; a++)
+#pragma unroll
+      for (int b = a + 1; b < N; b++) {
+        const float pp = ph[a] * ph[b];
+        st += m.tau_ab[a][b] * pp;
+        st1 += pp;
+      }
+    const float tphi = st1 != 0.f ? st / st1 : m.tau;
+    const float f = m.dt / (tphi * m.eps);
+#pragma unroll
+    for (int a = 0; a < N; a++)
+      if (divphi[a] != 0.f) dp[a] = f * (lambda[a] - sum_l);
+    // projection onto the Gibbs simplex (simplex_projection.h:1-49)
+    float over = 0.f, sum_in = 0.f;
+    int count = 0;
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      const float v = ph[a] + dp[a];
+      if (divphi[a] != 0.f && v > 0.f && v < 1.f) {
+        count++;
+        sum_in += ph[a];
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      const float v = ph[a] + dp[a];
+      if (v < 0.f) {
+        dp[a] -= v;
+        over -= v;
+      }
+    }
+    if (over > 0.f) {
+#pragma unroll
+      for (int b = 0; b < N; b++) {
+        const float v = ph[b] + dp[b];
+        if (divphi[b] != 0.f && v > 0.f && v < 1.f) dp[b] -= sum_in != 0.f ? over * ph[b] / sum_in : over / (float)count;
+      }
+    }
+    int hit = -1;
+#pragma unroll
+    for (int a = 0; a < N; a++)
+      if (hit < 0 && divphi[a] != 0.f && ph[a] + dp[a] > 1.f) hit = a;
+    if (hit >= 0) {
 #pragma unroll
       for (int a = 0; a < N; a++)
-        if (hit < 0 && divphi[a] != 0.f && ph[a] + dp[a] > 1.f) hit = a;
-      if (hit >= 0) {
-#pragma unroll
-        for (int a = 0; a < N; a++)
-          if (divphi[a] != 0.f) dp[a] = (a == hit) ? 1.f - ph[a] : -ph[a];
-      }
+        if (divphi[a] != 0.f) dp[a] = (a == hit) ? 1.f - ph[a] : -ph[a];
     }
 #pragma unroll
     for (int a = 0; a < N; a++) sdp[(a * X1 + i1) * Y1 + j1] = dp[a];
   }
-  }  // !pure
   __syncthreads();
 
-  // ---- face fluxes of the mu update: dt * D grad mu - jscale * j_at
-  // (calculate_gradients.h:132-185, calculate_fluxes_concentration.h:4-145)
-  auto face_flux = [&](int ic, int jc, int in, int jn, bool xface, bool skip_at, float* out) {
-    // ic, jc / in, jn: region-1 coordinates of the two cells (n = +x or +y neighbour)
-    float pc[N], pn[N], tc[N], tn[N], gn[N];
+  // ---- face flux of the mu update: dt * D grad mu - jscale * j_at through the
+  // face between region-1 cells c and its +x / +y neighbour n
+  // (calculate_gradients.h:132-185, calculate_fluxes_concentration.h:4-145).
+  // Both cells of a face evaluate it with the same code and inputs.
+  auto face_flux = [&](int ic, int jc, bool xface, bool skip_at, float* out) {
+    const int in = xface ? ic + 1 : ic, jn = xface ? jc : jc + 1;
+    float pc[N], pn[N];
 #pragma unroll
     for (int a = 0; a < N; a++) {
       pc[a] = PH(a, ic + 1, jc + 1);
       pn[a] = PH(a, in + 1, jn + 1);
+    }
+    float muc[K1], mun[K1];
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      muc[k] = MU(k, ic, jc);
+      mun[k] = MU(k, in, jn);
+    }
+    float Dc[MK][MK], Dn[MK][MK];
+    mobility<N, K1>(m, pc, Dc);
+    mobility<N, K1>(m, pn, Dn);
+    diff_flux<K1>(m, Dc, Dn, muc, mun, xface ? m.dx_inv : m.dy_inv, out);
+    if (skip_at) return;
+    float tc[N], tn[N], gn[N];
+    bool any = false;
+#pragma unroll
+    for (int a = 0; a < N; a++) {
       gn[a] = (pn[a] - pc[a]) * (xface ? m.dx_inv : m.dy_inv);
       if (xface) {  // tangential: centred y gradient of each cell
         tc[a] = (PH(a, ic + 1, jc + 2) - PH(a, ic + 1, jc)) * m.half_dy_inv;
@@ -493,207 +686,173 @@ __global__ void __launch_bounds__(256) k_step32(const Inst* __restrict__ insts, 
         tc[a] = 0.5f * (PH(a, ic + 2, jc + 1) - PH(a, ic, jc + 1)) * m.dx_inv;
         tn[a] = 0.5f * (PH(a, in + 2, jn + 1) - PH(a, in, jn + 1)) * m.dx_inv;
       }
+      any |= (gn[a] != 0.f) | (tc[a] != 0.f) | (tn[a] != 0.f);
     }
-    float muc[K1], mun[K1];
+    if (!any) return;
+    const float tl = 0.5f * (tc[L] + tn[L]);
+    const float norm_l = sqrtf(tl * tl + gn[L] * gn[L]);
 #pragma unroll
-    for (int k = 0; k < K1; k++) {
-      muc[k] = smu[(k * X1 + ic) * Y1 + jc];
-      mun[k] = smu[(k * X1 + in) * Y1 + jn];
-    }
-    // diffusion: face mobility (D(c) + D(n))/2 with D = sum_b DC_b phi_b (functionD.h)
-    const float h = xface ? m.dx_inv : m.dy_inv;
-#pragma unroll
-    for (int k = 0; k < K1; k++) {
-      float jd = 0.f;
-#pragma unroll
-      for (int l = 0; l < K1; l++) {
-        float dcs = 0.f, dns = 0.f;
-#pragma unroll
-        for (int b = 0; b < N; b++) {
-          dcs += m.DC[b][k][l] * pc[b];
-          dns += m.DC[b][k][l] * pn[b];
-        }
-        jd += 0.5f * (dcs + dns) * (mun[l] - muc[l]) * h;
+    for (int a = 0; a < N - 1; a++) {
+      const float ta = 0.5f * (tc[a] + tn[a]);
+      const float n2 = ta * ta + gn[a] * gn[a];
+      if (n2 == 0.f) continue;
+      const float rn = rsqrtf(n2);
+      float sp = gn[a] * gn[L] + ta * tl;
+      if (norm_l > 0.f) sp *= rn / norm_l;
+      float sc = 1.f, sn = 1.f;
+      if (m.obstacle) {
+        const float uc = pc[a] * (1.f - pc[a]), un = pn[a] * (1.f - pn[a]);
+        sc = uc > 0.f ? pc[a] * (1.f - hphi<N>(pc, a)) * rsqrtf(uc) : 0.f;
+        sn = un > 0.f ? pn[a] * (1.f - hphi<N>(pn, a)) * rsqrtf(un) : 0.f;
       }
-      out[k] = m.dt * jd;
-    }
-    // antitrapping current
-    if (!skip_at && !pure) {
-      const float tl = 0.5f * (tc[L] + tn[L]);
-      const float norm_l = sqrtf(tl * tl + gn[L] * gn[L]);
+      const float dpc = sdp[(a * X1 + ic) * Y1 + jc], dpn = sdp[(a * X1 + in) * Y1 + jn];
+      const float pref = fabsf(sp) * (m.obstacle ? 0.5f : m.s_well) * gn[a] * rn;
 #pragma unroll
-      for (int a = 0; a < N - 1; a++) {
-        const float ta = 0.5f * (tc[a] + tn[a]);
-        const float n2 = ta * ta + gn[a] * gn[a];
-        if (n2 == 0.f) continue;
-        const float rn = rsqrtf(n2);
-        float sp = gn[a] * gn[L] + ta * tl;
-        if (norm_l > 0.f) sp *= rn / norm_l;
-        float sc = 1.f, sn = 1.f;
-        if (m.obstacle) {
-          const float uc = pc[a] * (1.f - pc[a]), un = pn[a] * (1.f - pn[a]);
-          sc = uc > 0.f ? pc[a] * (1.f - hphi<N>(pc, a)) * rsqrtf(uc) : 0.f;
-          sn = un > 0.f ? pn[a] * (1.f - hphi<N>(pn, a)) * rsqrtf(un) : 0.f;
-        }
-        const float dpc = sdp[(a * X1 + ic) * Y1 + jc], dpn = sdp[(a * X1 + in) * Y1 + jn];
-        const float pref = fabsf(sp) * (m.obstacle ? 0.5f : m.s_well) * gn[a] * rn;
-#pragma unroll
-        for (int k = 0; k < K1; k++) {
-          const float dcn = c_mu<K1>(m, mun, L, k) - c_mu<K1>(m, mun, a, k);
-          const float dcc = c_mu<K1>(m, muc, L, k) - c_mu<K1>(m, muc, a, k);
-          const float j = m.atf[a][k] * pref * (sn * dcn * dpn + sc * dcc * dpc);
-          out[k] -= m.jscale * j;
-        }
+      for (int k = 0; k < K1; k++) {
+        const float dcn = c_mu<K1>(m, mun, L, k) - c_mu<K1>(m, mun, a, k);
+        const float dcc = c_mu<K1>(m, muc, L, k) - c_mu<K1>(m, muc, a, k);
+        const float jt = m.atf[a][k] * pref * (sn * dcn * dpn + sc * dcc * dpc);
+        out[k] = __fsub_rn(out[k], __fmul_rn(m.jscale, jt));
       }
     }
   };
+
   // x-faces between region-1 rows i and i+1, i in [0, TX], tile columns
   for (int e = threadIdx.x; e < (TX + 1) * TY; e += nt) {
     const int i = e / TY, j = 1 + e % TY;
     float f[K1];
-    face_flux(i, j, i + 1, j, true, false, f);
+    face_flux(i, j, true, false, f);
 #pragma unroll
     for (int k = 0; k < K1; k++) sfx[(k * (TX + 1) + i) * TY + (j - 1)] = f[k];
   }
   // y-faces between region-1 columns j and j+1, j in [0, TY], tile rows; the face whose
   // lower cell sits on interior row mesh_y-5 (gidy == MESH_Y-2) carries no antitrapping
+  // current (calculate_fluxes_concentration.h:65)
   for (int e = threadIdx.x; e < TX * (TY + 1); e += nt) {
     const int i = 1 + e / (TY + 1), j = e % (TY + 1);
-    const int gy = y0 - 1 + j;  // interior row of the lower cell
     float f[K1];
-    face_flux(i, j, i, j + 1, false, gy == m.skip_row, f);
+    face_flux(i, j, false, y0 - 1 + j == m.skip_row, f);
 #pragma unroll
     for (int k = 0; k < K1; k++) sfy[(k * TX + (i - 1)) * (TY + 1) + j] = f[k];
   }
   __syncthreads();
 
   // ---- mu and phi update of the tile (calculate_divergence_concentration.h:4-153)
-  for (int e = threadIdx.x; e < TX * TY; e += nt) {
-    const int ti = e / TY, tj = e % TY;
-    const int x = x0 + ti, y = y0 + tj;
-    if (x >= mx || y >= my) continue;
-    const int i1 = ti + 1, j1 = tj + 1;
-    float ph[N], dp[N], mu[K1], dc[K1];
+  for (int ti = warp; ti < TX; ti += nw) {
+    const int x = x0 + ti;
+    if (x >= mx) break;
 #pragma unroll
-    for (int a = 0; a < N; a++) {
-      ph[a] = PH(a, i1 + 1, j1 + 1);
-      dp[a] = sdp[(a * X1 + i1) * Y1 + j1];
-    }
-#pragma unroll
-    for (int k = 0; k < K1; k++) {
-      mu[k] = smu[(k * X1 + i1) * Y1 + j1];
-      dc[k] = (sfx[(k * (TX + 1) + ti + 1) * TY + tj] - sfx[(k * (TX + 1) + ti) * TY + tj]) * m.dx_inv +
-              (sfy[(k * TX + ti) * (TY + 1) + tj + 1] - sfy[(k * TX + ti) * (TY + 1) + tj]) * m.dy_inv;
-    }
-    int bulk = -1;
-#pragma unroll
-    for (int a = 0; a < N; a++)
-      if (bulk < 0 && ph[a] == 1.f) bulk = a;
-    float mnew[K1];
-    if (bulk >= 0) {
-      // c -> c + dc in the bulk phase, mu = dF/dc there (functionF_01.h:19-29)
-      float c[K1];
-#pragma unroll
-      for (int a = 0; a < N; a++)
-        if (a == bulk) {
-#pragma unroll
-          for (int k = 0; k < K1; k++) c[k] = c_mu<K1>(m, mu, a, k) + dc[k];
-#pragma unroll
-          for (int k = 0; k < K1; k++) {
-            float s = 2.f * m.A[a][k][k] * c[k] + m.Beff[a][k];
-#pragma unroll
-            for (int l = 0; l < K1; l++)
-              if (l != k) s += m.A[a][k][l] * c[l];
-            mnew[k] = s;
-          }
-        }
-    } else {
-      float hh[N];
-#pragma unroll
-      for (int a = 0; a < N; a++) hh[a] = hphi<N>(ph, a);
-      // dc -= sum_a c_a(mu) * dh_a/dt
+    for (int c0 = 0; c0 < TY; c0 += 32) {
+      const int tj = c0 + lane, y = y0 + tj;
+      if (y >= my) continue;
+      const int i1 = ti + 1, j1 = tj + 1;
+      float ph[N], dp[N], mu[K1], dc[K1];
 #pragma unroll
       for (int a = 0; a < N; a++) {
-        float sdh = 0.f;
-#pragma unroll
-        for (int b = 0; b < N; b++) sdh += dhphi<N>(ph, a, b) * dp[b];
-#pragma unroll
-        for (int k = 0; k < K1; k++) dc[k] -= c_mu<K1>(m, mu, a, k) * sdh;
+        ph[a] = PH(a, i1 + 1, j1 + 1);
+        dp[a] = sdp[(a * X1 + i1) * Y1 + j1];
       }
-      if (K1 == 1) {
-        float d = 0.f;
 #pragma unroll
-        for (int a = 0; a < N; a++) d += m.cmu[a][0][0] * hh[a];
-        mnew[0] = mu[0] + dc[0] / d;
+      for (int k = 0; k < K1; k++) {
+        mu[k] = MU(k, i1, j1);
+        dc[k] = flux_div(m, sfx[(k * (TX + 1) + ti + 1) * TY + tj], sfx[(k * (TX + 1) + ti) * TY + tj],
+                         sfy[(k * TX + ti) * (TY + 1) + tj + 1], sfy[(k * TX + ti) * (TY + 1) + tj]);
+      }
+      int bulk = -1;
+#pragma unroll
+      for (int a = 0; a < N; a++)
+        if (bulk < 0 && ph[a] == 1.f) bulk = a;
+      float mnew[K1];
+      if (bulk >= 0) {
+        bulk_update<N, K1>(m, bulk, mu, dc, mnew);
       } else {
-        // (dc/dmu) = sum_a cmu_a h_a, inverted in FP64
-        double D[MK][MK];
+        float hh[N];
 #pragma unroll
-        for (int k = 0; k < K1; k++)
+        for (int a = 0; a < N; a++) hh[a] = hphi<N>(ph, a);
+        // dc -= sum_a c_a(mu) * dh_a/dt
 #pragma unroll
-          for (int l = 0; l < K1; l++) {
-            double s = 0.0;
+        for (int a = 0; a < N; a++) {
+          float sdh = 0.f;
 #pragma unroll
-            for (int a = 0; a < N; a++) s += m.cmu_d[a][k][l] * (double)hh[a];
-            D[k][l] = s;
-          }
-        double dm[K1];
-        if (m.mu_solver == GP_MU_BINARY) {  // BINARY = 1 updates the first potential only
+          for (int b = 0; b < N; b++) sdh += dhphi<N>(ph, a, b) * dp[b];
 #pragma unroll
-          for (int k = 0; k < K1; k++) dm[k] = k == 0 ? (double)dc[0] / D[0][0] : 0.0;
-        } else if (m.mu_solver == GP_MU_DILUTE) {
-#pragma unroll
-          for (int k = 0; k < K1; k++) dm[k] = (double)dc[k] / D[k][k];
-        } else if (K1 == 2) {
-          const double det = D[0][0] * D[K1 - 1][K1 - 1] - D[0][K1 - 1] * D[K1 - 1][0];
-          dm[0] = (D[K1 - 1][K1 - 1] * dc[0] - D[0][K1 - 1] * dc[K1 - 1]) / det;
-          dm[K1 - 1] = (D[0][0] * dc[K1 - 1] - D[K1 - 1][0] * dc[0]) / det;
-        } else {
-          // Gauss-Jordan with partial pivoting, K1 <= 3
-          double Aug[MK][MK + 1];
-#pragma unroll
-          for (int k = 0; k < K1; k++) {
-#pragma unroll
-            for (int l = 0; l < K1; l++) Aug[k][l] = D[k][l];
-            Aug[k][K1] = dc[k];
-          }
-#pragma unroll
-          for (int c = 0; c < K1; c++) {
-            int piv = c;
-#pragma unroll
-            for (int r = c + 1; r < K1; r++)
-              if (fabs(Aug[r][c]) > fabs(Aug[piv][c])) piv = r;
-#pragma unroll
-            for (int r = 0; r < K1; r++)
-              if (r == piv && piv != c) {
-#pragma unroll
-                for (int l = 0; l <= K1; l++) {
-                  const double t = Aug[c][l];
-                  Aug[c][l] = Aug[r][l];
-                  Aug[r][l] = t;
-                }
-              }
-            const double inv = 1.0 / Aug[c][c];
-#pragma unroll
-            for (int r = 0; r < K1; r++) {
-              if (r == c) continue;
-              const double f = Aug[r][c] * inv;
-#pragma unroll
-              for (int l = 0; l <= K1; l++) Aug[r][l] -= f * Aug[c][l];
-            }
-          }
-#pragma unroll
-          for (int k = 0; k < K1; k++) dm[k] = Aug[k][K1] / Aug[k][k];
+          for (int k = 0; k < K1; k++) dc[k] -= c_mu<K1>(m, mu, a, k) * sdh;
         }
+        if (K1 == 1) {
+          float d = 0.f;
 #pragma unroll
-        for (int k = 0; k < K1; k++) mnew[k] = mu[k] + (float)dm[k];
+          for (int a = 0; a < N; a++) d += m.cmu[a][0][0] * hh[a];
+          mnew[0] = mu[0] + dc[0] / d;
+        } else {
+          // (dc/dmu) = sum_a cmu_a h_a, inverted in FP64
+          double D[MK][MK];
+#pragma unroll
+          for (int k = 0; k < K1; k++)
+#pragma unroll
+            for (int l = 0; l < K1; l++) {
+              double sv = 0.0;
+#pragma unroll
+              for (int a = 0; a < N; a++) sv += m.cmu_d[a][k][l] * (double)hh[a];
+              D[k][l] = sv;
+            }
+          double dm[K1];
+          if (m.mu_solver == GP_MU_BINARY) {  // BINARY = 1 updates the first potential only
+#pragma unroll
+            for (int k = 0; k < K1; k++) dm[k] = k == 0 ? (double)dc[0] / D[0][0] : 0.0;
+          } else if (m.mu_solver == GP_MU_DILUTE) {
+#pragma unroll
+            for (int k = 0; k < K1; k++) dm[k] = (double)dc[k] / D[k][k];
+          } else if (K1 == 2) {
+            const double det = D[0][0] * D[K1 - 1][K1 - 1] - D[0][K1 - 1] * D[K1 - 1][0];
+            dm[0] = (D[K1 - 1][K1 - 1] * dc[0] - D[0][K1 - 1] * dc[K1 - 1]) / det;
+            dm[K1 - 1] = (D[0][0] * dc[K1 - 1] - D[K1 - 1][0] * dc[0]) / det;
+          } else {
+            // Gauss-Jordan with partial pivoting, K1 <= 3
+            double Aug[MK][MK + 1];
+#pragma unroll
+            for (int k = 0; k < K1; k++) {
+#pragma unroll
+              for (int l = 0; l < K1; l++) Aug[k][l] = D[k][l];
+              Aug[k][K1] = dc[k];
+            }
+#pragma unroll
+            for (int c = 0; c < K1; c++) {
+              int piv = c;
+#pragma unroll
+              for (int r = c + 1; r < K1; r++)
+                if (fabs(Aug[r][c]) > fabs(Aug[piv][c])) piv = r;
+#pragma unroll
+              for (int r = 0; r < K1; r++)
+                if (r == piv && piv != c) {
+#pragma unroll
+                  for (int l = 0; l <= K1; l++) {
+                    const double t = Aug[c][l];
+                    Aug[c][l] = Aug[r][l];
+                    Aug[r][l] = t;
+                  }
+                }
+              const double inv = 1.0 / Aug[c][c];
+#pragma unroll
+              for (int r = 0; r < K1; r++) {
+                if (r == c) continue;
+                const double f = Aug[r][c] * inv;
+#pragma unroll
+                for (int l = 0; l <= K1; l++) Aug[r][l] -= f * Aug[c][l];
+              }
+            }
+#pragma unroll
+            for (int k = 0; k < K1; k++) dm[k] = Aug[k][K1] / Aug[k][k];
+          }
+#pragma unroll
+          for (int k = 0; k < K1; k++) mnew[k] = mu[k] + (float)dm[k];
+        }
       }
+      const int64_t o = (int64_t)x * I.pitch + y;
+#pragma unroll
+      for (int k = 0; k < K1; k++) I.mu_out[o + k * I.plane] = mnew[k];
+#pragma unroll
+      for (int a = 0; a < N; a++) I.phi_out[o + a * I.plane] = __fadd_rn(ph[a], dp[a]);
     }
-    const int64_t o = (int64_t)x * I.pitch + y;
-#pragma unroll
-    for (int k = 0; k < K1; k++) I.mu_out[o + k * I.plane] = mnew[k];
-#pragma unroll
-    for (int a = 0; a < N; a++) I.phi_out[o + a * I.plane] = ph[a] + dp[a];
   }
 }
 
