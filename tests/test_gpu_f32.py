@@ -152,3 +152,16 @@ def test_autotune_restores_state_and_caches(tmp_path):
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
         assert os.path.exists(cache) and len(open(cache).read().split()) == 8
         assert b.autotune(cache) == (tx, ty)  # read back from the cache
+
+
+def test_tip_velocity_within_half_percent_of_fp64():
+    """The north-star bar on a reduced corner dendrite (256^2, 8,000 steps): the
+    FP32 form's tip velocity within 0.5% of the FP64 form's, solute mass within
+    1e-4 (the full 1024^2 x 50,000-step run: python -m microsim_b200.validate)."""
+    from microsim_b200 import validate
+    r = validate.compare(mesh=256, steps=8000, every=500)
+    assert r["nonfinite"] == 0
+    assert r["tip_velocity_fp64"] > 0
+    assert r["tip_velocity_rel_err"] <= 5e-3
+    assert r["tip_position_rel_err"] <= 1e-3
+    assert r["solute_rel_diff"] <= 1e-4
