@@ -108,6 +108,7 @@ _SIGS = {
     "gp_batch_sync": (C.c_int, [C.c_void_p]),
     "gp_batch_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(GpStats)]),
     "gp_batch_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "gp_batch_set_narrowband": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "gp_batch_stream": (C.c_void_p, [C.c_void_p]),
     "gp_batch_launch_count": (C.c_int64, [C.c_void_p]),
@@ -329,6 +330,9 @@ class Batch:
 
     def set_tile(self, tx: int, ty: int):
         _check("gp_batch_set_tile", lib().gp_batch_set_tile(self._h, tx, ty))
+
+    def set_narrowband(self, on: bool):
+        _check("gp_batch_set_narrowband", lib().gp_batch_set_narrowband(self._h, 1 if on else 0))
 
     def autotune(self, cache_path: str | None = None):
         tx, ty = C.c_int(), C.c_int()

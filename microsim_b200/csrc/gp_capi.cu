@@ -28,6 +28,9 @@ void gp_f32_batch_bind(gp_f32_batch* b, int i, float* phiA, float* muA, float* p
 cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty);
 int gp_f32_batch_tiles(const gp_f32_batch* b);
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s);
+cudaError_t gp_f32_batch_invalidate(gp_f32_batch* b, cudaStream_t s);
+void gp_f32_batch_set_narrowband(gp_f32_batch* b, int on);
+int gp_f32_batch_launches_per_step(const gp_f32_batch* b);
 int gp_f32_tile_shape_count();
 void gp_f32_tile_shape(int i, int* tx, int* ty);
 
@@ -228,6 +231,7 @@ extern "C" int gp_upload(gp_ctx* c, const double* phi, const double* mu) {
   if (!c || !phi || !mu) return GP_E_ARG;
   int rc = copy_planes(c, phi, c->phi[c->cur], c->m.N, true);
   if (rc == GP_OK) rc = copy_planes(c, mu, c->mu[c->cur], c->m.K1, true);
+  if (rc == GP_OK && c->f32) GP_CUDA(gp_f32_batch_invalidate(c->f32, c->stream));
   if (rc == GP_OK) GP_CUDA(cudaStreamSynchronize(c->stream));
   c->have_prev = 0;
   return rc;
@@ -263,7 +267,7 @@ extern "C" int gp_step(gp_ctx* c, int64_t nsteps) {
       c->launches += 2;
     } else {
       GP_CUDA(gp_f32_batch_launch(c->f32, c->cur, c->stream));
-      c->launches += 1;
+      c->launches += gp_f32_batch_launches_per_step(c->f32);
     }
     c->cur = nxt;
     c->have_prev = 1;
@@ -563,6 +567,7 @@ extern "C" int gp_batch_upload(gp_batch* b, int i, const double* phi, const doub
   if (!b || i < 0 || i >= b->n || !phi || !mu) return GP_E_ARG;
   int rc = batch_copy(b, i, phi, b->models[i].N, true, true);
   if (rc == GP_OK) rc = batch_copy(b, i, mu, b->models[i].K1, false, true);
+  if (rc == GP_OK) GP_CUDA(gp_f32_batch_invalidate(b->f32, b->stream));
   if (rc == GP_OK) GP_CUDA(cudaStreamSynchronize(b->stream));
   b->have_prev = 0;
   return rc;
@@ -606,13 +611,13 @@ extern "C" int gp_batch_step(gp_batch* b, int64_t nsteps) {
       if (rc != GP_OK) return rc;
     }
     GP_CUDA(cudaGraphLaunch(b->graph[b->parity], b->stream));
-    b->launches += b->graph_steps;
+    b->launches += (int64_t)b->graph_steps * gp_f32_batch_launches_per_step(b->f32);
     nsteps -= b->graph_steps;
     b->have_prev = 1;
   }
   for (; nsteps > 0; nsteps--) {
     GP_CUDA(gp_f32_batch_launch(b->f32, b->parity, b->stream));
-    b->launches++;
+    b->launches += gp_f32_batch_launches_per_step(b->f32);
     b->parity ^= 1;
     b->have_prev = 1;
   }
@@ -719,7 +724,7 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
     GP_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
     GP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    b->launches += 13;
+    b->launches += 13 * gp_f32_batch_launches_per_step(b->f32);
     if (ms < best) {
       best = ms;
       best_tx = tx;
@@ -743,6 +748,14 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   }
   if (tx_out) *tx_out = best_tx;
   if (ty_out) *ty_out = best_ty;
+  return GP_OK;
+}
+
+extern "C" int gp_batch_set_narrowband(gp_batch* b, int on) {
+  if (!b) return GP_E_ARG;
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  gp_f32_batch_set_narrowband(b->f32, on);
+  batch_drop_graphs(b);
   return GP_OK;
 }
 

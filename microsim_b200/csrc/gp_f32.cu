@@ -236,9 +236,25 @@ struct Tile {
   static constexpr size_t bytes = total * sizeof(float);
 };
 
+// Tile index -> instance (binary search on tile_begin).
+__device__ __forceinline__ int find_inst(const Inst* __restrict__ insts, int ninst, int tile) {
+  int lo = 0, hi = ninst - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (insts[mid].tile_begin <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Work of one launch: with list == nullptr every block takes tile blockIdx.x;
+// otherwise blocks are persistent and take entries of `list` (cnt[1] entries)
+// from the queue counter cnt[3].  Each tile writes the purity flag of its
+// output (1 + phase when every output cell is that pure phase, 0 otherwise).
 template <int N, int K1, bool ANISO, int TX, int TY>
-__global__ void __launch_bounds__(256) k_step32(const Inst* __restrict__ insts, int ninst,
-                                                const Model* __restrict__ models) {
+__global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 2)) k_step32(const Inst* __restrict__ insts, int ninst,
+                                                const Model* __restrict__ models, const int* __restrict__ list,
+                                                int* __restrict__ cnt, uint8_t* __restrict__ flags_out) {
   using T = Tile<N, K1, ANISO, TX, TY>;
   constexpr int X2 = T::X2, Y2 = T::Y2, X1 = T::X1, Y1 = T::Y1, W = T::W, Q = T::Q;
   constexpr int L = N - 1;
@@ -248,23 +264,31 @@ __global__ void __launch_bounds__(256) k_step32(const Inst* __restrict__ insts, 
   float* sdp = sm + T::o_dphi;
   __shared__ __align__(16) Model sModel;
   __shared__ __align__(16) Inst sInst;
-  __shared__ int s_inst;
+  __shared__ int s_tile, s_model, s_reload, s_outb;
   const int nt = blockDim.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = nt >> 5;
+  if (threadIdx.x == 0) s_model = -1;
 
-  // which instance / tile (binary search on tile_begin)
-  const int tile = blockIdx.x;
+  for (int iter = 0;; iter++) {
   if (threadIdx.x == 0) {
-    int lo = 0, hi = ninst - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (insts[mid].tile_begin <= tile) lo = mid;
-      else hi = mid - 1;
+    int t = -1;
+    if (list) {
+      const int idx = atomicAdd(&cnt[3], 1);
+      if (idx < cnt[1]) t = list[idx];
+    } else if (iter == 0) {
+      t = blockIdx.x;
     }
-    s_inst = lo;
-    sInst = insts[lo];
+    s_tile = t;
+    s_outb = -1;
+    if (t >= 0) {
+      sInst = insts[find_inst(insts, ninst, t)];
+      s_reload = sInst.model != s_model;
+      s_model = sInst.model;
+    }
   }
   __syncthreads();
-  {  // the instance's model constants into shared memory
+  const int tile = s_tile;
+  if (tile < 0) break;
+  if (s_reload) {  // the instance's model constants into shared memory
     const float4* src = reinterpret_cast<const float4*>(models + sInst.model);
     float4* dst = reinterpret_cast<float4*>(&sModel);
     for (int e = threadIdx.x; e < (int)(sizeof(Model) / 16); e += nt) dst[e] = __ldg(src + e);
@@ -369,7 +393,9 @@ __global__ void __launch_bounds__(256) k_step32(const Inst* __restrict__ insts, 
         for (int a = 0; a < N; a++) I.phi_out[o + a * I.plane] = (a == b0) ? 1.f : 0.f;
       }
     }
-    return;
+    __syncthreads();
+    if (threadIdx.x == 0 && flags_out) flags_out[tile] = (uint8_t)(1 + b0);
+    continue;
   }
 
   // ---- tile touches an interface.  Active ring cells (some divphi != 0) are
@@ -738,6 +764,8 @@ __global__ void __launch_bounds__(256) k_step32(const Inst* __restrict__ insts, 
   __syncthreads();
 
   // ---- mu and phi update of the tile (calculate_divergence_concentration.h:4-153)
+  int outb = -1;      // the pure phase of every cell this thread wrote, if any
+  bool outpure = true;
   for (int ti = warp; ti < TX; ti += nw) {
     const int x = x0 + ti;
     if (x >= mx) break;
@@ -850,10 +878,159 @@ __global__ void __launch_bounds__(256) k_step32(const Inst* __restrict__ insts, 
       const int64_t o = (int64_t)x * I.pitch + y;
 #pragma unroll
       for (int k = 0; k < K1; k++) I.mu_out[o + k * I.plane] = mnew[k];
+      int hot = -1;
+      bool onehot = true;
 #pragma unroll
-      for (int a = 0; a < N; a++) I.phi_out[o + a * I.plane] = __fadd_rn(ph[a], dp[a]);
+      for (int a = 0; a < N; a++) {
+        const float v = __fadd_rn(ph[a], dp[a]);
+        I.phi_out[o + a * I.plane] = v;
+        if (v == 1.f && hot < 0) hot = a;
+        else if (__float_as_uint(v) != 0u) onehot = false;  // -0 is not the pure field's +0
+      }
+      onehot &= hot >= 0;
+      if (!onehot || (outb >= 0 && outb != hot)) outpure = false;
+      else outb = hot;
     }
   }
+  // purity flag of the output tile
+  if (outpure && outb >= 0) atomicCAS(&s_outb, -1, outb);
+  __syncthreads();
+  const bool tile_pure = __syncthreads_and(outpure && (outb < 0 || outb == s_outb)) != 0;
+  if (threadIdx.x == 0 && flags_out) flags_out[tile] = (tile_pure && s_outb >= 0) ? (uint8_t)(1 + s_outb) : 0;
+  }  // tile loop
+}
+
+// Tiles whose staged region is one pure phase b (known from the purity flags of
+// the tile and its eight neighbours): the update is diffusion of mu inside
+// phase b, phi stays the one-hot field of b.  Lean kernel (mu only, no phi read;
+// phi written only when the output buffer does not already hold that field),
+// persistent over the `list` queue (cnt[0] entries, counter cnt[2]).  The mu
+// arithmetic is the shared helpers' -- the same bits as the full kernel.
+template <int N, int K1, int TX, int TY>
+__global__ void __launch_bounds__(256) k_pure32(const Inst* __restrict__ insts, int ninst,
+                                                const Model* __restrict__ models, const int* __restrict__ list,
+                                                int* __restrict__ cnt, uint8_t* __restrict__ flags_out) {
+  constexpr int X1 = TX + 2, W = TY + 8, Q = W / 4;
+  extern __shared__ __align__(16) float smu[];  // [K1][X1][W]
+  __shared__ __align__(16) Inst sInst;
+  __shared__ int s_tile, s_b, s_old;
+  const int nt = blockDim.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = nt >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int idx = atomicAdd(&cnt[2], 1);
+      int t = -1;
+      if (idx < cnt[0]) {
+        const int e = list[idx];
+        t = e & 0xFFFFFF;
+        s_b = e >> 24;
+        sInst = insts[find_inst(insts, ninst, t)];
+        s_old = flags_out[t];
+      }
+      s_tile = t;
+    }
+    __syncthreads();
+    const int tile = s_tile;
+    if (tile < 0) break;
+    const Inst& I = sInst;
+    const Model& m = models[I.model];
+    const int b0 = s_b;
+    const int lt = tile - I.tile_begin;
+    const int x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
+    // interior tile (classification guarantees it): aligned rows y0-4 .. y0+TY+3
+    for (int e = threadIdx.x; e < K1 * X1 * Q; e += nt) {
+      const int k = e / (X1 * Q), r = (e / Q) % X1, q = e % Q;
+      const float4 v = __ldg(reinterpret_cast<const float4*>(I.mu + k * I.plane + (int64_t)(x0 - 1 + r) * I.pitch +
+                                                             (y0 - 4)) + q);
+      reinterpret_cast<float4*>(smu + (k * X1 + r) * W)[q] = v;
+    }
+    __syncthreads();
+    float Db[MK][MK];
+#pragma unroll
+    for (int a = 0; a < N; a++)
+      if (a == b0) {
+#pragma unroll
+        for (int k = 0; k < K1; k++)
+#pragma unroll
+          for (int l = 0; l < K1; l++) Db[k][l] = m.DC[a][k][l];
+      }
+    const bool write_phi = s_old != 1 + b0;
+    auto MU = [&](int k, int i, int j) -> float { return smu[(k * X1 + i) * W + j + 3]; };
+    for (int r = warp; r < TX; r += nw) {
+      const int x = x0 + r;
+#pragma unroll
+      for (int c0 = 0; c0 < TY; c0 += 32) {
+        const int c = c0 + lane, y = y0 + c;
+        const int i1 = r + 1, j1 = c + 1;
+        float mc[K1], mb[K1], mf[K1], ml[K1], mr[K1];
+#pragma unroll
+        for (int k = 0; k < K1; k++) {
+          mc[k] = MU(k, i1, j1);
+          mb[k] = MU(k, i1 - 1, j1);
+          mf[k] = MU(k, i1 + 1, j1);
+          ml[k] = MU(k, i1, j1 - 1);
+          mr[k] = MU(k, i1, j1 + 1);
+        }
+        float fxp[K1], fxm[K1], fyp[K1], fym[K1], dc[K1], mnew[K1];
+        diff_flux<K1>(m, Db, Db, mc, mf, m.dx_inv, fxp);
+        diff_flux<K1>(m, Db, Db, mb, mc, m.dx_inv, fxm);
+        diff_flux<K1>(m, Db, Db, mc, mr, m.dy_inv, fyp);
+        diff_flux<K1>(m, Db, Db, ml, mc, m.dy_inv, fym);
+#pragma unroll
+        for (int k = 0; k < K1; k++) dc[k] = flux_div(m, fxp[k], fxm[k], fyp[k], fym[k]);
+        bulk_update<N, K1>(m, b0, mc, dc, mnew);
+        const int64_t o = (int64_t)x * I.pitch + y;
+#pragma unroll
+        for (int k = 0; k < K1; k++) I.mu_out[o + k * I.plane] = mnew[k];
+        if (write_phi) {
+#pragma unroll
+          for (int a = 0; a < N; a++) I.phi_out[o + a * I.plane] = (a == b0) ? 1.f : 0.f;
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) flags_out[tile] = (uint8_t)(1 + b0);
+  }
+}
+
+// Split the tiles of one step into the pure list (entry: tile | phase << 24)
+// and the list for the full kernel.  A tile is pure when it is an interior tile
+// (its staged region needs no boundary map) and it and its eight neighbours
+// were written as the same pure phase in the previous step.
+template <int TX, int TY>
+__global__ void __launch_bounds__(256) k_classify(const Inst* __restrict__ insts, const int* __restrict__ tile_inst,
+                                                  int total, const uint8_t* __restrict__ flags_in,
+                                                  int* __restrict__ plist, int* __restrict__ glist,
+                                                  int* __restrict__ cnt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  bool pure = false, gen = false;
+  int code = 0;
+  if (t < total) {
+    const Inst& I = insts[tile_inst[t]];
+    const int lt = t - I.tile_begin, tx = lt / I.tiles_y, ty = lt % I.tiles_y;
+    const int x0 = tx * TX, y0 = ty * TY;
+    const uint8_t f = flags_in[t];
+    if (f && x0 >= 2 && x0 + TX + 2 <= I.mx && y0 >= 4 && y0 + TY + 4 <= I.my) {
+      pure = true;
+#pragma unroll
+      for (int dx = -1; dx <= 1; dx++)
+#pragma unroll
+        for (int dy = -1; dy <= 1; dy++) pure &= flags_in[I.tile_begin + (tx + dx) * I.tiles_y + (ty + dy)] == f;
+      code = t | ((int)(f - 1) << 24);
+    }
+    gen = !pure;
+  }
+  const int lane = threadIdx.x & 31;
+  const unsigned bp = __ballot_sync(0xffffffffu, pure), bg = __ballot_sync(0xffffffffu, gen);
+  int basep = 0, baseg = 0;
+  if (lane == 0) {
+    if (bp) basep = atomicAdd(&cnt[0], __popc(bp));
+    if (bg) baseg = atomicAdd(&cnt[1], __popc(bg));
+  }
+  basep = __shfl_sync(0xffffffffu, basep, 0);
+  baseg = __shfl_sync(0xffffffffu, baseg, 0);
+  const unsigned below = (1u << lane) - 1u;
+  if (pure) plist[basep + __popc(bp & below)] = code;
+  if (gen) glist[baseg + __popc(bg & below)] = t;
 }
 
 // ---------------------------------------------------------------- host side
@@ -910,51 +1087,47 @@ Model make_model(const gp_model& g) {
 
 using namespace gp32;
 
-// A batch of FP32 instances on the current device.
-struct gp_f32_batch {
-  int n = 0, N = 0, K1 = 0, aniso = 0;
-  int tx = 16, ty = 32;  // tile shape (autotuned)
-  std::vector<gp_model> gm;
-  std::vector<Inst> hinst[2];  // [buffer parity]
-  Inst* dinst[2] = {nullptr, nullptr};
-  Model* dmodel = nullptr;
-  int total_tiles = 0;
+// Kernels of one (N, K1, anisotropy, tile shape).
+struct KernelSet {
+  void (*general)(const Inst*, int, const Model*, const int*, int*, uint8_t*);
+  void (*pure)(const Inst*, int, const Model*, const int*, int*, uint8_t*);
+  void (*classify)(const Inst*, const int*, int, const uint8_t*, int*, int*, int*);
+  size_t smem_general, smem_pure;
 };
 
-typedef void (*launch_fn)(const Inst*, int, const Model*, int, cudaStream_t);
-
 template <int N, int K1, bool AN, int TX, int TY>
-static void launch_tile(const Inst* inst, int ninst, const Model* models, int tiles, cudaStream_t s) {
-  using T = Tile<N, K1, AN, TX, TY>;
-  static unsigned long long configured = 0;  // one bit per device
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && !(configured & (1ull << dev))) {
-    cudaFuncSetAttribute(k_step32<N, K1, AN, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes);
-    configured |= 1ull << dev;
-  }
-  k_step32<N, K1, AN, TX, TY><<<tiles, 256, T::bytes, s>>>(inst, ninst, models);
+static KernelSet make_set() {
+  KernelSet k;
+  k.general = k_step32<N, K1, AN, TX, TY>;
+  k.pure = k_pure32<N, K1, TX, TY>;
+  k.classify = k_classify<TX, TY>;
+  k.smem_general = Tile<N, K1, AN, TX, TY>::bytes;
+  k.smem_pure = (size_t)K1 * (TX + 2) * (TY + 8) * sizeof(float);
+  return k;
 }
 
 template <int N, int K1, bool AN>
-static launch_fn pick_tile(int tx, int ty) {
-  if (tx == 16 && ty == 32) return launch_tile<N, K1, AN, 16, 32>;
-  if (tx == 8 && ty == 32) return launch_tile<N, K1, AN, 8, 32>;
-  if (tx == 32 && ty == 32) return launch_tile<N, K1, AN, 32, 32>;
-  if (tx == 16 && ty == 64) return launch_tile<N, K1, AN, 16, 64>;
-  return nullptr;
+static bool pick_tile(int tx, int ty, KernelSet* k) {
+  if (tx == 16 && ty == 32) { *k = make_set<N, K1, AN, 16, 32>(); return true; }
+  if (tx == 8 && ty == 32) { *k = make_set<N, K1, AN, 8, 32>(); return true; }
+  if (tx == 32 && ty == 32) { *k = make_set<N, K1, AN, 32, 32>(); return true; }
+  if (tx == 16 && ty == 64) { *k = make_set<N, K1, AN, 16, 64>(); return true; }
+  return false;
 }
 
-static launch_fn pick(int N, int K1, int an, int tx, int ty) {
-#define GP_PICK(NN, KK)                                                                 \
-  if (N == NN && K1 == KK) return an ? pick_tile<NN, KK, true>(tx, ty) : pick_tile<NN, KK, false>(tx, ty);
+static bool pick(int N, int K1, int an, int tx, int ty, KernelSet* k) {
+#define GP_PICK(NN, KK)                                                                        \
+  if (N == NN && K1 == KK) return an ? pick_tile<NN, KK, true>(tx, ty, k) : pick_tile<NN, KK, false>(tx, ty, k);
   GP_PICK(2, 1) GP_PICK(2, 2) GP_PICK(3, 1) GP_PICK(3, 2) GP_PICK(4, 1) GP_PICK(4, 2)
   GP_PICK(2, 3) GP_PICK(3, 3) GP_PICK(4, 3)
 #undef GP_PICK
-  return nullptr;
+  return false;
 }
 
-int gp_f32_supported(const gp_model& m) { return pick(m.N, m.K1, m.anisotropy, 16, 32) != nullptr; }
+int gp_f32_supported(const gp_model& m) {
+  KernelSet k;
+  return pick(m.N, m.K1, m.anisotropy, 16, 32, &k);
+}
 
 // tile shapes offered to the autotuner
 static const int kTileShapes[][2] = {{16, 32}, {8, 32}, {32, 32}, {16, 64}};
@@ -966,14 +1139,45 @@ void gp_f32_tile_shape(int i, int* tx, int* ty) {
   *ty = kTileShapes[i][1];
 }
 
-// Create a batch from n models (same N, K1, anisotropy switch); state buffers
-// are owned by the caller of gp_f32_batch_bind.
+// A batch of FP32 instances on the current device.
+struct gp_f32_batch {
+  int n = 0, N = 0, K1 = 0, aniso = 0;
+  int tx = 16, ty = 32;  // tile shape (autotuned)
+  int narrowband = 1;    // classify tiles and send pure ones to the lean kernel
+  std::vector<gp_model> gm;
+  std::vector<Inst> hinst[2];  // [buffer parity]
+  Inst* dinst[2] = {nullptr, nullptr};
+  Model* dmodel = nullptr;
+  int total_tiles = 0;
+  KernelSet ks;
+  uint8_t* dflags = nullptr;  // [2][total_tiles] purity flags of the state in buffer p
+  int* dplist = nullptr;      // [total_tiles]
+  int* dglist = nullptr;      // [total_tiles]
+  int* dcnt = nullptr;        // [4] pure count, general count, pure queue, general queue
+  int* dtile_inst = nullptr;  // [total_tiles] instance of each tile
+  int grid_general = 0, grid_pure = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+};
+
+void gp_f32_batch_destroy(gp_f32_batch* b);
+
+static void free_tiles(gp_f32_batch* b) {
+  cudaFree(b->dflags);
+  cudaFree(b->dplist);
+  cudaFree(b->dglist);
+  cudaFree(b->dtile_inst);
+  b->dflags = nullptr;
+  b->dplist = b->dglist = b->dtile_inst = nullptr;
+}
+
 cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** out) {
   if (n < 1) return cudaErrorInvalidValue;
   for (int i = 1; i < n; i++)
     if (models[i].N != models[0].N || models[i].K1 != models[0].K1 || models[i].anisotropy != models[0].anisotropy)
       return cudaErrorInvalidValue;
-  if (!pick(models[0].N, models[0].K1, models[0].anisotropy, 16, 32)) return cudaErrorNotSupported;
+  KernelSet ks;
+  if (!pick(models[0].N, models[0].K1, models[0].anisotropy, 16, 32, &ks)) return cudaErrorNotSupported;
   gp_f32_batch* b = new gp_f32_batch();
   b->n = n;
   b->N = models[0].N;
@@ -984,15 +1188,16 @@ cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** ou
   for (int i = 0; i < n; i++) hm[i] = make_model(models[i]);
   cudaError_t e = cudaMalloc(&b->dmodel, sizeof(Model) * n);
   if (e == cudaSuccess) e = cudaMemcpy(b->dmodel, hm.data(), sizeof(Model) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dcnt, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
   for (int p = 0; e == cudaSuccess && p < 2; p++) {
     b->hinst[p].resize(n);
     e = cudaMalloc(&b->dinst[p], sizeof(Inst) * n);
   }
   if (e != cudaSuccess) {
-    cudaFree(b->dmodel);
-    cudaFree(b->dinst[0]);
-    cudaFree(b->dinst[1]);
-    delete b;
+    gp_f32_batch_destroy(b);
     return e;
   }
   *out = b;
@@ -1001,9 +1206,15 @@ cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** ou
 
 void gp_f32_batch_destroy(gp_f32_batch* b) {
   if (!b) return;
+  if (b->side) cudaStreamSynchronize(b->side);
   cudaFree(b->dmodel);
   cudaFree(b->dinst[0]);
   cudaFree(b->dinst[1]);
+  cudaFree(b->dcnt);
+  free_tiles(b);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->ev_join) cudaEventDestroy(b->ev_join);
+  if (b->side) cudaStreamDestroy(b->side);
   delete b;
 }
 
@@ -1025,12 +1236,24 @@ void gp_f32_batch_bind(gp_f32_batch* b, int i, float* phiA, float* muA, float* p
   }
 }
 
+// The purity flags describe the buffers' contents; after the state changes
+// behind the kernels' back (upload, restore) they are reset to "unknown".
+cudaError_t gp_f32_batch_invalidate(gp_f32_batch* b, cudaStream_t s) {
+  if (!b->dflags) return cudaSuccess;
+  return cudaMemsetAsync(b->dflags, 0, 2 * (size_t)b->total_tiles, s);
+}
+
+void gp_f32_batch_set_narrowband(gp_f32_batch* b, int on) { b->narrowband = on ? 1 : 0; }
+
 // Recompute the tile decomposition for shape (tx, ty) and upload the instance tables.
 cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
-  if (!pick(b->N, b->K1, b->aniso, tx, ty)) return cudaErrorInvalidValue;
+  KernelSet ks;
+  if (!pick(b->N, b->K1, b->aniso, tx, ty, &ks)) return cudaErrorInvalidValue;
   b->tx = tx;
   b->ty = ty;
+  b->ks = ks;
   int t = 0;
+  std::vector<int> tile_inst;
   for (int i = 0; i < b->n; i++) {
     const int txs = (int)((b->gm[i].mesh_x + tx - 1) / tx), tys = (int)((b->gm[i].mesh_y + ty - 1) / ty);
     for (int p = 0; p < 2; p++) {
@@ -1038,21 +1261,65 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
       b->hinst[p][i].tile_begin = t;
     }
     t += txs * tys;
+    tile_inst.insert(tile_inst.end(), (size_t)txs * tys, i);
   }
+  if (t >= (1 << 24)) return cudaErrorInvalidValue;  // tile ids share an int with the phase in the pure list
   b->total_tiles = t;
   for (int p = 0; p < 2; p++) {
     cudaError_t e = cudaMemcpy(b->dinst[p], b->hinst[p].data(), sizeof(Inst) * b->n, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return e;
   }
-  return cudaSuccess;
+  free_tiles(b);
+  cudaError_t e = cudaMalloc(&b->dflags, 2 * (size_t)t);
+  if (e == cudaSuccess) e = cudaMemset(b->dflags, 0, 2 * (size_t)t);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dplist, sizeof(int) * t);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dglist, sizeof(int) * t);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dtile_inst, sizeof(int) * t);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->dtile_inst, tile_inst.data(), sizeof(int) * t, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return e;
+  // dynamic shared memory limits and persistent grid sizes
+  int dev = 0, sms = 0, occ_g = 0, occ_p = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaFuncSetAttribute(ks.general, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_general);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(ks.pure, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_pure);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, ks.general, 256, ks.smem_general);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, ks.pure, 256, ks.smem_pure);
+  if (e != cudaSuccess) return e;
+  b->grid_general = sms * (occ_g > 0 ? occ_g : 1);
+  b->grid_pure = sms * (occ_p > 0 ? occ_p : 1);
+  return cudaDeviceSynchronize();  // the flag reset above must land before any stream uses them
 }
 
 int gp_f32_batch_tiles(const gp_f32_batch* b) { return b->total_tiles; }
 
 // One step of every instance, reading buffer parity `parity`.
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
-  launch_fn f = pick(b->N, b->K1, b->aniso, b->tx, b->ty);
-  if (!f) return cudaErrorInvalidValue;
-  f(b->dinst[parity & 1], b->n, b->dmodel, b->total_tiles, s);
-  return cudaGetLastError();
+  const KernelSet& k = b->ks;
+  const int p = parity & 1;
+  uint8_t* flags_in = b->dflags + (size_t)p * b->total_tiles;
+  uint8_t* flags_out = b->dflags + (size_t)(p ^ 1) * b->total_tiles;
+  if (!b->narrowband) {
+    k.general<<<b->total_tiles, 256, k.smem_general, s>>>(b->dinst[p], b->n, b->dmodel, nullptr, nullptr, flags_out);
+    return cudaGetLastError();
+  }
+  cudaError_t e = cudaMemsetAsync(b->dcnt, 0, 4 * sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  k.classify<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dinst[p], b->dtile_inst, b->total_tiles, flags_in,
+                                                          b->dplist, b->dglist, b->dcnt);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // the pure tiles and the rest run concurrently (disjoint tiles and flags)
+  if ((e = cudaEventRecord(b->ev_fork, s)) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess) return e;
+  k.pure<<<b->grid_pure, 256, k.smem_pure, b->side>>>(b->dinst[p], b->n, b->dmodel, b->dplist, b->dcnt, flags_out);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k.general<<<b->grid_general, 256, k.smem_general, s>>>(b->dinst[p], b->n, b->dmodel, b->dglist, b->dcnt,
+                                                         flags_out);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess) return e;
+  return cudaStreamWaitEvent(s, b->ev_join, 0);
 }
+
+// kernel launches one gp_f32_batch_launch issues
+int gp_f32_batch_launches_per_step(const gp_f32_batch* b) { return b->narrowband ? 3 : 1; }
