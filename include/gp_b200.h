@@ -187,10 +187,14 @@ int gp_batch_sync(gp_batch *b);
 int gp_batch_get_stats(gp_batch *b, int i, gp_stats *out);
 /* Tile shape of the fused kernel (tx along x, ty along y): 16x32, 8x32, 32x32, 16x64. */
 int gp_batch_set_tile(gp_batch *b, int tx, int ty);
-/* Narrow band (on by default): each step first sorts tiles into those whose
- * neighbourhood is one pure phase -- updated by a lean diffusion-only kernel --
- * and the rest, run concurrently; the results are bit-identical with it off. */
+/* Narrow band (on by default): tiles whose cells and two-cell ring were one
+ * pure phase after the previous step (per-tile purity words written by every
+ * step) take a lean diffusion-only kernel, the rest the full kernel, both
+ * launched concurrently; the results are bit-identical with it off. */
 int gp_batch_set_narrowband(gp_batch *b, int on);
+/* Tiles the next step sends to the lean kernel, and all tiles of the batch
+ * (diagnostics; synchronises the batch's stream). */
+int gp_batch_lean_tiles(gp_batch *b, int64_t *lean, int64_t *total);
 /* Measured sweep over the tile shapes on the batch's own state (restored
  * afterwards); the winner is cached in cache_path (may be NULL) per batch
  * signature and read back on the next call. */

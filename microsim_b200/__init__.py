@@ -109,6 +109,7 @@ _SIGS = {
     "gp_batch_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(GpStats)]),
     "gp_batch_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gp_batch_set_narrowband": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_batch_lean_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "gp_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "gp_batch_stream": (C.c_void_p, [C.c_void_p]),
     "gp_batch_launch_count": (C.c_int64, [C.c_void_p]),
@@ -333,6 +334,12 @@ class Batch:
 
     def set_narrowband(self, on: bool):
         _check("gp_batch_set_narrowband", lib().gp_batch_set_narrowband(self._h, 1 if on else 0))
+
+    def lean_tiles(self):
+        """(tiles the next step updates with the lean kernel, all tiles)."""
+        lean, total = C.c_int64(), C.c_int64()
+        _check("gp_batch_lean_tiles", lib().gp_batch_lean_tiles(self._h, C.byref(lean), C.byref(total)))
+        return lean.value, total.value
 
     def autotune(self, cache_path: str | None = None):
         tx, ty = C.c_int(), C.c_int()

@@ -29,6 +29,7 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty);
 int gp_f32_batch_tiles(const gp_f32_batch* b);
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s);
 cudaError_t gp_f32_batch_invalidate(gp_f32_batch* b, cudaStream_t s);
+cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s, int64_t* lean);
 void gp_f32_batch_set_narrowband(gp_f32_batch* b, int on);
 int gp_f32_batch_launches_per_step(const gp_f32_batch* b);
 int gp_f32_tile_shape_count();
@@ -756,6 +757,13 @@ extern "C" int gp_batch_set_narrowband(gp_batch* b, int on) {
   GP_CUDA(cudaStreamSynchronize(b->stream));
   gp_f32_batch_set_narrowband(b->f32, on);
   batch_drop_graphs(b);
+  return GP_OK;
+}
+
+extern "C" int gp_batch_lean_tiles(gp_batch* b, int64_t* lean, int64_t* total) {
+  if (!b || !lean || !total) return GP_E_ARG;
+  GP_CUDA(gp_f32_batch_lean_tiles(b->f32, b->parity, b->stream, lean));
+  *total = gp_f32_batch_tiles(b->f32);
   return GP_OK;
 }
 

@@ -66,6 +66,7 @@ struct alignas(16) Inst {
   int tiles_y;     // tiles along y
   int tile_begin;  // first global tile index of this instance
   int model;       // index into the model array
+  int tiles_x;     // tiles along x
   gp_bc bc;
 };
 
@@ -236,25 +237,67 @@ struct Tile {
   static constexpr size_t bytes = total * sizeof(float);
 };
 
-// Tile index -> instance (binary search on tile_begin).
-__device__ __forceinline__ int find_inst(const Inst* __restrict__ insts, int ninst, int tile) {
-  int lo = 0, hi = ninst - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (insts[mid].tile_begin <= tile) lo = mid;
-    else hi = mid - 1;
+// ---------------------------------------------------------------- narrow band
+//
+// Far from every interface a cell's phi is the one-hot field of one phase and
+// its update is diffusion of mu inside that phase.  Each step writes, per tile,
+// a purity word describing its output: five 4-bit fields, each 1 + b when every
+// in-grid cell of that part of the tile holds the one-hot field of phase b
+// (exactly 1.0f and +0.0f), else 0.  The parts: the whole tile, its first and
+// last two rows (x) and its first and last two columns (y).
+enum { PF_CORE = 0, PF_XLO = 4, PF_XHI = 8, PF_YLO = 12, PF_YHI = 16 };
+__host__ __device__ __forceinline__ int pf(uint32_t w, int f) { return (int)((w >> f) & 15u); }
+__host__ __device__ __forceinline__ uint32_t pf_all(int c) { return (uint32_t)c * 0x11111u; }
+
+// Phase b >= 0 when tile t may take the lean update: in the input, the tile
+// and the two-cell ring the full update reads around it (tile +- 2, the phi
+// region it stages) hold the one-hot field of phase b, known from the purity
+// words of the tile and its eight neighbours.  Where the ring leaves the grid
+// it is the Neumann mirror of the tile's own cells (rows 1, 2 and M-2, M-3:
+// the tile needs 3 cells on that axis); a periodic wrap is not trusted.
+// The full update of such a tile is its pure-phase path, so the lean update
+// gives the same bits.  -1 otherwise.
+__host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ F, const Inst& I, int t, int TX,
+                                                   int TY) {
+  const int c = pf(F[t], PF_CORE);
+  if (!c) return -1;
+  const int ny = I.tiles_y, lt = t - I.tile_begin, tx = lt / ny, ty = lt % ny;
+  const int ex = I.mx - tx * TX < TX ? I.mx - tx * TX : TX, ey = I.my - ty * TY < TY ? I.my - ty * TY : TY;
+  const bool xm = tx > 0, xp = tx + 1 < I.tiles_x, ym = ty > 0, yp = ty + 1 < ny;
+  if ((!xm || !xp) && !(I.bc.phi_x == GP_BC_NEUMANN && ex >= 3)) return -1;
+  if ((!ym || !yp) && !(I.bc.phi_y == GP_BC_NEUMANN && ey >= 3)) return -1;
+  if (xm && pf(F[t - ny], PF_XHI) != c) return -1;
+  if (xp && pf(F[t + ny], PF_XLO) != c) return -1;
+  if (ym && pf(F[t - 1], PF_YHI) != c) return -1;
+  if (yp && pf(F[t + 1], PF_YLO) != c) return -1;
+  if (xm && ym) {
+    const uint32_t v = F[t - ny - 1];
+    if (pf(v, PF_XHI) != c && pf(v, PF_YHI) != c) return -1;
   }
-  return lo;
+  if (xm && yp) {
+    const uint32_t v = F[t - ny + 1];
+    if (pf(v, PF_XHI) != c && pf(v, PF_YLO) != c) return -1;
+  }
+  if (xp && ym) {
+    const uint32_t v = F[t + ny - 1];
+    if (pf(v, PF_XLO) != c && pf(v, PF_YHI) != c) return -1;
+  }
+  if (xp && yp) {
+    const uint32_t v = F[t + ny + 1];
+    if (pf(v, PF_XLO) != c && pf(v, PF_YLO) != c) return -1;
+  }
+  return c - 1;
 }
 
-// Work of one launch: with list == nullptr every block takes tile blockIdx.x;
-// otherwise blocks are persistent and take entries of `list` (cnt[1] entries)
-// from the queue counter cnt[3].  Each tile writes the purity flag of its
-// output (1 + phase when every output cell is that pure phase, 0 otherwise).
+// Full update of the tiles.  With glist == nullptr block k takes tile k (grid
+// = all tiles).  Otherwise the blocks are persistent and take the cnt[0]
+// tiles of glist through the queue head cnt[1]; the last block to finish
+// resets the counters (cnt[2] counts finished blocks) for the next step.
+// Every tile writes the purity word of its output.
 template <int N, int K1, bool ANISO, int TX, int TY>
-__global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 2)) k_step32(const Inst* __restrict__ insts, int ninst,
-                                                const Model* __restrict__ models, const int* __restrict__ list,
-                                                int* __restrict__ cnt, uint8_t* __restrict__ flags_out) {
+__global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 2))
+    k_step32(const Inst* __restrict__ insts, const Model* __restrict__ models, const int* __restrict__ tile_inst,
+             const int* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out) {
   using T = Tile<N, K1, ANISO, TX, TY>;
   constexpr int X2 = T::X2, Y2 = T::Y2, X1 = T::X1, Y1 = T::Y1, W = T::W, Q = T::Q;
   constexpr int L = N - 1;
@@ -264,25 +307,27 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
   float* sdp = sm + T::o_dphi;
   __shared__ __align__(16) Model sModel;
   __shared__ __align__(16) Inst sInst;
-  __shared__ int s_tile, s_model, s_reload, s_outb;
+  __shared__ int s_tile, s_model, s_reload;
+  __shared__ unsigned s_bad;
   const int nt = blockDim.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = nt >> 5;
   if (threadIdx.x == 0) s_model = -1;
 
   for (int iter = 0;; iter++) {
+  __syncthreads();  // the previous tile's shared state is no longer read
   if (threadIdx.x == 0) {
     int t = -1;
-    if (list) {
-      const int idx = atomicAdd(&cnt[3], 1);
-      if (idx < cnt[1]) t = list[idx];
+    if (glist) {
+      const int i = atomicAdd(&cnt[1], 1);
+      if (i < cnt[0]) t = glist[i];
     } else if (iter == 0) {
       t = blockIdx.x;
     }
     s_tile = t;
-    s_outb = -1;
     if (t >= 0) {
-      sInst = insts[find_inst(insts, ninst, t)];
+      sInst = insts[tile_inst[t]];
       s_reload = sInst.model != s_model;
       s_model = sInst.model;
+      s_bad = 0u;
     }
   }
   __syncthreads();
@@ -394,7 +439,7 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0 && flags_out) flags_out[tile] = (uint8_t)(1 + b0);
+    if (threadIdx.x == 0) flags_out[tile] = pf_all(1 + b0);
     continue;
   }
 
@@ -764,8 +809,7 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
   __syncthreads();
 
   // ---- mu and phi update of the tile (calculate_divergence_concentration.h:4-153)
-  int outb = -1;      // the pure phase of every cell this thread wrote, if any
-  bool outpure = true;
+  uint8_t* s_cls = reinterpret_cast<uint8_t*>(sm + T::o_list);  // [TX][TY] one-hot phase of the output, or 0xFF
   for (int ti = warp; ti < TX; ti += nw) {
     const int x = x0 + ti;
     if (x >= mx) break;
@@ -887,150 +931,236 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
         if (v == 1.f && hot < 0) hot = a;
         else if (__float_as_uint(v) != 0u) onehot = false;  // -0 is not the pure field's +0
       }
-      onehot &= hot >= 0;
-      if (!onehot || (outb >= 0 && outb != hot)) outpure = false;
-      else outb = hot;
+      s_cls[ti * TY + tj] = (onehot && hot >= 0) ? (uint8_t)hot : (uint8_t)0xFF;
     }
   }
-  // purity flag of the output tile
-  if (outpure && outb >= 0) atomicCAS(&s_outb, -1, outb);
   __syncthreads();
-  const bool tile_pure = __syncthreads_and(outpure && (outb < 0 || outb == s_outb)) != 0;
-  if (threadIdx.x == 0 && flags_out) flags_out[tile] = (tile_pure && s_outb >= 0) ? (uint8_t)(1 + s_outb) : 0;
+  // purity word of the output tile (whole tile, first/last two rows, first/last two columns)
+  {
+    const int ex = min(TX, mx - x0), ey = min(TY, my - y0);
+    const int r0 = s_cls[0], rxh = s_cls[(ex - 1) * TY], ryh = s_cls[ey - 1];
+    unsigned bad = 0u;
+    for (int e = threadIdx.x; e < TX * TY; e += nt) {
+      const int i = e / TY, j = e % TY;
+      if (i >= ex || j >= ey) continue;
+      const int v = s_cls[e];
+      if (v != r0) bad |= (i < 2 ? 3u : 1u) | (j < 2 ? 8u : 0u);
+      if (i >= ex - 2 && v != rxh) bad |= 4u;
+      if (j >= ey - 2 && v != ryh) bad |= 16u;
+    }
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if (lane == 0 && bad) atomicOr(&s_bad, bad);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned B = s_bad;
+      uint32_t w = 0u;
+      if (!(B & 1u) && r0 != 0xFF) w |= (uint32_t)(1 + r0) << PF_CORE;
+      if (!(B & 2u) && r0 != 0xFF) w |= (uint32_t)(1 + r0) << PF_XLO;
+      if (!(B & 4u) && rxh != 0xFF) w |= (uint32_t)(1 + rxh) << PF_XHI;
+      if (!(B & 8u) && r0 != 0xFF) w |= (uint32_t)(1 + r0) << PF_YLO;
+      if (!(B & 16u) && ryh != 0xFF) w |= (uint32_t)(1 + ryh) << PF_YHI;
+      flags_out[tile] = w;
+    }
+  }
   }  // tile loop
+  if (glist && threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&cnt[2], 1) == (int)gridDim.x - 1) {
+      cnt[0] = 0;
+      cnt[1] = 0;
+      cnt[2] = 0;
+    }
+  }
 }
 
-// Tiles whose staged region is one pure phase b (known from the purity flags of
-// the tile and its eight neighbours): the update is diffusion of mu inside
-// phase b, phi stays the one-hot field of b.  Lean kernel (mu only, no phi read;
-// phi written only when the output buffer does not already hold that field),
-// persistent over the `list` queue (cnt[0] entries, counter cnt[2]).  The mu
-// arithmetic is the shared helpers' -- the same bits as the full kernel.
+// Lean update of one tile that lean_phase accepted with phase b: diffusion of
+// mu inside phase b; phi stays the one-hot field of b and is written only when
+// the output buffer does not hold it already (its purity word says so).
+//
+// One warp per tile.  A row of the tile is G = TY/4 lanes of four cells each
+// (float4 loads and stores); the warp's 32/G lane groups take RG consecutive
+// rows each and stream them along x: each x-face flux is evaluated once and
+// carried to the next row, the y-faces between a lane's cells once, the
+// lane-boundary faces from the neighbour lane's cell (shuffle) -- the same
+// helper calls on the same operands as the full update's pure path, hence the
+// same bits.  Rows are loaded RB at a time ahead of their use; rows, halo
+// columns and partial tiles go through the boundary map.
 template <int N, int K1, int TX, int TY>
-__global__ void __launch_bounds__(256) k_pure32(const Inst* __restrict__ insts, int ninst,
-                                                const Model* __restrict__ models, const int* __restrict__ list,
-                                                int* __restrict__ cnt, uint8_t* __restrict__ flags_out) {
-  constexpr int X1 = TX + 2, W = TY + 8, Q = W / 4;
-  extern __shared__ __align__(16) float smu[];  // [K1][X1][W]
-  __shared__ __align__(16) Inst sInst;
-  __shared__ int s_tile, s_b, s_old;
-  const int nt = blockDim.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = nt >> 5;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const int idx = atomicAdd(&cnt[2], 1);
-      int t = -1;
-      if (idx < cnt[0]) {
-        const int e = list[idx];
-        t = e & 0xFFFFFF;
-        s_b = e >> 24;
-        sInst = insts[find_inst(insts, ninst, t)];
-        s_old = flags_out[t];
-      }
-      s_tile = t;
+struct Lean {
+  static constexpr int G = TY / 4;     // lanes per tile row
+  static constexpr int NG = 32 / G;    // row groups per warp
+  static constexpr int RG = TX / NG;   // rows per group
+  static constexpr int RB = RG < 8 / K1 ? RG : 8 / K1;  // rows loaded ahead
+  static_assert(G * NG == 32 && RG * NG == TX, "tile shape");
+};
+
+template <int N, int K1, int TX, int TY>
+__device__ __forceinline__ void lean_tile(const Inst& I, const Model& m, uint32_t* __restrict__ flags_out, int t,
+                                          int b, int lane) {
+  using S = Lean<N, K1, TX, TY>;
+  constexpr int G = S::G, RG = S::RG, RB = S::RB;
+  const int lt = t - I.tile_begin, x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
+  const int mx = I.mx, my = I.my, xend = min(x0 + TX, mx);
+  const int64_t pitch = I.pitch, plane = I.plane;
+  const float* mu = I.mu;
+  const gp_bc bc = I.bc;
+  const int lg = lane % G, xs = x0 + (lane / G) * RG, yb = y0 + 4 * lg;
+  const bool vec = yb + 3 < my;  // the lane's four cells are in the grid
+  const int yh = gp_map_any(lg == 0 ? y0 - 1 : y0 + TY, my, bc.mu_y);  // halo column of the row's end lanes
+  const bool edge = lg == 0 || lg == G - 1;
+  float Db[MK][MK];
+#pragma unroll
+  for (int a = 0; a < N; a++)
+    if (a == b) {
+#pragma unroll
+      for (int k = 0; k < K1; k++)
+#pragma unroll
+        for (int l = 0; l < K1; l++) Db[k][l] = m.DC[a][k][l];
     }
-    __syncthreads();
-    const int tile = s_tile;
-    if (tile < 0) break;
-    const Inst& I = sInst;
-    const Model& m = models[I.model];
-    const int b0 = s_b;
-    const int lt = tile - I.tile_begin;
-    const int x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
-    // interior tile (classification guarantees it): aligned rows y0-4 .. y0+TY+3
-    for (int e = threadIdx.x; e < K1 * X1 * Q; e += nt) {
-      const int k = e / (X1 * Q), r = (e / Q) % X1, q = e % Q;
-      const float4 v = __ldg(reinterpret_cast<const float4*>(I.mu + k * I.plane + (int64_t)(x0 - 1 + r) * I.pitch +
-                                                             (y0 - 4)) + q);
-      reinterpret_cast<float4*>(smu + (k * X1 + r) * W)[q] = v;
-    }
-    __syncthreads();
-    float Db[MK][MK];
+  const bool write_phi = pf(flags_out[t], PF_CORE) != 1 + b;
+
+  auto load_row = [&](int x, float (&v)[4][K1]) {
+    const float* row = mu + (int64_t)gp_map_any(x, mx, bc.mu_x) * pitch;
 #pragma unroll
-    for (int a = 0; a < N; a++)
-      if (a == b0) {
+    for (int k = 0; k < K1; k++) {
+      if (vec) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(row + k * plane + yb));
+        v[0][k] = q.x;
+        v[1][k] = q.y;
+        v[2][k] = q.z;
+        v[3][k] = q.w;
+      } else {
 #pragma unroll
-        for (int k = 0; k < K1; k++)
-#pragma unroll
-          for (int l = 0; l < K1; l++) Db[k][l] = m.DC[a][k][l];
+        for (int j = 0; j < 4; j++) v[j][k] = __ldg(row + k * plane + gp_map_any(yb + j, my, bc.mu_y));
       }
-    const bool write_phi = s_old != 1 + b0;
-    auto MU = [&](int k, int i, int j) -> float { return smu[(k * X1 + i) * W + j + 3]; };
-    for (int r = warp; r < TX; r += nw) {
-      const int x = x0 + r;
+    }
+  };
+
+  float cur[4][K1], fxm[4][K1];
+  {
+    float prev[4][K1];
+    load_row(xs - 1, prev);
+    load_row(xs, cur);
 #pragma unroll
-      for (int c0 = 0; c0 < TY; c0 += 32) {
-        const int c = c0 + lane, y = y0 + c;
-        const int i1 = r + 1, j1 = c + 1;
-        float mc[K1], mb[K1], mf[K1], ml[K1], mr[K1];
+    for (int j = 0; j < 4; j++) diff_flux<K1>(m, Db, Db, prev[j], cur[j], m.dx_inv, fxm[j]);
+  }
+#pragma unroll
+  for (int r0 = 0; r0 < RG; r0 += RB) {
+    float nx[RB][4][K1], hv[RB][K1];
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+      const int x = xs + r0 + r;
+      load_row(x + 1, nx[r]);
+      const float* row = mu + (int64_t)gp_map_any(x, mx, bc.mu_x) * pitch + yh;
+#pragma unroll
+      for (int k = 0; k < K1; k++) hv[r][k] = edge ? __ldg(row + k * plane) : 0.f;
+    }
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+      const int x = xs + r0 + r;
+      float left[K1], right[K1], fy[5][K1], fxp[4][K1];
+#pragma unroll
+      for (int k = 0; k < K1; k++) {
+        const float up = __shfl_up_sync(0xffffffffu, cur[3][k], 1, G);
+        const float dn = __shfl_down_sync(0xffffffffu, cur[0][k], 1, G);
+        left[k] = lg == 0 ? hv[r][k] : up;
+        right[k] = lg == G - 1 ? hv[r][k] : dn;
+      }
+      diff_flux<K1>(m, Db, Db, left, cur[0], m.dy_inv, fy[0]);
+#pragma unroll
+      for (int j = 0; j < 3; j++) diff_flux<K1>(m, Db, Db, cur[j], cur[j + 1], m.dy_inv, fy[j + 1]);
+      diff_flux<K1>(m, Db, Db, cur[3], right, m.dy_inv, fy[4]);
+      float mnew[4][K1];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        diff_flux<K1>(m, Db, Db, cur[j], nx[r][j], m.dx_inv, fxp[j]);
+        float dc[K1];
+#pragma unroll
+        for (int k = 0; k < K1; k++) dc[k] = flux_div(m, fxp[j][k], fxm[j][k], fy[j + 1][k], fy[j][k]);
+        bulk_update<N, K1>(m, b, cur[j], dc, mnew[j]);
+      }
+      if (x < xend) {
+        const int64_t o = (int64_t)x * pitch + yb;
+        if (vec) {
+#pragma unroll
+          for (int k = 0; k < K1; k++)
+            *reinterpret_cast<float4*>(I.mu_out + o + k * plane) =
+                make_float4(mnew[0][k], mnew[1][k], mnew[2][k], mnew[3][k]);
+          if (write_phi) {
+#pragma unroll
+            for (int a = 0; a < N; a++) {
+              const float v = a == b ? 1.f : 0.f;
+              *reinterpret_cast<float4*>(I.phi_out + o + a * plane) = make_float4(v, v, v, v);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (yb + j < my) {
+#pragma unroll
+              for (int k = 0; k < K1; k++) I.mu_out[o + j + k * plane] = mnew[j][k];
+              if (write_phi) {
+#pragma unroll
+                for (int a = 0; a < N; a++) I.phi_out[o + j + a * plane] = a == b ? 1.f : 0.f;
+              }
+            }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++)
 #pragma unroll
         for (int k = 0; k < K1; k++) {
-          mc[k] = MU(k, i1, j1);
-          mb[k] = MU(k, i1 - 1, j1);
-          mf[k] = MU(k, i1 + 1, j1);
-          ml[k] = MU(k, i1, j1 - 1);
-          mr[k] = MU(k, i1, j1 + 1);
+          fxm[j][k] = fxp[j][k];
+          cur[j][k] = nx[r][j][k];
         }
-        float fxp[K1], fxm[K1], fyp[K1], fym[K1], dc[K1], mnew[K1];
-        diff_flux<K1>(m, Db, Db, mc, mf, m.dx_inv, fxp);
-        diff_flux<K1>(m, Db, Db, mb, mc, m.dx_inv, fxm);
-        diff_flux<K1>(m, Db, Db, mc, mr, m.dy_inv, fyp);
-        diff_flux<K1>(m, Db, Db, ml, mc, m.dy_inv, fym);
-#pragma unroll
-        for (int k = 0; k < K1; k++) dc[k] = flux_div(m, fxp[k], fxm[k], fyp[k], fym[k]);
-        bulk_update<N, K1>(m, b0, mc, dc, mnew);
-        const int64_t o = (int64_t)x * I.pitch + y;
-#pragma unroll
-        for (int k = 0; k < K1; k++) I.mu_out[o + k * I.plane] = mnew[k];
-        if (write_phi) {
-#pragma unroll
-          for (int a = 0; a < N; a++) I.phi_out[o + a * I.plane] = (a == b0) ? 1.f : 0.f;
-        }
-      }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) flags_out[tile] = (uint8_t)(1 + b0);
+  }
+  __syncwarp();
+  if (lane == 0) flags_out[t] = pf_all(1 + b);
+}
+
+// The lean tiles of one step.  Warps scan the tiles w, w + W, w + 2W, ...
+// (W = warps of the grid), 32 candidates per ballot, and update the accepted
+// ones.
+template <int N, int K1, int TX, int TY>
+__global__ void __launch_bounds__(256) k_lean32(const Inst* __restrict__ insts, const Model* __restrict__ models,
+                                                const int* __restrict__ tile_inst,
+                                                const uint32_t* __restrict__ flags_in,
+                                                uint32_t* __restrict__ flags_out, int total) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = gw; base < total; base += 32 * nwarp) {
+    const int64_t tc = base + lane * nwarp;
+    int bc = -1;
+    if (tc < total) bc = lean_phase(flags_in, insts[tile_inst[tc]], (int)tc, TX, TY);
+    unsigned todo = __ballot_sync(0xffffffffu, bc >= 0);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int t = (int)(base + src * nwarp);
+      const int b = __shfl_sync(0xffffffffu, bc, src);
+      const Inst& I = insts[tile_inst[t]];
+      lean_tile<N, K1, TX, TY>(I, models[I.model], flags_out, t, b, lane);
+    }
   }
 }
 
-// Split the tiles of one step into the pure list (entry: tile | phase << 24)
-// and the list for the full kernel.  A tile is pure when it is an interior tile
-// (its staged region needs no boundary map) and it and its eight neighbours
-// were written as the same pure phase in the previous step.
+// The tiles of one step that lean_phase rejects, appended to glist (count in
+// cnt[0]) for the full kernel.
 template <int TX, int TY>
-__global__ void __launch_bounds__(256) k_classify(const Inst* __restrict__ insts, const int* __restrict__ tile_inst,
-                                                  int total, const uint8_t* __restrict__ flags_in,
-                                                  int* __restrict__ plist, int* __restrict__ glist,
-                                                  int* __restrict__ cnt) {
+__global__ void __launch_bounds__(256) k_general_list(const Inst* __restrict__ insts,
+                                                      const int* __restrict__ tile_inst,
+                                                      const uint32_t* __restrict__ flags_in, int total,
+                                                      int* __restrict__ glist, int* __restrict__ cnt) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  bool pure = false, gen = false;
-  int code = 0;
-  if (t < total) {
-    const Inst& I = insts[tile_inst[t]];
-    const int lt = t - I.tile_begin, tx = lt / I.tiles_y, ty = lt % I.tiles_y;
-    const int x0 = tx * TX, y0 = ty * TY;
-    const uint8_t f = flags_in[t];
-    if (f && x0 >= 2 && x0 + TX + 2 <= I.mx && y0 >= 4 && y0 + TY + 4 <= I.my) {
-      pure = true;
-#pragma unroll
-      for (int dx = -1; dx <= 1; dx++)
-#pragma unroll
-        for (int dy = -1; dy <= 1; dy++) pure &= flags_in[I.tile_begin + (tx + dx) * I.tiles_y + (ty + dy)] == f;
-      code = t | ((int)(f - 1) << 24);
-    }
-    gen = !pure;
-  }
+  const bool gen = t < total && lean_phase(flags_in, insts[tile_inst[t]], t, TX, TY) < 0;
+  const unsigned bal = __ballot_sync(0xffffffffu, gen);
   const int lane = threadIdx.x & 31;
-  const unsigned bp = __ballot_sync(0xffffffffu, pure), bg = __ballot_sync(0xffffffffu, gen);
-  int basep = 0, baseg = 0;
-  if (lane == 0) {
-    if (bp) basep = atomicAdd(&cnt[0], __popc(bp));
-    if (bg) baseg = atomicAdd(&cnt[1], __popc(bg));
-  }
-  basep = __shfl_sync(0xffffffffu, basep, 0);
-  baseg = __shfl_sync(0xffffffffu, baseg, 0);
-  const unsigned below = (1u << lane) - 1u;
-  if (pure) plist[basep + __popc(bp & below)] = code;
-  if (gen) glist[baseg + __popc(bg & below)] = t;
+  int base = 0;
+  if (lane == 0 && bal) base = atomicAdd(&cnt[0], __popc(bal));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (gen) glist[base + __popc(bal & ((1u << lane) - 1u))] = t;
 }
 
 // ---------------------------------------------------------------- host side
@@ -1089,20 +1219,19 @@ using namespace gp32;
 
 // Kernels of one (N, K1, anisotropy, tile shape).
 struct KernelSet {
-  void (*general)(const Inst*, int, const Model*, const int*, int*, uint8_t*);
-  void (*pure)(const Inst*, int, const Model*, const int*, int*, uint8_t*);
-  void (*classify)(const Inst*, const int*, int, const uint8_t*, int*, int*, int*);
-  size_t smem_general, smem_pure;
+  void (*general)(const Inst*, const Model*, const int*, const int*, int*, uint32_t*);
+  void (*lean)(const Inst*, const Model*, const int*, const uint32_t*, uint32_t*, int);
+  void (*list)(const Inst*, const int*, const uint32_t*, int, int*, int*);
+  size_t smem_general;
 };
 
 template <int N, int K1, bool AN, int TX, int TY>
 static KernelSet make_set() {
   KernelSet k;
   k.general = k_step32<N, K1, AN, TX, TY>;
-  k.pure = k_pure32<N, K1, TX, TY>;
-  k.classify = k_classify<TX, TY>;
+  k.lean = k_lean32<N, K1, TX, TY>;
+  k.list = k_general_list<TX, TY>;
   k.smem_general = Tile<N, K1, AN, TX, TY>::bytes;
-  k.smem_pure = (size_t)K1 * (TX + 2) * (TY + 8) * sizeof(float);
   return k;
 }
 
@@ -1143,19 +1272,18 @@ void gp_f32_tile_shape(int i, int* tx, int* ty) {
 struct gp_f32_batch {
   int n = 0, N = 0, K1 = 0, aniso = 0;
   int tx = 16, ty = 32;  // tile shape (autotuned)
-  int narrowband = 1;    // classify tiles and send pure ones to the lean kernel
+  int narrowband = 1;    // send the tiles lean_phase accepts to the lean kernel
   std::vector<gp_model> gm;
   std::vector<Inst> hinst[2];  // [buffer parity]
   Inst* dinst[2] = {nullptr, nullptr};
   Model* dmodel = nullptr;
   int total_tiles = 0;
   KernelSet ks;
-  uint8_t* dflags = nullptr;  // [2][total_tiles] purity flags of the state in buffer p
-  int* dplist = nullptr;      // [total_tiles]
-  int* dglist = nullptr;      // [total_tiles]
-  int* dcnt = nullptr;        // [4] pure count, general count, pure queue, general queue
-  int* dtile_inst = nullptr;  // [total_tiles] instance of each tile
-  int grid_general = 0, grid_pure = 0;
+  uint32_t* dflags = nullptr;  // [2][total_tiles] purity words of the state in buffer p
+  int* dtile_inst = nullptr;   // [total_tiles] instance of each tile
+  int* dglist = nullptr;       // [total_tiles] tiles of the full kernel
+  int* dcnt = nullptr;         // [4] list count, queue head, finished blocks
+  int grid_general = 0, grid_lean = 0;
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
@@ -1164,11 +1292,11 @@ void gp_f32_batch_destroy(gp_f32_batch* b);
 
 static void free_tiles(gp_f32_batch* b) {
   cudaFree(b->dflags);
-  cudaFree(b->dplist);
-  cudaFree(b->dglist);
   cudaFree(b->dtile_inst);
+  cudaFree(b->dglist);
   b->dflags = nullptr;
-  b->dplist = b->dglist = b->dtile_inst = nullptr;
+  b->dtile_inst = nullptr;
+  b->dglist = nullptr;
 }
 
 cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** out) {
@@ -1189,6 +1317,7 @@ cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** ou
   cudaError_t e = cudaMalloc(&b->dmodel, sizeof(Model) * n);
   if (e == cudaSuccess) e = cudaMemcpy(b->dmodel, hm.data(), sizeof(Model) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc(&b->dcnt, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->dcnt, 0, 4 * sizeof(int));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
@@ -1210,8 +1339,8 @@ void gp_f32_batch_destroy(gp_f32_batch* b) {
   cudaFree(b->dmodel);
   cudaFree(b->dinst[0]);
   cudaFree(b->dinst[1]);
-  cudaFree(b->dcnt);
   free_tiles(b);
+  cudaFree(b->dcnt);
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->ev_join) cudaEventDestroy(b->ev_join);
   if (b->side) cudaStreamDestroy(b->side);
@@ -1240,7 +1369,7 @@ void gp_f32_batch_bind(gp_f32_batch* b, int i, float* phiA, float* muA, float* p
 // behind the kernels' back (upload, restore) they are reset to "unknown".
 cudaError_t gp_f32_batch_invalidate(gp_f32_batch* b, cudaStream_t s) {
   if (!b->dflags) return cudaSuccess;
-  return cudaMemsetAsync(b->dflags, 0, 2 * (size_t)b->total_tiles, s);
+  return cudaMemsetAsync(b->dflags, 0, 2 * sizeof(uint32_t) * (size_t)b->total_tiles, s);
 }
 
 void gp_f32_batch_set_narrowband(gp_f32_batch* b, int on) { b->narrowband = on ? 1 : 0; }
@@ -1257,38 +1386,36 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   for (int i = 0; i < b->n; i++) {
     const int txs = (int)((b->gm[i].mesh_x + tx - 1) / tx), tys = (int)((b->gm[i].mesh_y + ty - 1) / ty);
     for (int p = 0; p < 2; p++) {
+      b->hinst[p][i].tiles_x = txs;
       b->hinst[p][i].tiles_y = tys;
       b->hinst[p][i].tile_begin = t;
     }
     t += txs * tys;
     tile_inst.insert(tile_inst.end(), (size_t)txs * tys, i);
   }
-  if (t >= (1 << 24)) return cudaErrorInvalidValue;  // tile ids share an int with the phase in the pure list
   b->total_tiles = t;
   for (int p = 0; p < 2; p++) {
     cudaError_t e = cudaMemcpy(b->dinst[p], b->hinst[p].data(), sizeof(Inst) * b->n, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return e;
   }
   free_tiles(b);
-  cudaError_t e = cudaMalloc(&b->dflags, 2 * (size_t)t);
-  if (e == cudaSuccess) e = cudaMemset(b->dflags, 0, 2 * (size_t)t);
-  if (e == cudaSuccess) e = cudaMalloc(&b->dplist, sizeof(int) * t);
-  if (e == cudaSuccess) e = cudaMalloc(&b->dglist, sizeof(int) * t);
+  cudaError_t e = cudaMalloc(&b->dflags, 2 * sizeof(uint32_t) * (size_t)t);
+  if (e == cudaSuccess) e = cudaMemset(b->dflags, 0, 2 * sizeof(uint32_t) * (size_t)t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dtile_inst, sizeof(int) * t);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dglist, sizeof(int) * t);
   if (e == cudaSuccess)
     e = cudaMemcpy(b->dtile_inst, tile_inst.data(), sizeof(int) * t, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return e;
   // dynamic shared memory limits and persistent grid sizes
-  int dev = 0, sms = 0, occ_g = 0, occ_p = 0;
+  int dev = 0, sms = 0, occ_g = 0, occ_l = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   e = cudaFuncSetAttribute(ks.general, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_general);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(ks.pure, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_pure);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, ks.general, 256, ks.smem_general);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, ks.pure, 256, ks.smem_pure);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, ks.lean, 256, 0);
   if (e != cudaSuccess) return e;
   b->grid_general = sms * (occ_g > 0 ? occ_g : 1);
-  b->grid_pure = sms * (occ_p > 0 ? occ_p : 1);
+  b->grid_lean = sms * (occ_l > 0 ? occ_l : 1);
   return cudaDeviceSynchronize();  // the flag reset above must land before any stream uses them
 }
 
@@ -1298,27 +1425,46 @@ int gp_f32_batch_tiles(const gp_f32_batch* b) { return b->total_tiles; }
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   const KernelSet& k = b->ks;
   const int p = parity & 1;
-  uint8_t* flags_in = b->dflags + (size_t)p * b->total_tiles;
-  uint8_t* flags_out = b->dflags + (size_t)(p ^ 1) * b->total_tiles;
+  const uint32_t* flags_in = b->dflags + (size_t)p * b->total_tiles;
+  uint32_t* flags_out = b->dflags + (size_t)(p ^ 1) * b->total_tiles;
   if (!b->narrowband) {
-    k.general<<<b->total_tiles, 256, k.smem_general, s>>>(b->dinst[p], b->n, b->dmodel, nullptr, nullptr, flags_out);
+    k.general<<<b->total_tiles, 256, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr,
+                                                          flags_out);
     return cudaGetLastError();
   }
-  cudaError_t e = cudaMemsetAsync(b->dcnt, 0, 4 * sizeof(int), s);
-  if (e != cudaSuccess) return e;
-  k.classify<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dinst[p], b->dtile_inst, b->total_tiles, flags_in,
-                                                          b->dplist, b->dglist, b->dcnt);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  // the pure tiles and the rest run concurrently (disjoint tiles and flags)
+  // the lean tiles (side stream) and the rest run concurrently: disjoint tiles and words
+  cudaError_t e;
   if ((e = cudaEventRecord(b->ev_fork, s)) != cudaSuccess) return e;
   if ((e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess) return e;
-  k.pure<<<b->grid_pure, 256, k.smem_pure, b->side>>>(b->dinst[p], b->n, b->dmodel, b->dplist, b->dcnt, flags_out);
+  k.lean<<<b->grid_lean, 256, 0, b->side>>>(b->dinst[p], b->dmodel, b->dtile_inst, flags_in, flags_out,
+                                            b->total_tiles);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k.general<<<b->grid_general, 256, k.smem_general, s>>>(b->dinst[p], b->n, b->dmodel, b->dglist, b->dcnt,
+  k.list<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dinst[p], b->dtile_inst, flags_in, b->total_tiles, b->dglist,
+                                                      b->dcnt);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k.general<<<b->grid_general, 256, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, b->dglist, b->dcnt,
                                                          flags_out);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess) return e;
   return cudaStreamWaitEvent(s, b->ev_join, 0);
+}
+
+// Tiles the next step (reading buffer parity `parity`) sends to the lean
+// kernel: lean_phase evaluated on the host over a copy of the purity words.
+cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s, int64_t* lean) {
+  std::vector<uint32_t> F(b->total_tiles);
+  cudaError_t e = cudaMemcpyAsync(F.data(), b->dflags + (size_t)(parity & 1) * b->total_tiles,
+                                  sizeof(uint32_t) * F.size(), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  int64_t n = 0;
+  for (int i = 0; i < b->n; i++) {
+    const Inst& I = b->hinst[parity & 1][i];
+    for (int t = I.tile_begin; t < I.tile_begin + I.tiles_x * I.tiles_y; t++)
+      n += b->narrowband && lean_phase(F.data(), I, t, b->tx, b->ty) >= 0;
+  }
+  *lean = n;
+  return cudaSuccess;
 }
 
 // kernel launches one gp_f32_batch_launch issues

@@ -168,23 +168,41 @@ def test_tip_velocity_within_half_percent_of_fp64():
 
 
 def test_narrow_band_is_bit_identical_to_the_full_kernel():
-    """Tiles sorted into the lean pure-phase kernel give the same bits as the
-    full kernel on every tile (and the skipped phi writes leave the right values)."""
-    cases = [configs.binary_case(200, 160, gap=1.0, supersat=0.55, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
+    """Tiles sent to the lean pure-phase kernel get the same bits as from the
+    full kernel, for every tile shape: Neumann borders (mirrored rings), a
+    periodic batch member (wrapped rings are never trusted), partial edge tiles
+    with fewer than three cells on an axis, the skipped phi writes, and a
+    re-upload in mid-run (purity words reset)."""
+    cases = [configs.binary_case(200, 150, gap=1.0, supersat=0.55, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
                                  seed=(0, 0, 8.0)),
              configs.binary_case(160, 224, gap=1.0, supersat=0.4, eps=3.0, delta=0.03, theta=15.0, dt=0.05,
-                                 tau=1.3332, seed=(80, 100, 9.0), bc=(3, 3, 3, 3))]
+                                 tau=1.3332, seed=(80, 100, 9.0), bc=(3, 3, 3, 3)),
+             configs.binary_case(98, 130, gap=1.0, supersat=0.5, eps=4.0, delta=0.01, dt=0.05, tau=1.7776,
+                                 seed=(49, 65, 7.0))]
     loaded = [mb.load_case(c) for c in cases]
-    res = []
-    for on in (True, False):
-        with mb.Batch([m for m, _, _ in loaded]) as b:
+    models = [m for m, _, _ in loaded]
+
+    def run(on, tile, reupload=False):
+        with mb.Batch(models) as b:
+            b.set_tile(*tile)
             b.set_narrowband(on)
             for i, (_, p, u) in enumerate(loaded):
                 b.upload(i, p, u)
-            b.step(301)  # graph replays and direct launches, both buffer parities
-            res.append([b.download(i) for i in range(len(loaded))])
-    for (p1, u1), (p0, u0) in zip(*res):
-        assert np.array_equal(p1, p0) and np.array_equal(u1, u0)
+            b.step(150)  # graph replays and direct launches, both buffer parities
+            if reupload:
+                for i, st in enumerate([b.download(i) for i in range(len(models))]):
+                    b.upload(i, *st)
+            b.step(151)
+            lean = b.lean_tiles()
+            return [b.download(i) for i in range(len(models))], lean
+
+    ref, (lean0, _) = run(False, (16, 32))
+    assert lean0 == 0
+    for tile in [(16, 32), (8, 32), (32, 32), (16, 64)]:
+        got, (lean, total) = run(True, tile, reupload=tile == (16, 32))
+        assert lean > total // 2, (tile, lean, total)  # the lean kernel does most of the work
+        for (p1, u1), (p0, u0) in zip(got, ref):
+            assert np.array_equal(p1, p0) and np.array_equal(u1, u0), tile
     # four phases, two chemical potentials: pure grains of every solid phase and the liquid
     m, phi, mu = mb.load_case(configs.c3(steps=200, mesh=160, nseeds=6, rng_seed=7))
     res = []
@@ -193,5 +211,7 @@ def test_narrow_band_is_bit_identical_to_the_full_kernel():
             b.set_narrowband(on)
             b.upload(0, phi, mu)
             b.step(120)
-            res.append(b.download(0))
-    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+            res.append((b.download(0), b.lean_tiles()))
+    (a, la), (c, lc) = res
+    assert la[0] > 0 and lc[0] == 0
+    assert np.array_equal(a[0], c[0]) and np.array_equal(a[1], c[1])
