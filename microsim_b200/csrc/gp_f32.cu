@@ -37,6 +37,8 @@ constexpr int MK = GP_MAX_K1;
 // FP32 model constants of one instance (built on the host from gp_model).
 struct alignas(16) Model {
   float dx_inv, dy_inv, half_dy_inv, dt, eps, inv_eps, tau, w_obst, jscale, s_well;
+  float hx, hy;    // dt / (2 dx^2), dt / (2 dy^2): face flux (D_c + D_n) * h * (mu_n - mu_c), net = sum of differences
+  float jsx, jsy;  // antitrapping scale of an x / y face: jscale / dx, jscale / dy
   int obstacle, mu_solver, skip_row, pad;
   float Gamma[MP][MP];
   float Gabc[MP][MP][MP];
@@ -120,7 +122,7 @@ __device__ __forceinline__ float c_mu(const Model& m, const float* mu, int a, in
 __device__ __forceinline__ float aniso_ac(float dab, float q0, float q1) {
   const float q2 = q0 * q0 + q1 * q1;
   if (q2 > 1.0e-15f) {
-    const float inv = __frcp_rn(q2);
+    const float inv = 1.f / q2;
     const float x2 = q0 * q0 * inv, y2 = q1 * q1 * inv;
     return 1.f - dab * (3.f - 4.f * (x2 * x2 + y2 * y2));
   }
@@ -132,7 +134,7 @@ __device__ __forceinline__ void aniso_terms(float dab, float q0, float q1, float
                                             float& e1) {
   q2 = q0 * q0 + q1 * q1;
   if (q2 > 1.0e-15f) {
-    const float inv = __frcp_rn(q2);
+    const float inv = 1.f / q2;
     const float x2 = q0 * q0 * inv, y2 = q1 * q1 * inv;
     const float s4 = x2 * x2 + y2 * y2;  // sum q_i^4 / |q|^4
     ac = 1.f - dab * (3.f - 4.f * s4);
@@ -152,20 +154,19 @@ __device__ __forceinline__ void aniso_terms(float dab, float q0, float q1, float
 // re-associated by the compiler), so a cell gets the same bits whichever path
 // its tile takes -- the result does not depend on the tile shape.
 
-// Diffusion flux of every component through one face, dt * sum_l (D_c + D_n)/2
-// (mu_n - mu_c) * h (calculate_gradients.h:132-185 with functionD.h).
+// Diffusion flux of every component through one face, scaled by the face's
+// 1/dx of the divergence: sum_l (D_c + D_n)_kl * dt/(2 dx^2) * (mu_n - mu_c)_l
+// (calculate_gradients.h:132-185 with functionD.h; hh = Model::hx or hy).
 template <int K1>
 __device__ __forceinline__ void diff_flux(const Model& m, const float (&Dc)[MK][MK], const float (&Dn)[MK][MK],
-                                          const float* muc, const float* mun, float h, float* out) {
+                                          const float* muc, const float* mun, float hh, float* out) {
 #pragma unroll
   for (int k = 0; k < K1; k++) {
-    float jd = 0.f;
+    float jd = __fmul_rn(__fmul_rn(__fadd_rn(Dc[k][0], Dn[k][0]), hh), __fsub_rn(mun[0], muc[0]));
 #pragma unroll
-    for (int l = 0; l < K1; l++) {
-      const float dm = __fmul_rn(__fmul_rn(0.5f, __fadd_rn(Dc[k][l], Dn[k][l])), __fsub_rn(mun[l], muc[l]));
-      jd = __fadd_rn(jd, __fmul_rn(dm, h));
-    }
-    out[k] = __fmul_rn(m.dt, jd);
+    for (int l = 1; l < K1; l++)
+      jd = __fmaf_rn(__fmul_rn(__fadd_rn(Dc[k][l], Dn[k][l]), hh), __fsub_rn(mun[l], muc[l]), jd);
+    out[k] = jd;
   }
 }
 
@@ -183,9 +184,9 @@ __device__ __forceinline__ void mobility(const Model& m, const float* ph, float 
     }
 }
 
-// net face flux into a cell: (F(+x) - F(-x))/dx + (F(+y) - F(-y))/dy
+// net face flux into a cell (the fluxes carry the 1/dx of the divergence)
 __device__ __forceinline__ float flux_div(const Model& m, float fxp, float fxm, float fyp, float fym) {
-  return __fadd_rn(__fmul_rn(__fsub_rn(fxp, fxm), m.dx_inv), __fmul_rn(__fsub_rn(fyp, fym), m.dy_inv));
+  return __fadd_rn(__fsub_rn(fxp, fxm), __fsub_rn(fyp, fym));
 }
 
 // bulk cell of phase `bulk`: c -> c + dc, mu = dF/dc (calculate_divergence_concentration.h:216-224)
@@ -236,6 +237,22 @@ struct Tile {
   static constexpr int total = o_act + X1 * Y1;
   static constexpr size_t bytes = total * sizeof(float);
 };
+
+// Asynchronous global -> shared copies (cp.async), completed per thread by
+// wait_group / wait_all and published to the block by a barrier.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------- narrow band
 //
@@ -291,8 +308,9 @@ __host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ 
 
 // Full update of the tiles.  With glist == nullptr block k takes tile k (grid
 // = all tiles).  Otherwise the blocks are persistent and take the cnt[0]
-// tiles of glist through the queue head cnt[1]; the last block to finish
-// resets the counters (cnt[2] counts finished blocks) for the next step.
+// tiles of glist: block k entry k first, then entries grid + (queue head
+// cnt[1]); the last block to finish resets the counters (cnt[2] counts
+// finished blocks) for the next step.
 // Every tile writes the purity word of its output.
 template <int N, int K1, bool ANISO, int TX, int TY>
 __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 2))
@@ -316,8 +334,8 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
   __syncthreads();  // the previous tile's shared state is no longer read
   if (threadIdx.x == 0) {
     int t = -1;
-    if (glist) {
-      const int i = atomicAdd(&cnt[1], 1);
+    if (glist) {  // block k starts with entry k, then takes entries grid, grid + 1, ... from the queue
+      const int i = iter == 0 ? (int)blockIdx.x : (int)gridDim.x + atomicAdd(&cnt[1], 1);
       if (i < cnt[0]) t = glist[i];
     } else if (iter == 0) {
       t = blockIdx.x;
@@ -349,19 +367,16 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
 
   // ---- stage phi (tile +- 2) and mu (tile +- 1)
   const bool inner = x0 >= 2 && x0 + TX + 2 <= mx && y0 >= 4 && y0 + TY + 4 <= my;
+  // (asynchronous copies: every load of the tile is in flight at once)
   if (inner) {
     // whole 16-byte aligned rows y0-4 .. y0+TY+3, no boundary maps needed
     for (int e = threadIdx.x; e < N * X2 * Q; e += nt) {
       const int a = e / (X2 * Q), r = (e / Q) % X2, q = e % Q;
-      const float4 v = __ldg(reinterpret_cast<const float4*>(I.phi + a * I.plane + (int64_t)(x0 - 2 + r) * I.pitch +
-                                                             (y0 - 4)) + q);
-      reinterpret_cast<float4*>(sphi + (a * X2 + r) * W)[q] = v;
+      cp_async16(sphi + (a * X2 + r) * W + 4 * q, I.phi + a * I.plane + (int64_t)(x0 - 2 + r) * I.pitch + (y0 - 4) + 4 * q);
     }
     for (int e = threadIdx.x; e < K1 * X1 * Q; e += nt) {
       const int k = e / (X1 * Q), r = (e / Q) % X1, q = e % Q;
-      const float4 v = __ldg(reinterpret_cast<const float4*>(I.mu + k * I.plane + (int64_t)(x0 - 1 + r) * I.pitch +
-                                                             (y0 - 4)) + q);
-      reinterpret_cast<float4*>(smu + (k * X1 + r) * W)[q] = v;
+      cp_async16(smu + (k * X1 + r) * W + 4 * q, I.mu + k * I.plane + (int64_t)(x0 - 1 + r) * I.pitch + (y0 - 4) + 4 * q);
     }
   } else {
     for (int e = threadIdx.x; e < X2 * Y2; e += nt) {
@@ -369,16 +384,17 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
       const int gx = gp_map_any(x0 - 2 + i, mx, I.bc.phi_x), gy = gp_map_any(y0 - 2 + j, my, I.bc.phi_y);
       const float* p = I.phi + (int64_t)gx * I.pitch + gy;
 #pragma unroll
-      for (int a = 0; a < N; a++) sphi[(a * X2 + i) * W + j + 2] = __ldg(p + a * I.plane);
+      for (int a = 0; a < N; a++) cp_async4(sphi + (a * X2 + i) * W + j + 2, p + a * I.plane);
     }
     for (int e = threadIdx.x; e < X1 * Y1; e += nt) {
       const int i = e / Y1, j = e % Y1;
       const int gx = gp_map_any(x0 - 1 + i, mx, I.bc.mu_x), gy = gp_map_any(y0 - 1 + j, my, I.bc.mu_y);
       const float* p = I.mu + (int64_t)gx * I.pitch + gy;
 #pragma unroll
-      for (int k = 0; k < K1; k++) smu[(k * X1 + i) * W + j + 3] = __ldg(p + k * I.plane);
+      for (int k = 0; k < K1; k++) cp_async4(smu + (k * X1 + i) * W + j + 3, p + k * I.plane);
     }
   }
+  cp_async_wait_all();
   __syncthreads();
 
   // ---- pure-tile test: when every staged cell is the same pure phase, Delta-phi
@@ -424,10 +440,10 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
           mr[k] = MU(k, i1, j1 + 1);
         }
         float fxp[K1], fxm[K1], fyp[K1], fym[K1], dc[K1], mnew[K1];
-        diff_flux<K1>(m, Db, Db, mc, mf, m.dx_inv, fxp);
-        diff_flux<K1>(m, Db, Db, mb, mc, m.dx_inv, fxm);
-        diff_flux<K1>(m, Db, Db, mc, mr, m.dy_inv, fyp);
-        diff_flux<K1>(m, Db, Db, ml, mc, m.dy_inv, fym);
+        diff_flux<K1>(m, Db, Db, mc, mf, m.hx, fxp);
+        diff_flux<K1>(m, Db, Db, mb, mc, m.hx, fxm);
+        diff_flux<K1>(m, Db, Db, mc, mr, m.hy, fyp);
+        diff_flux<K1>(m, Db, Db, ml, mc, m.hy, fym);
 #pragma unroll
         for (int k = 0; k < K1; k++) dc[k] = flux_div(m, fxp[k], fxm[k], fyp[k], fym[k]);
         bulk_update<N, K1>(m, b0, mc, dc, mnew);
@@ -743,7 +759,7 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
     float Dc[MK][MK], Dn[MK][MK];
     mobility<N, K1>(m, pc, Dc);
     mobility<N, K1>(m, pn, Dn);
-    diff_flux<K1>(m, Dc, Dn, muc, mun, xface ? m.dx_inv : m.dy_inv, out);
+    diff_flux<K1>(m, Dc, Dn, muc, mun, xface ? m.hx : m.hy, out);
     if (skip_at) return;
     float tc[N], tn[N], gn[N];
     bool any = false;
@@ -783,7 +799,7 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
         const float dcn = c_mu<K1>(m, mun, L, k) - c_mu<K1>(m, mun, a, k);
         const float dcc = c_mu<K1>(m, muc, L, k) - c_mu<K1>(m, muc, a, k);
         const float jt = m.atf[a][k] * pref * (sn * dcn * dpn + sc * dcc * dpc);
-        out[k] = __fsub_rn(out[k], __fmul_rn(m.jscale, jt));
+        out[k] = __fsub_rn(out[k], __fmul_rn(xface ? m.jsx : m.jsy, jt));
       }
     }
   };
@@ -973,41 +989,79 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
   }
 }
 
-// Lean update of one tile that lean_phase accepted with phase b: diffusion of
-// mu inside phase b; phi stays the one-hot field of b and is written only when
+// Lean update of the tiles lean_phase accepts (phase b): diffusion of mu
+// inside phase b; phi stays the one-hot field of b and is written only when
 // the output buffer does not hold it already (its purity word says so).
 //
-// One warp per tile.  A row of the tile is G = TY/4 lanes of four cells each
-// (float4 loads and stores); the warp's 32/G lane groups take RG consecutive
-// rows each and stream them along x: each x-face flux is evaluated once and
-// carried to the next row, the y-faces between a lane's cells once, the
-// lane-boundary faces from the neighbour lane's cell (shuffle) -- the same
-// helper calls on the same operands as the full update's pure path, hence the
-// same bits.  Rows are loaded RB at a time ahead of their use; rows, halo
-// columns and partial tiles go through the boundary map.
+// One warp per tile.  A row of the tile is G = TY/4 lanes of four cells each;
+// the warp's 32/G lane groups take RG consecutive rows each and stream them
+// along x: each x-face flux is evaluated once and carried to the next row, the
+// y-faces between a lane's cells once, the lane-boundary faces from the
+// neighbour lane's cell (shuffle) -- the same helper calls on the same operands
+// as the full update's pure path, hence the same bits.  A group's RG + 2 mu
+// rows and its halo columns are staged in the warp's shared-memory buffer by
+// asynchronous copies (cp.async), double-buffered: the next tile's rows are in
+// flight while the current tile is computed.  Rows, halo columns and partial
+// tiles go through the boundary map.
 template <int N, int K1, int TX, int TY>
 struct Lean {
   static constexpr int G = TY / 4;     // lanes per tile row
   static constexpr int NG = 32 / G;    // row groups per warp
   static constexpr int RG = TX / NG;   // rows per group
-  static constexpr int RB = RG < 8 / K1 ? RG : 8 / K1;  // rows loaded ahead
+  static constexpr int ROWS = RG + 2;  // rows a group stages
+  static constexpr int HALO = NG * ROWS * K1 * TY;      // offset of the halo columns in a buffer
+  static constexpr int BUF = HALO + NG * RG * K1 * 2;   // floats per buffer
+  static constexpr int WARPS = 4;                       // warps per block
+  static constexpr size_t smem = (size_t)WARPS * 2 * BUF * sizeof(float);
   static_assert(G * NG == 32 && RG * NG == TX, "tile shape");
+  static_assert(HALO % 4 == 0 && BUF % 4 == 0, "16-byte aligned rows");
 };
 
+// Issue the copies of tile t's mu rows and halo columns into buffer `buf`.
 template <int N, int K1, int TX, int TY>
-__device__ __forceinline__ void lean_tile(const Inst& I, const Model& m, uint32_t* __restrict__ flags_out, int t,
-                                          int b, int lane) {
+__device__ __forceinline__ void lean_stage(const Inst& I, int t, float* buf, int lane) {
   using S = Lean<N, K1, TX, TY>;
-  constexpr int G = S::G, RG = S::RG, RB = S::RB;
+  constexpr int G = S::G, RG = S::RG, ROWS = S::ROWS;
   const int lt = t - I.tile_begin, x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
-  const int mx = I.mx, my = I.my, xend = min(x0 + TX, mx);
+  const int mx = I.mx, my = I.my, lg = lane % G, grp = lane / G, xs = x0 + grp * RG, yb = y0 + 4 * lg;
   const int64_t pitch = I.pitch, plane = I.plane;
-  const float* mu = I.mu;
-  const gp_bc bc = I.bc;
-  const int lg = lane % G, xs = x0 + (lane / G) * RG, yb = y0 + 4 * lg;
-  const bool vec = yb + 3 < my;  // the lane's four cells are in the grid
-  const int yh = gp_map_any(lg == 0 ? y0 - 1 : y0 + TY, my, bc.mu_y);  // halo column of the row's end lanes
-  const bool edge = lg == 0 || lg == G - 1;
+  const bool vec = yb + 3 < my;
+#pragma unroll
+  for (int r = 0; r < ROWS; r++) {
+    const float* row = I.mu + (int64_t)gp_map_any(xs - 1 + r, mx, I.bc.mu_x) * pitch;
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      float* dst = buf + ((grp * ROWS + r) * K1 + k) * TY + 4 * lg;
+      if (vec) {
+        cp_async16(dst, row + k * plane + yb);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) cp_async4(dst + j, row + k * plane + gp_map_any(yb + j, my, I.bc.mu_y));
+      }
+    }
+  }
+  if (lg == 0 || lg == G - 1) {
+    const int col = gp_map_any(lg == 0 ? y0 - 1 : y0 + TY, my, I.bc.mu_y);
+#pragma unroll
+    for (int r = 0; r < RG; r++) {
+      const float* src = I.mu + (int64_t)gp_map_any(xs + r, mx, I.bc.mu_x) * pitch + col;
+#pragma unroll
+      for (int k = 0; k < K1; k++) cp_async4(buf + S::HALO + ((grp * RG + r) * K1 + k) * 2 + (lg ? 1 : 0), src + k * plane);
+    }
+  }
+}
+
+// Update tile t from its staged rows.
+template <int N, int K1, int TX, int TY>
+__device__ __forceinline__ void lean_compute(const Inst& I, const Model& m, uint32_t* __restrict__ flags_out, int t,
+                                             int b, const float* buf, int lane) {
+  using S = Lean<N, K1, TX, TY>;
+  constexpr int G = S::G, RG = S::RG, ROWS = S::ROWS;
+  const int lt = t - I.tile_begin, x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
+  const int mx = I.mx, my = I.my, lg = lane % G, grp = lane / G, xs = x0 + grp * RG, yb = y0 + 4 * lg;
+  const int xend = min(x0 + TX, mx);
+  const int64_t pitch = I.pitch, plane = I.plane;
+  const bool vec = yb + 3 < my;
   float Db[MK][MK];
 #pragma unroll
   for (int a = 0; a < N; a++)
@@ -1018,102 +1072,84 @@ __device__ __forceinline__ void lean_tile(const Inst& I, const Model& m, uint32_
         for (int l = 0; l < K1; l++) Db[k][l] = m.DC[a][k][l];
     }
   const bool write_phi = pf(flags_out[t], PF_CORE) != 1 + b;
-
-  auto load_row = [&](int x, float (&v)[4][K1]) {
-    const float* row = mu + (int64_t)gp_map_any(x, mx, bc.mu_x) * pitch;
+  auto row = [&](int r, float (&v)[4][K1]) {
 #pragma unroll
     for (int k = 0; k < K1; k++) {
-      if (vec) {
-        const float4 q = __ldg(reinterpret_cast<const float4*>(row + k * plane + yb));
-        v[0][k] = q.x;
-        v[1][k] = q.y;
-        v[2][k] = q.z;
-        v[3][k] = q.w;
-      } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++) v[j][k] = __ldg(row + k * plane + gp_map_any(yb + j, my, bc.mu_y));
-      }
+      const float4 q = *reinterpret_cast<const float4*>(buf + ((grp * ROWS + r) * K1 + k) * TY + 4 * lg);
+      v[0][k] = q.x;
+      v[1][k] = q.y;
+      v[2][k] = q.z;
+      v[3][k] = q.w;
     }
   };
-
   float cur[4][K1], fxm[4][K1];
   {
     float prev[4][K1];
-    load_row(xs - 1, prev);
-    load_row(xs, cur);
+    row(0, prev);
+    row(1, cur);
 #pragma unroll
-    for (int j = 0; j < 4; j++) diff_flux<K1>(m, Db, Db, prev[j], cur[j], m.dx_inv, fxm[j]);
+    for (int j = 0; j < 4; j++) diff_flux<K1>(m, Db, Db, prev[j], cur[j], m.hx, fxm[j]);
   }
 #pragma unroll
-  for (int r0 = 0; r0 < RG; r0 += RB) {
-    float nx[RB][4][K1], hv[RB][K1];
+  for (int r = 0; r < RG; r++) {
+    const int x = xs + r;
+    float nx[4][K1], left[K1], right[K1], fy[5][K1];
+    row(r + 2, nx);
 #pragma unroll
-    for (int r = 0; r < RB; r++) {
-      const int x = xs + r0 + r;
-      load_row(x + 1, nx[r]);
-      const float* row = mu + (int64_t)gp_map_any(x, mx, bc.mu_x) * pitch + yh;
-#pragma unroll
-      for (int k = 0; k < K1; k++) hv[r][k] = edge ? __ldg(row + k * plane) : 0.f;
+    for (int k = 0; k < K1; k++) {
+      const float up = __shfl_up_sync(0xffffffffu, cur[3][k], 1, G);
+      const float dn = __shfl_down_sync(0xffffffffu, cur[0][k], 1, G);
+      const float h = buf[S::HALO + ((grp * RG + r) * K1 + k) * 2 + (lg ? 1 : 0)];
+      left[k] = lg == 0 ? h : up;
+      right[k] = lg == G - 1 ? h : dn;
     }
+    diff_flux<K1>(m, Db, Db, left, cur[0], m.hy, fy[0]);
 #pragma unroll
-    for (int r = 0; r < RB; r++) {
-      const int x = xs + r0 + r;
-      float left[K1], right[K1], fy[5][K1], fxp[4][K1];
+    for (int j = 0; j < 3; j++) diff_flux<K1>(m, Db, Db, cur[j], cur[j + 1], m.hy, fy[j + 1]);
+    diff_flux<K1>(m, Db, Db, cur[3], right, m.hy, fy[4]);
+    float mnew[4][K1];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      float fxp[K1], dc[K1];
+      diff_flux<K1>(m, Db, Db, cur[j], nx[j], m.hx, fxp);
 #pragma unroll
       for (int k = 0; k < K1; k++) {
-        const float up = __shfl_up_sync(0xffffffffu, cur[3][k], 1, G);
-        const float dn = __shfl_down_sync(0xffffffffu, cur[0][k], 1, G);
-        left[k] = lg == 0 ? hv[r][k] : up;
-        right[k] = lg == G - 1 ? hv[r][k] : dn;
+        dc[k] = flux_div(m, fxp[k], fxm[j][k], fy[j + 1][k], fy[j][k]);
+        fxm[j][k] = fxp[k];
       }
-      diff_flux<K1>(m, Db, Db, left, cur[0], m.dy_inv, fy[0]);
+      bulk_update<N, K1>(m, b, cur[j], dc, mnew[j]);
+    }
+    if (x < xend) {
+      const int64_t o = (int64_t)x * pitch + yb;
+      if (vec) {
 #pragma unroll
-      for (int j = 0; j < 3; j++) diff_flux<K1>(m, Db, Db, cur[j], cur[j + 1], m.dy_inv, fy[j + 1]);
-      diff_flux<K1>(m, Db, Db, cur[3], right, m.dy_inv, fy[4]);
-      float mnew[4][K1];
+        for (int k = 0; k < K1; k++)
+          *reinterpret_cast<float4*>(I.mu_out + o + k * plane) =
+              make_float4(mnew[0][k], mnew[1][k], mnew[2][k], mnew[3][k]);
+        if (write_phi) {
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        diff_flux<K1>(m, Db, Db, cur[j], nx[r][j], m.dx_inv, fxp[j]);
-        float dc[K1];
+          for (int a = 0; a < N; a++) {
+            const float v = a == b ? 1.f : 0.f;
+            *reinterpret_cast<float4*>(I.phi_out + o + a * plane) = make_float4(v, v, v, v);
+          }
+        }
+      } else {
 #pragma unroll
-        for (int k = 0; k < K1; k++) dc[k] = flux_div(m, fxp[j][k], fxm[j][k], fy[j + 1][k], fy[j][k]);
-        bulk_update<N, K1>(m, b, cur[j], dc, mnew[j]);
-      }
-      if (x < xend) {
-        const int64_t o = (int64_t)x * pitch + yb;
-        if (vec) {
+        for (int j = 0; j < 4; j++)
+          if (yb + j < my) {
 #pragma unroll
-          for (int k = 0; k < K1; k++)
-            *reinterpret_cast<float4*>(I.mu_out + o + k * plane) =
-                make_float4(mnew[0][k], mnew[1][k], mnew[2][k], mnew[3][k]);
-          if (write_phi) {
+            for (int k = 0; k < K1; k++) I.mu_out[o + j + k * plane] = mnew[j][k];
+            if (write_phi) {
 #pragma unroll
-            for (int a = 0; a < N; a++) {
-              const float v = a == b ? 1.f : 0.f;
-              *reinterpret_cast<float4*>(I.phi_out + o + a * plane) = make_float4(v, v, v, v);
+              for (int a = 0; a < N; a++) I.phi_out[o + j + a * plane] = a == b ? 1.f : 0.f;
             }
           }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 4; j++)
-            if (yb + j < my) {
-#pragma unroll
-              for (int k = 0; k < K1; k++) I.mu_out[o + j + k * plane] = mnew[j][k];
-              if (write_phi) {
-#pragma unroll
-                for (int a = 0; a < N; a++) I.phi_out[o + j + a * plane] = a == b ? 1.f : 0.f;
-              }
-            }
-        }
       }
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-#pragma unroll
-        for (int k = 0; k < K1; k++) {
-          fxm[j][k] = fxp[j][k];
-          cur[j][k] = nx[r][j][k];
-        }
     }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int k = 0; k < K1; k++) cur[j][k] = nx[j][k];
   }
   __syncwarp();
   if (lane == 0) flags_out[t] = pf_all(1 + b);
@@ -1121,13 +1157,16 @@ __device__ __forceinline__ void lean_tile(const Inst& I, const Model& m, uint32_
 
 // The lean tiles of one step.  Warps scan the tiles w, w + W, w + 2W, ...
 // (W = warps of the grid), 32 candidates per ballot, and update the accepted
-// ones.
+// ones, staging the next tile while computing the current one.
 template <int N, int K1, int TX, int TY>
-__global__ void __launch_bounds__(256) k_lean32(const Inst* __restrict__ insts, const Model* __restrict__ models,
+__global__ void __launch_bounds__(128) k_lean32(const Inst* __restrict__ insts, const Model* __restrict__ models,
                                                 const int* __restrict__ tile_inst,
                                                 const uint32_t* __restrict__ flags_in,
                                                 uint32_t* __restrict__ flags_out, int total) {
+  using S = Lean<N, K1, TX, TY>;
+  extern __shared__ __align__(16) float lsm[];
   const int lane = threadIdx.x & 31;
+  float* wbuf = lsm + (threadIdx.x >> 5) * 2 * S::BUF;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t base = gw; base < total; base += 32 * nwarp) {
@@ -1135,13 +1174,29 @@ __global__ void __launch_bounds__(256) k_lean32(const Inst* __restrict__ insts, 
     int bc = -1;
     if (tc < total) bc = lean_phase(flags_in, insts[tile_inst[tc]], (int)tc, TX, TY);
     unsigned todo = __ballot_sync(0xffffffffu, bc >= 0);
-    while (todo) {
-      const int src = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const int t = (int)(base + src * nwarp);
-      const int b = __shfl_sync(0xffffffffu, bc, src);
+    if (!todo) continue;
+    int src = __ffs(todo) - 1;
+    todo &= todo - 1;
+    int t = (int)(base + src * nwarp), b = __shfl_sync(0xffffffffu, bc, src);
+    lean_stage<N, K1, TX, TY>(insts[tile_inst[t]], t, wbuf, lane);
+    cp_async_commit();
+    for (int i = 0; t >= 0; i++) {
+      int tn = -1, bn = -1;
+      if (todo) {
+        src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        tn = (int)(base + src * nwarp);
+        bn = __shfl_sync(0xffffffffu, bc, src);
+        lean_stage<N, K1, TX, TY>(insts[tile_inst[tn]], tn, wbuf + ((i + 1) & 1) * S::BUF, lane);
+      }
+      cp_async_commit();
+      cp_async_wait_prev();  // all but the copies just issued: tile t is staged
+      __syncwarp();
       const Inst& I = insts[tile_inst[t]];
-      lean_tile<N, K1, TX, TY>(I, models[I.model], flags_out, t, b, lane);
+      lean_compute<N, K1, TX, TY>(I, models[I.model], flags_out, t, b, wbuf + (i & 1) * S::BUF, lane);
+      __syncwarp();  // buffer (i & 1) is reused by the copies issued in iteration i + 1
+      t = tn;
+      b = bn;
     }
   }
 }
@@ -1177,6 +1232,10 @@ Model make_model(const gp_model& g) {
   m.tau = (float)g.tau;
   m.w_obst = (float)g.w_obstacle;
   m.jscale = (float)(g.obstacle ? g.jat_obst : g.jat_well);
+  m.hx = (float)(0.5 * g.dt / (g.dx * g.dx));
+  m.hy = (float)(0.5 * g.dt / (g.dy * g.dy));
+  m.jsx = (float)((g.obstacle ? g.jat_obst : g.jat_well) / g.dx);
+  m.jsy = (float)((g.obstacle ? g.jat_obst : g.jat_well) / g.dy);
   m.s_well = (float)g.s_well;
   m.obstacle = g.obstacle;
   m.mu_solver = g.mu_solver;
@@ -1222,7 +1281,7 @@ struct KernelSet {
   void (*general)(const Inst*, const Model*, const int*, const int*, int*, uint32_t*);
   void (*lean)(const Inst*, const Model*, const int*, const uint32_t*, uint32_t*, int);
   void (*list)(const Inst*, const int*, const uint32_t*, int, int*, int*);
-  size_t smem_general;
+  size_t smem_general, smem_lean;
 };
 
 template <int N, int K1, bool AN, int TX, int TY>
@@ -1232,6 +1291,7 @@ static KernelSet make_set() {
   k.lean = k_lean32<N, K1, TX, TY>;
   k.list = k_general_list<TX, TY>;
   k.smem_general = Tile<N, K1, AN, TX, TY>::bytes;
+  k.smem_lean = Lean<N, K1, TX, TY>::smem;
   return k;
 }
 
@@ -1412,7 +1472,8 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   e = cudaFuncSetAttribute(ks.general, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_general);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, ks.general, 256, ks.smem_general);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, ks.lean, 256, 0);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(ks.lean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_lean);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, ks.lean, 128, ks.smem_lean);
   if (e != cudaSuccess) return e;
   b->grid_general = sms * (occ_g > 0 ? occ_g : 1);
   b->grid_lean = sms * (occ_l > 0 ? occ_l : 1);
@@ -1436,7 +1497,7 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   cudaError_t e;
   if ((e = cudaEventRecord(b->ev_fork, s)) != cudaSuccess) return e;
   if ((e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess) return e;
-  k.lean<<<b->grid_lean, 256, 0, b->side>>>(b->dinst[p], b->dmodel, b->dtile_inst, flags_in, flags_out,
+  k.lean<<<b->grid_lean, 128, k.smem_lean, b->side>>>(b->dinst[p], b->dmodel, b->dtile_inst, flags_in, flags_out,
                                             b->total_tiles);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k.list<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dinst[p], b->dtile_inst, flags_in, b->total_tiles, b->dglist,
