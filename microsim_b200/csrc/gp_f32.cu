@@ -189,29 +189,54 @@ __device__ __forceinline__ float flux_div(const Model& m, float fxp, float fxm, 
   return __fadd_rn(__fsub_rn(fxp, fxm), __fsub_rn(fyp, fym));
 }
 
-// bulk cell of phase `bulk`: c -> c + dc, mu = dF/dc (calculate_divergence_concentration.h:216-224)
+// bulk cell of one phase: c -> c + dc, mu = dF/dc (calculate_divergence_concentration.h:216-224),
+// with that phase's cmu, Beff and A
+template <int K1>
+__device__ __forceinline__ void bulk_update_v(const float (&cm)[MK][MK], const float (&be)[MK],
+                                              const float (&aa)[MK][MK], const float* mu, const float* dc,
+                                              float* mnew) {
+  float c[K1];
+#pragma unroll
+  for (int k = 0; k < K1; k++) {
+    float s = 0.f;
+#pragma unroll
+    for (int l = 0; l < K1; l++) s = __fmaf_rn(cm[k][l], __fsub_rn(mu[l], be[l]), s);
+    c[k] = __fadd_rn(s, dc[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < K1; k++) {
+    float s = __fmaf_rn(__fmul_rn(2.f, aa[k][k]), c[k], be[k]);
+#pragma unroll
+    for (int l = 0; l < K1; l++)
+      if (l != k) s = __fmaf_rn(aa[k][l], c[l], s);
+    mnew[k] = s;
+  }
+}
+
+// the constants bulk_update_v needs, of phase b
 template <int N, int K1>
-__device__ __forceinline__ void bulk_update(const Model& m, int bulk, const float* mu, const float* dc, float* mnew) {
+__device__ __forceinline__ void phase_consts(const Model& m, int b, float (&cm)[MK][MK], float (&be)[MK],
+                                             float (&aa)[MK][MK]) {
 #pragma unroll
   for (int a = 0; a < N; a++)
-    if (a == bulk) {
-      float c[K1];
+    if (a == b) {
 #pragma unroll
       for (int k = 0; k < K1; k++) {
-        float s = 0.f;
+        be[k] = m.Beff[a][k];
 #pragma unroll
-        for (int l = 0; l < K1; l++) s = __fmaf_rn(m.cmu[a][k][l], __fsub_rn(mu[l], m.Beff[a][l]), s);
-        c[k] = __fadd_rn(s, dc[k]);
-      }
-#pragma unroll
-      for (int k = 0; k < K1; k++) {
-        float s = __fmaf_rn(__fmul_rn(2.f, m.A[a][k][k]), c[k], m.Beff[a][k]);
-#pragma unroll
-        for (int l = 0; l < K1; l++)
-          if (l != k) s = __fmaf_rn(m.A[a][k][l], c[l], s);
-        mnew[k] = s;
+        for (int l = 0; l < K1; l++) {
+          cm[k][l] = m.cmu[a][k][l];
+          aa[k][l] = m.A[a][k][l];
+        }
       }
     }
+}
+
+template <int N, int K1>
+__device__ __forceinline__ void bulk_update(const Model& m, int bulk, const float* mu, const float* dc, float* mnew) {
+  float cm[MK][MK], be[MK], aa[MK][MK];
+  phase_consts<N, K1>(m, bulk, cm, be, aa);
+  bulk_update_v<K1>(cm, be, aa, mu, dc, mnew);
 }
 
 // ---------------------------------------------------------------- the fused step
@@ -1019,12 +1044,35 @@ struct Lean {
 
 // Issue the copies of tile t's mu rows and halo columns into buffer `buf`.
 template <int N, int K1, int TX, int TY>
-__device__ __forceinline__ void lean_stage(const Inst& I, int t, float* buf, int lane) {
+__device__ __forceinline__ void lean_stage(const Inst& Ig, int t, float* buf, int lane) {
   using S = Lean<N, K1, TX, TY>;
   constexpr int G = S::G, RG = S::RG, ROWS = S::ROWS;
+  const Inst I = Ig;  // one copy into registers
   const int lt = t - I.tile_begin, x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
   const int mx = I.mx, my = I.my, lg = lane % G, grp = lane / G, xs = x0 + grp * RG, yb = y0 + 4 * lg;
   const int64_t pitch = I.pitch, plane = I.plane;
+  const bool edge = lg == 0 || lg == G - 1;
+  float* hdst = buf + S::HALO + grp * RG * K1 * 2 + (lg ? 1 : 0);
+  if (x0 >= 1 && x0 + TX < mx && y0 >= 1 && y0 + TY < my) {  // every staged cell is in the grid
+    const float* src = I.mu + (int64_t)(xs - 1) * pitch + yb;
+    float* dst = buf + grp * ROWS * K1 * TY + 4 * lg;
+#pragma unroll
+    for (int r = 0; r < ROWS; r++) {
+#pragma unroll
+      for (int k = 0; k < K1; k++) cp_async16(dst + (r * K1 + k) * TY, src + k * plane);
+      src += pitch;
+    }
+    if (edge) {
+      const float* h = I.mu + (int64_t)xs * pitch + (lg == 0 ? y0 - 1 : y0 + TY);
+#pragma unroll
+      for (int r = 0; r < RG; r++) {
+#pragma unroll
+        for (int k = 0; k < K1; k++) cp_async4(hdst + (r * K1 + k) * 2, h + k * plane);
+        h += pitch;
+      }
+    }
+    return;
+  }
   const bool vec = yb + 3 < my;
 #pragma unroll
   for (int r = 0; r < ROWS; r++) {
@@ -1040,29 +1088,36 @@ __device__ __forceinline__ void lean_stage(const Inst& I, int t, float* buf, int
       }
     }
   }
-  if (lg == 0 || lg == G - 1) {
+  if (edge) {
     const int col = gp_map_any(lg == 0 ? y0 - 1 : y0 + TY, my, I.bc.mu_y);
 #pragma unroll
     for (int r = 0; r < RG; r++) {
       const float* src = I.mu + (int64_t)gp_map_any(xs + r, mx, I.bc.mu_x) * pitch + col;
 #pragma unroll
-      for (int k = 0; k < K1; k++) cp_async4(buf + S::HALO + ((grp * RG + r) * K1 + k) * 2 + (lg ? 1 : 0), src + k * plane);
+      for (int k = 0; k < K1; k++) cp_async4(hdst + (r * K1 + k) * 2, src + k * plane);
     }
   }
 }
 
 // Update tile t from its staged rows.
 template <int N, int K1, int TX, int TY>
-__device__ __forceinline__ void lean_compute(const Inst& I, const Model& m, uint32_t* __restrict__ flags_out, int t,
-                                             int b, const float* buf, int lane) {
+__device__ __forceinline__ void lean_compute(const Inst& Ig, const Model* __restrict__ models,
+                                             uint32_t* __restrict__ flags_out, int t, int b, const float* buf,
+                                             int lane) {
   using S = Lean<N, K1, TX, TY>;
   constexpr int G = S::G, RG = S::RG, ROWS = S::ROWS;
+  const Inst I = Ig;  // one copy into registers
   const int lt = t - I.tile_begin, x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
   const int mx = I.mx, my = I.my, lg = lane % G, grp = lane / G, xs = x0 + grp * RG, yb = y0 + 4 * lg;
   const int xend = min(x0 + TX, mx);
   const int64_t pitch = I.pitch, plane = I.plane;
+  float* const mu_out = I.mu_out;
+  float* const phi_out = I.phi_out;
   const bool vec = yb + 3 < my;
-  float Db[MK][MK];
+  // the phase's constants, once per tile into registers
+  const Model& m = models[I.model];
+  const float hx = m.hx, hy = m.hy;
+  float Db[MK][MK], cm[MK][MK], be[MK], aa[MK][MK];
 #pragma unroll
   for (int a = 0; a < N; a++)
     if (a == b) {
@@ -1071,6 +1126,7 @@ __device__ __forceinline__ void lean_compute(const Inst& I, const Model& m, uint
 #pragma unroll
         for (int l = 0; l < K1; l++) Db[k][l] = m.DC[a][k][l];
     }
+  phase_consts<N, K1>(m, b, cm, be, aa);
   const bool write_phi = pf(flags_out[t], PF_CORE) != 1 + b;
   auto row = [&](int r, float (&v)[4][K1]) {
 #pragma unroll
@@ -1088,7 +1144,7 @@ __device__ __forceinline__ void lean_compute(const Inst& I, const Model& m, uint
     row(0, prev);
     row(1, cur);
 #pragma unroll
-    for (int j = 0; j < 4; j++) diff_flux<K1>(m, Db, Db, prev[j], cur[j], m.hx, fxm[j]);
+    for (int j = 0; j < 4; j++) diff_flux<K1>(m, Db, Db, prev[j], cur[j], hx, fxm[j]);
   }
 #pragma unroll
   for (int r = 0; r < RG; r++) {
@@ -1103,34 +1159,34 @@ __device__ __forceinline__ void lean_compute(const Inst& I, const Model& m, uint
       left[k] = lg == 0 ? h : up;
       right[k] = lg == G - 1 ? h : dn;
     }
-    diff_flux<K1>(m, Db, Db, left, cur[0], m.hy, fy[0]);
+    diff_flux<K1>(m, Db, Db, left, cur[0], hy, fy[0]);
 #pragma unroll
-    for (int j = 0; j < 3; j++) diff_flux<K1>(m, Db, Db, cur[j], cur[j + 1], m.hy, fy[j + 1]);
-    diff_flux<K1>(m, Db, Db, cur[3], right, m.hy, fy[4]);
+    for (int j = 0; j < 3; j++) diff_flux<K1>(m, Db, Db, cur[j], cur[j + 1], hy, fy[j + 1]);
+    diff_flux<K1>(m, Db, Db, cur[3], right, hy, fy[4]);
     float mnew[4][K1];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       float fxp[K1], dc[K1];
-      diff_flux<K1>(m, Db, Db, cur[j], nx[j], m.hx, fxp);
+      diff_flux<K1>(m, Db, Db, cur[j], nx[j], hx, fxp);
 #pragma unroll
       for (int k = 0; k < K1; k++) {
         dc[k] = flux_div(m, fxp[k], fxm[j][k], fy[j + 1][k], fy[j][k]);
         fxm[j][k] = fxp[k];
       }
-      bulk_update<N, K1>(m, b, cur[j], dc, mnew[j]);
+      bulk_update_v<K1>(cm, be, aa, cur[j], dc, mnew[j]);
     }
     if (x < xend) {
       const int64_t o = (int64_t)x * pitch + yb;
       if (vec) {
 #pragma unroll
         for (int k = 0; k < K1; k++)
-          *reinterpret_cast<float4*>(I.mu_out + o + k * plane) =
+          *reinterpret_cast<float4*>(mu_out + o + k * plane) =
               make_float4(mnew[0][k], mnew[1][k], mnew[2][k], mnew[3][k]);
         if (write_phi) {
 #pragma unroll
           for (int a = 0; a < N; a++) {
             const float v = a == b ? 1.f : 0.f;
-            *reinterpret_cast<float4*>(I.phi_out + o + a * plane) = make_float4(v, v, v, v);
+            *reinterpret_cast<float4*>(phi_out + o + a * plane) = make_float4(v, v, v, v);
           }
         }
       } else {
@@ -1138,10 +1194,10 @@ __device__ __forceinline__ void lean_compute(const Inst& I, const Model& m, uint
         for (int j = 0; j < 4; j++)
           if (yb + j < my) {
 #pragma unroll
-            for (int k = 0; k < K1; k++) I.mu_out[o + j + k * plane] = mnew[j][k];
+            for (int k = 0; k < K1; k++) mu_out[o + j + k * plane] = mnew[j][k];
             if (write_phi) {
 #pragma unroll
-              for (int a = 0; a < N; a++) I.phi_out[o + j + a * plane] = a == b ? 1.f : 0.f;
+              for (int a = 0; a < N; a++) phi_out[o + j + a * plane] = a == b ? 1.f : 0.f;
             }
           }
       }
@@ -1192,8 +1248,7 @@ __global__ void __launch_bounds__(128) k_lean32(const Inst* __restrict__ insts, 
       cp_async_commit();
       cp_async_wait_prev();  // all but the copies just issued: tile t is staged
       __syncwarp();
-      const Inst& I = insts[tile_inst[t]];
-      lean_compute<N, K1, TX, TY>(I, models[I.model], flags_out, t, b, wbuf + (i & 1) * S::BUF, lane);
+      lean_compute<N, K1, TX, TY>(insts[tile_inst[t]], models, flags_out, t, b, wbuf + (i & 1) * S::BUF, lane);
       __syncwarp();  // buffer (i & 1) is reused by the copies issued in iteration i + 1
       t = tn;
       b = bn;
