@@ -1,24 +1,33 @@
 """Benchmark of the grand-potential explicit step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2|c4|c1] [--precision fp32|fp64]
+                    [--workload c4|c2|c1]
 
 One "step" is one explicit time step (phase-field half step, boundary copy,
 concentration half step) of the whole workload, the unit of the reference's
 time loop (microsim_gp.c:102-106).  The metric is cell-updates/s = interior
 cells x steps / time.
 
-Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events on
-the context's own stream, with an L2 flush (a 256 MiB write, more than the
-126 MB L2) between timed steps and outside the events; the state of one 1024^2
-instance would otherwise stay L2-resident.  Multi-GPU (torchrun): every rank
-runs its own replica of the workload (the single-instance step does not
-shard), barrier before and after, max over ranks.
+Workloads: c4 (default) is the batched sweep the FP32-batched metric is quoted
+on: 256 binary dendrite instances of sides 128..512, 25.1 M cells, one batch
+(narrow band, CUDA-graph replay, autotuned tile); c2 a single 1024^2 dendrite;
+c1 a single 200^2 seed.  The state is first advanced part-way through the run
+(untimed), so the interfaces have grown.
+
+Timing: W untimed warm-up steps, then K steps bracketed by CUDA events on the
+batch's own stream.  A workload whose state fits in L2 is timed step by step
+with an L2 flush (a 256 MiB write, more than the 126 MB L2) between steps and
+outside the events; the batched sweep (301 MB per buffer) is larger than L2
+and is timed as one graph-replayed run.  The same K steps are then replayed
+with per-kernel CUDA events (direct launches) for the roofline of the dominant
+kernel, and the FP64 plain step is timed on the same workload.  Multi-GPU
+(torchrun): every rank runs its own replica of the workload (instances do not
+exchange data), barrier before and after, max over ranks.
 
 The reference arm (--impl reference) times the reference serial solver,
 compiled from its own sources (oracle/_ref/gp_ref_harness), on the host's
-cores: one process per core, each on the same workload for a bounded number of
-steps.
+cores: one process per core, each on one instance of the workload (distinct
+instances for the batched sweep) for a bounded number of steps.
 """
 from __future__ import annotations
 
@@ -141,15 +150,14 @@ def reference_rate(cases, steps: int, procs: int, timeout: float = 900.0):
     from oracle import gp_oracle as O
     if not os.path.exists(O.HARNESS_PATH):
         return None, "oracle/_ref/gp_ref_harness missing"
-    case = max(cases, key=lambda c: c.cells)
+    # one instance per process: the workload's instances in turn (a single-instance workload repeats it)
+    chosen = [cases[i % len(cases)] for i in range(procs)]
     with tempfile.TemporaryDirectory() as td:
-        case.write(td)
         ps = []
-        for i in range(procs):
+        for i, case in enumerate(chosen):
             wd = os.path.join(td, f"w{i}")
             os.makedirs(wd)
-            for f in ("Input.in", "Filling.in"):
-                os.link(os.path.join(td, f), os.path.join(wd, f))
+            case.write(wd)
             ps.append(subprocess.Popen([O.HARNESS_PATH, "Input.in", "Filling.in", "out", "-", str(steps)], cwd=wd,
                                        stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
         secs = []
@@ -160,8 +168,10 @@ def reference_rate(cases, steps: int, procs: int, timeout: float = 900.0):
                     secs.append(float(line.split()[0].split("=")[1]))
     if len(secs) != procs:
         return None, "reference harness failed"
-    rate = procs * case.cells * steps / max(secs)
-    return rate, f"{case.mesh_x}x{case.mesh_y}, {steps} steps per process, {procs} processes (one per core)"
+    rate = sum(c.cells for c in chosen) * steps / max(secs)
+    sides = sorted({f"{c.mesh_x}x{c.mesh_y}" for c in chosen})
+    return rate, (f"{procs} processes (one per core), one instance each ({', '.join(sides)}), "
+                  f"{steps} steps per process; rate = cells x steps / slowest process")
 
 
 def run_reference_arm(args, world, rank):
@@ -216,6 +226,7 @@ def timed_single(ctx, steps, warmup, flush, stream):
     torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     l0 = ctx.launches
+    torch.cuda.nvtx.range_push("timed")  # lets a profiler select the timed launches
     for i in range(steps):
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -225,7 +236,47 @@ def timed_single(ctx, steps, warmup, flush, stream):
             evs[i][1].record(stream)
     ctx.sync()
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     return sum(a.elapsed_time(b) for a, b in evs), ctx.launches - l0
+
+
+def traffic_table():
+    """Per-launch DRAM bytes of the step kernels measured by ncu on the bench
+    workloads (profiles/dram_traffic.txt: "<workload> <kernel> <bytes>")."""
+    t = {}
+    p = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    if os.path.exists(p):
+        for line in open(p):
+            f = line.split()
+            if len(f) == 3 and not line.startswith("#"):
+                t[(f[0], f[1])] = float(f[2])
+    return t
+
+
+def fp64_plain_rate(models, fields, steps, warmup, dev, world):
+    """FP64 plain step (bit-exact to the reference) over every instance of the
+    workload: one context per instance, K steps each bracketed by CUDA events
+    on its stream; time = sum over instances."""
+    import torch
+    import microsim_b200 as mb
+    total_ms, cells = 0.0, 0
+    for m, (p, u) in zip(models, fields):
+        with mb.Context(m, mb.GP_FP64) as c:
+            c.upload(p, u)
+            c.step(warmup)
+            c.sync()
+            s = torch.cuda.ExternalStream(c.stream, device=dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(s):
+                e0.record(s)
+            c.step(steps)
+            with torch.cuda.stream(s):
+                e1.record(s)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            cells += m.mesh_x * m.mesh_y
+    total_ms = allmax(total_ms, world)
+    return {"value": world * cells * steps / (total_ms / 1e3), "unit": UNIT, "ms_per_step": total_ms / steps}
 
 
 def run_ours(args, world, rank, local):
@@ -242,60 +293,70 @@ def run_ours(args, world, rank, local):
     cells = sum(m.mesh_x * m.mesh_y for m in models)
     N, K1 = models[0].N, models[0].K1
     peak, peak_kind = measured_peaks()
-    fp64 = None
-    tile = None
     barrier(world)
-    if len(models) == 1:
-        m = models[0]
-        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-        prec = mb.GP_FP32 if args.precision == "fp32" else mb.GP_FP64
-        ctx = mb.Context(m, prec)
-        ctx.upload(*fields[0])
-        stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
-        with ClockSampler(local) as clk:
+
+    # ---- the chosen form (FP32 batch: narrow band, CUDA-graph replay)
+    ctx = mb.Batch(models)
+    for i, f in enumerate(fields):
+        ctx.upload(i, *f)
+    tile = ctx.autotune(None) if not args.no_autotune else (16, 32)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    state_mb = cells * (N + K1) * 4 / 1e6
+    with ClockSampler(local) as clk:
+        if state_mb < 300:  # would stay L2-resident: flush between steps, per-step events
+            flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
             ms, launches = timed_single(ctx, args.steps, args.warmup, flush, stream)
-        l2 = "flushed between timed steps (256 MiB write outside the events)"
-        if prec == mb.GP_FP32 and not args.no_fp64:
-            c64 = mb.Context(m, mb.GP_FP64)
-            c64.upload(*fields[0])
-            s64 = torch.cuda.ExternalStream(c64.stream, device=dev)
-            ms64, _ = timed_single(c64, args.steps, args.warmup, flush, s64)
-            c64.close()
-            ms64 = allmax(ms64, world)
-            fp64 = {"value": world * cells * args.steps / (ms64 / 1e3), "unit": UNIT,
-                    "ms_per_step": ms64 / args.steps}
-    else:
-        prec = mb.GP_FP32
-        ctx = mb.Batch(models)
-        for i, f in enumerate(fields):
-            ctx.upload(i, *f)
-        tile = ctx.autotune(None) if not args.no_autotune else None
-        stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
-        ctx.step(args.warmup)
-        ctx.sync()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        l0 = ctx.launches
-        with ClockSampler(local) as clk:
+            l2 = "flushed between timed steps (256 MiB write outside the events)"
+        else:
+            ctx.step(args.warmup)
+            ctx.sync()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = ctx.launches
+            torch.cuda.nvtx.range_push("timed")  # lets a profiler select the timed launches
             with torch.cuda.stream(stream):
                 e0.record(stream)
             ctx.step(args.steps)
             with torch.cuda.stream(stream):
                 e1.record(stream)
             ctx.sync()
-        launches = ctx.launches - l0
-        ms = e0.elapsed_time(e1)
-        l2 = "inputs larger than L2 (state %.0f MB per buffer)" % (cells * (N + K1) * 4 / 1e6)
+            torch.cuda.nvtx.range_pop()
+            launches = ctx.launches - l0
+            ms = e0.elapsed_time(e1)
+            l2 = "inputs larger than L2 (state %.0f MB per buffer)" % state_mb
     torch.cuda.synchronize()
     barrier(world)
     ms = allmax(ms, world)
     step_ms = ms / args.steps
     value = world * cells * args.steps / (ms / 1e3)
-    esize = 4 if prec == mb.GP_FP32 else 8
-    alg_bytes = 2 * (N + K1) * esize
-    achieved = cells / (step_ms / 1e3) * alg_bytes / 1e9
 
-    # end to end through the C ABI: pinned host state in, K steps with the
+    # ---- per-kernel CUDA-event timing of the same steps (direct launches)
+    lean_tiles, tiles, lean_cells = ctx.lean_stats()
+    ctx.set_timing(True)
+    ctx.step(args.steps)
+    kt = ctx.kernel_ms()
+    ctx.set_timing(False)
+    gen_cells = cells - lean_cells
+    kernels = {
+        "k_lean32": {"ms": kt["lean"], "bytes": lean_cells * 2 * K1 * 4,
+                     "what": f"mu read + write of the {lean_tiles} lean tiles ({2 * K1 * 4} B/cell)"},
+        "k_step32": {"ms": kt["general"], "bytes": gen_cells * 2 * (N + K1) * 4,
+                     "what": f"phi, mu read + write of the {tiles - lean_tiles} other tiles "
+                             f"({2 * (N + K1) * 4} B/cell)"},
+        "k_general_list": {"ms": kt["list"], "bytes": tiles * 4 * 9, "what": "purity words"},
+    }
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    d = kernels[dom]
+    achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9 if d["ms"] > 0 else None
+    traffic = traffic_table().get((args.workload, dom))
+    esize = 4
+    alg_bytes = 2 * (N + K1) * esize
+
+    # ---- FP64 plain on the same workload
+    fp64 = None
+    if not args.no_fp64:
+        fp64 = fp64_plain_rate(models, fields, max(3, min(args.steps, 10)), 1, dev, world)
+
+    # ---- end to end through the C ABI: pinned host state in, K steps with the
     # progress statistics read back each step, state out
     pinned = []
     for p, u in fields:
@@ -308,20 +369,13 @@ def run_ours(args, world, rank, local):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         e0.record(stream)
-    if len(models) == 1:
-        ctx.upload(*pinned[0])
-        for _ in range(args.steps):
-            ctx.step(1)
-            ctx.stats(allow_nonfinite=True)
-        ctx.download()
-    else:
-        for i, (p, u) in enumerate(pinned):
-            ctx.upload(i, p, u)
-        for _ in range(args.steps):
-            ctx.step(1)
-            ctx.stats(0, allow_nonfinite=True)
-        for i in range(len(models)):
-            ctx.download(i)
+    for i, (p, u) in enumerate(pinned):
+        ctx.upload(i, p, u)
+    for _ in range(args.steps):
+        ctx.step(1)
+        ctx.stats(0, allow_nonfinite=True)
+    for i in range(len(models)):
+        ctx.download(i)
     with torch.cuda.stream(stream):
         e1.record(stream)
     e1.synchronize()
@@ -340,15 +394,22 @@ def run_ours(args, world, rank, local):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if prec == mb.GP_FP32 else "f64", "data": "synthetic",
-            "config": {"workload": wname, "precision": args.precision if len(models) == 1 else "fp32",
-                       "instances": len(models), "cells_per_gpu": cells, "state_prepared_steps": prep,
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wname, "precision": "fp32", "instances": len(models), "cells_per_gpu": cells,
+                       "state_prepared_steps": prep,
                        "parallelism": f"replicas{world}" if world > 1 else "single", "l2": l2,
-                       "tile": list(tile) if len(models) > 1 and tile else [16, 32]},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "note": f"algorithmic {alg_bytes} B/cell-update (read+write phi, mu once) per "
-                                 f"launch of the fused step kernel; peak {peak_kind}"},
+                       "tile": list(tile), "lean_tiles": lean_tiles, "tiles": tiles},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None, "traffic": traffic,
+                         "bytes_per_launch": d["bytes"], "ms_per_launch": d["ms"],
+                         "note": f"dominant kernel {dom}: algorithmic bytes = {d['what']} / its mean CUDA-event "
+                                 f"duration; peak {peak_kind}; traffic = ncu dram bytes per launch "
+                                 f"(profiles/dram_traffic.txt)"},
+            "step_roofline": {"alg_bytes_per_cell": alg_bytes, "achieved": value / world * alg_bytes / 1e9,
+                              "frac": value / world * alg_bytes / 1e9 / peak,
+                              "note": "dense-step definition: read+write phi and mu once per cell-update; the "
+                                      "narrow band skips phi traffic of pure tiles, so this can exceed 1"},
+            "kernels_ms_per_step": {k: v["ms"] for k, v in kernels.items()},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": state_bytes / args.steps + 64 * 8},
@@ -367,9 +428,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c4"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--ref-steps", type=int, default=3)
+    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c4"])
+    ap.add_argument("--ref-steps", type=int, default=50)
     ap.add_argument("--prep-steps", type=int, default=-1,
                     help="steps of the FP32 form run before timing to reach a mid-run state (-1: half the run)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -192,9 +192,17 @@ int gp_batch_set_tile(gp_batch *b, int tx, int ty);
  * step) take a lean diffusion-only kernel, the rest the full kernel, both
  * launched concurrently; the results are bit-identical with it off. */
 int gp_batch_set_narrowband(gp_batch *b, int on);
-/* Tiles the next step sends to the lean kernel, and all tiles of the batch
- * (diagnostics; synchronises the batch's stream). */
-int gp_batch_lean_tiles(gp_batch *b, int64_t *lean, int64_t *total);
+/* Tiles the next step sends to the lean kernel, all tiles of the batch, and
+ * the interior cells of those lean tiles (diagnostics; synchronises the
+ * batch's stream). */
+int gp_batch_lean_tiles(gp_batch *b, int64_t *lean, int64_t *total, int64_t *lean_cells);
+/* Per-kernel timing (diagnostics): while on, steps launch directly (no graph
+ * replay), their kernels one after the other on the batch's stream, and record
+ * CUDA events around each kernel; gp_batch_kernel_ms gives
+ * the mean milliseconds per step of the lean kernel, the list kernel and the
+ * full kernel (ms3[0..2]) over the steps since timing was switched on. */
+int gp_batch_set_timing(gp_batch *b, int on);
+int gp_batch_kernel_ms(gp_batch *b, double *ms3, int64_t *steps);
 /* Measured sweep over the tile shapes on the batch's own state (restored
  * afterwards); the winner is cached in cache_path (may be NULL) per batch
  * signature and read back on the next call. */

@@ -109,7 +109,10 @@ _SIGS = {
     "gp_batch_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(GpStats)]),
     "gp_batch_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gp_batch_set_narrowband": (C.c_int, [C.c_void_p, C.c_int]),
-    "gp_batch_lean_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "gp_batch_lean_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_int64)]),
+    "gp_batch_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_batch_kernel_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "gp_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "gp_batch_stream": (C.c_void_p, [C.c_void_p]),
     "gp_batch_launch_count": (C.c_int64, [C.c_void_p]),
@@ -337,9 +340,25 @@ class Batch:
 
     def lean_tiles(self):
         """(tiles the next step updates with the lean kernel, all tiles)."""
-        lean, total = C.c_int64(), C.c_int64()
-        _check("gp_batch_lean_tiles", lib().gp_batch_lean_tiles(self._h, C.byref(lean), C.byref(total)))
-        return lean.value, total.value
+        return self.lean_stats()[:2]
+
+    def lean_stats(self):
+        """(lean tiles of the next step, all tiles, interior cells of the lean tiles)."""
+        lean, total, cells = C.c_int64(), C.c_int64(), C.c_int64()
+        _check("gp_batch_lean_tiles",
+               lib().gp_batch_lean_tiles(self._h, C.byref(lean), C.byref(total), C.byref(cells)))
+        return lean.value, total.value, cells.value
+
+    def set_timing(self, on: bool):
+        """Per-kernel CUDA-event timing of every step (steps launch directly while on)."""
+        _check("gp_batch_set_timing", lib().gp_batch_set_timing(self._h, 1 if on else 0))
+
+    def kernel_ms(self):
+        """Mean ms per step of the lean, list and full kernels since timing was switched on."""
+        ms = (C.c_double * 3)()
+        n = C.c_int64()
+        _check("gp_batch_kernel_ms", lib().gp_batch_kernel_ms(self._h, ms, C.byref(n)))
+        return {"lean": ms[0], "list": ms[1], "general": ms[2], "steps": n.value}
 
     def autotune(self, cache_path: str | None = None):
         tx, ty = C.c_int(), C.c_int()

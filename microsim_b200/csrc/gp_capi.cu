@@ -29,7 +29,11 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty);
 int gp_f32_batch_tiles(const gp_f32_batch* b);
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s);
 cudaError_t gp_f32_batch_invalidate(gp_f32_batch* b, cudaStream_t s);
-cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s, int64_t* lean);
+cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s, int64_t* lean,
+                                    int64_t* lean_cells);
+cudaError_t gp_f32_batch_set_timing(gp_f32_batch* b, int on);
+cudaError_t gp_f32_batch_kernel_ms(gp_f32_batch* b, double* ms, int64_t* steps);
+int gp_f32_batch_timing(const gp_f32_batch* b);
 void gp_f32_batch_set_narrowband(gp_f32_batch* b, int on);
 int gp_f32_batch_launches_per_step(const gp_f32_batch* b);
 int gp_f32_tile_shape_count();
@@ -606,7 +610,7 @@ static int batch_capture(gp_batch* b, int parity) {
 
 extern "C" int gp_batch_step(gp_batch* b, int64_t nsteps) {
   if (!b || nsteps < 0) return GP_E_ARG;
-  while (nsteps >= b->graph_steps) {
+  while (nsteps >= b->graph_steps && !gp_f32_batch_timing(b->f32)) {  // timed steps launch directly
     if (!b->graph[b->parity]) {
       int rc = batch_capture(b, b->parity);
       if (rc != GP_OK) return rc;
@@ -760,10 +764,24 @@ extern "C" int gp_batch_set_narrowband(gp_batch* b, int on) {
   return GP_OK;
 }
 
-extern "C" int gp_batch_lean_tiles(gp_batch* b, int64_t* lean, int64_t* total) {
-  if (!b || !lean || !total) return GP_E_ARG;
-  GP_CUDA(gp_f32_batch_lean_tiles(b->f32, b->parity, b->stream, lean));
+extern "C" int gp_batch_lean_tiles(gp_batch* b, int64_t* lean, int64_t* total, int64_t* lean_cells) {
+  if (!b || !lean || !total || !lean_cells) return GP_E_ARG;
+  GP_CUDA(gp_f32_batch_lean_tiles(b->f32, b->parity, b->stream, lean, lean_cells));
   *total = gp_f32_batch_tiles(b->f32);
+  return GP_OK;
+}
+
+extern "C" int gp_batch_set_timing(gp_batch* b, int on) {
+  if (!b) return GP_E_ARG;
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  GP_CUDA(gp_f32_batch_set_timing(b->f32, on));
+  batch_drop_graphs(b);
+  return GP_OK;
+}
+
+extern "C" int gp_batch_kernel_ms(gp_batch* b, double* ms3, int64_t* steps) {
+  if (!b || !ms3 || !steps) return GP_E_ARG;
+  GP_CUDA(gp_f32_batch_kernel_ms(b->f32, ms3, steps));
   return GP_OK;
 }
 

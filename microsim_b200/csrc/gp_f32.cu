@@ -1401,6 +1401,12 @@ struct gp_f32_batch {
   int grid_general = 0, grid_lean = 0;
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // per-kernel timing (off by default): a ring of event sets, one per step
+  static constexpr int kTimingSlots = 64;
+  int timing = 0, tn = 0, tdone = 0;
+  std::vector<cudaEvent_t> tev;  // [kTimingSlots][5]: lean start/end, list start, general start/end
+  double tms[3] = {0, 0, 0};     // accumulated lean, list, general milliseconds
+  int64_t tsteps = 0;
 };
 
 void gp_f32_batch_destroy(gp_f32_batch* b);
@@ -1456,6 +1462,7 @@ void gp_f32_batch_destroy(gp_f32_batch* b) {
   cudaFree(b->dinst[1]);
   free_tiles(b);
   cudaFree(b->dcnt);
+  for (cudaEvent_t ev : b->tev) cudaEventDestroy(ev);
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->ev_join) cudaEventDestroy(b->ev_join);
   if (b->side) cudaStreamDestroy(b->side);
@@ -1537,49 +1544,127 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
 
 int gp_f32_batch_tiles(const gp_f32_batch* b) { return b->total_tiles; }
 
+// Fold the event times of timing slot `slot` into the totals.
+static cudaError_t timing_collect(gp_f32_batch* b, int slot) {
+  cudaEvent_t* E = &b->tev[5 * slot];
+  cudaError_t e = cudaEventSynchronize(E[4]);
+  if (e == cudaSuccess) e = cudaEventSynchronize(E[1]);
+  if (e != cudaSuccess) return e;
+  float lean = 0.f, list = 0.f, gen = 0.f;
+  if (b->narrowband) {
+    cudaEventElapsedTime(&lean, E[0], E[1]);
+    cudaEventElapsedTime(&list, E[2], E[3]);
+  }
+  cudaEventElapsedTime(&gen, E[3], E[4]);
+  b->tms[0] += lean;
+  b->tms[1] += list;
+  b->tms[2] += gen;
+  b->tsteps++;
+  return cudaSuccess;
+}
+
+// Per-kernel timing: while on, every step records events around its kernels.
+cudaError_t gp_f32_batch_set_timing(gp_f32_batch* b, int on) {
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return e;
+  if (on && b->tev.empty()) {
+    b->tev.resize(5 * gp_f32_batch::kTimingSlots);
+    for (cudaEvent_t& ev : b->tev)
+      if ((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
+  }
+  b->timing = on ? 1 : 0;
+  b->tn = b->tdone = 0;
+  b->tms[0] = b->tms[1] = b->tms[2] = 0.0;
+  b->tsteps = 0;
+  return cudaSuccess;
+}
+
+// Mean milliseconds per step of the lean kernel, the list kernel and the full
+// kernel over the steps timed since timing was switched on.
+cudaError_t gp_f32_batch_kernel_ms(gp_f32_batch* b, double* ms, int64_t* steps) {
+  for (; b->tdone < b->tn; b->tdone++) {
+    cudaError_t e = timing_collect(b, b->tdone % gp_f32_batch::kTimingSlots);
+    if (e != cudaSuccess) return e;
+  }
+  for (int i = 0; i < 3; i++) ms[i] = b->tsteps ? b->tms[i] / (double)b->tsteps : 0.0;
+  *steps = b->tsteps;
+  return cudaSuccess;
+}
+
 // One step of every instance, reading buffer parity `parity`.
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   const KernelSet& k = b->ks;
   const int p = parity & 1;
   const uint32_t* flags_in = b->dflags + (size_t)p * b->total_tiles;
   uint32_t* flags_out = b->dflags + (size_t)(p ^ 1) * b->total_tiles;
+  cudaEvent_t* E = nullptr;
+  cudaError_t e;
+  if (b->timing) {
+    if (b->tn - b->tdone == gp_f32_batch::kTimingSlots) {  // ring full: fold the oldest slot first
+      if ((e = timing_collect(b, b->tdone % gp_f32_batch::kTimingSlots)) != cudaSuccess) return e;
+      b->tdone++;
+    }
+    E = &b->tev[5 * (b->tn++ % gp_f32_batch::kTimingSlots)];
+  }
   if (!b->narrowband) {
+    if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
     k.general<<<b->total_tiles, 256, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr,
                                                           flags_out);
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (E) {
+      if ((e = cudaEventRecord(E[4], s)) != cudaSuccess) return e;
+      if ((e = cudaEventRecord(E[1], s)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
   }
-  // the lean tiles (side stream) and the rest run concurrently: disjoint tiles and words
-  cudaError_t e;
-  if ((e = cudaEventRecord(b->ev_fork, s)) != cudaSuccess) return e;
-  if ((e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess) return e;
-  k.lean<<<b->grid_lean, 128, k.smem_lean, b->side>>>(b->dinst[p], b->dmodel, b->dtile_inst, flags_in, flags_out,
-                                            b->total_tiles);
+  // the lean tiles (side stream) and the rest run concurrently: disjoint tiles and words;
+  // timed steps run them one after the other on `s` so that each kernel's events bracket it alone
+  cudaStream_t ls = E ? s : b->side;
+  if (!E) {
+    if ((e = cudaEventRecord(b->ev_fork, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess) return e;
+  }
+  if (E && ((e = cudaEventRecord(E[0], ls)) != cudaSuccess)) return e;
+  k.lean<<<b->grid_lean, 128, k.smem_lean, ls>>>(b->dinst[p], b->dmodel, b->dtile_inst, flags_in, flags_out,
+                                                 b->total_tiles);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (E && ((e = cudaEventRecord(E[1], ls)) != cudaSuccess)) return e;
+  if (E && ((e = cudaEventRecord(E[2], s)) != cudaSuccess)) return e;
   k.list<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dinst[p], b->dtile_inst, flags_in, b->total_tiles, b->dglist,
                                                       b->dcnt);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
   k.general<<<b->grid_general, 256, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, b->dglist, b->dcnt,
                                                          flags_out);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (E) return cudaEventRecord(E[4], s);
   if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess) return e;
   return cudaStreamWaitEvent(s, b->ev_join, 0);
 }
 
+int gp_f32_batch_timing(const gp_f32_batch* b) { return b->timing; }
+
 // Tiles the next step (reading buffer parity `parity`) sends to the lean
 // kernel: lean_phase evaluated on the host over a copy of the purity words.
-cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s, int64_t* lean) {
+cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s, int64_t* lean,
+                                    int64_t* lean_cells) {
   std::vector<uint32_t> F(b->total_tiles);
   cudaError_t e = cudaMemcpyAsync(F.data(), b->dflags + (size_t)(parity & 1) * b->total_tiles,
                                   sizeof(uint32_t) * F.size(), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return e;
-  int64_t n = 0;
-  for (int i = 0; i < b->n; i++) {
+  int64_t n = 0, c = 0;
+  for (int i = 0; i < b->n && b->narrowband; i++) {
     const Inst& I = b->hinst[parity & 1][i];
     for (int t = I.tile_begin; t < I.tile_begin + I.tiles_x * I.tiles_y; t++)
-      n += b->narrowband && lean_phase(F.data(), I, t, b->tx, b->ty) >= 0;
+      if (lean_phase(F.data(), I, t, b->tx, b->ty) >= 0) {
+        const int lt = t - I.tile_begin, x0 = (lt / I.tiles_y) * b->tx, y0 = (lt % I.tiles_y) * b->ty;
+        n++;
+        c += (int64_t)(I.mx - x0 < b->tx ? I.mx - x0 : b->tx) * (I.my - y0 < b->ty ? I.my - y0 : b->ty);
+      }
   }
   *lean = n;
+  *lean_cells = c;
   return cudaSuccess;
 }
 
