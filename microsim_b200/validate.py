@@ -1,12 +1,22 @@
-"""FP32 chosen form against the FP64 plain form on one workload.
+"""FP32 chosen form against the FP64 plain form, per workload.
 
-    python -m microsim_b200.validate [--mesh 1024] [--steps 50000] [--every 1000]
+    python -m microsim_b200.validate [--workload c2|c4|c1|c3] [--steps S] [--every E] [--mesh M]
 
-Runs the corner dendrite of the 1024^2 workload (4-fold, delta = 0.02,
-supersaturation 0.55, growing-gap variant) in both forms, samples the tip
-position, tip radius, solute mass and solid fraction every `every` steps, and
-prints the relative errors of the FP32 form: tip velocity (least-squares slope
-over the last fifth of the run), final tip position and radius, solute mass.
+Runs each instance of the workload in both forms (the FP32 form through the
+batch API, narrow band on; the FP64 plain form one context per instance),
+samples every `every` steps the tip position along the growth axis through the
+seed (phi_solid = 0.5 crossing), the tip radius (corner dendrites), the FP64
+solute mass and the phase fractions, and prints the relative differences of
+the FP32 form:
+  * tip velocity: least-squares slope of the tip position over the last fifth
+    of the run (restating resources/PP_tools/frontvelocity.py);
+  * final tip position and radius (resources/PP_tools/tipradius.py);
+  * solute mass and phase fractions at the end.
+Workloads: c2 the 1024^2 corner dendrite (50,000 steps), c4 the 256-instance
+batched sweep (5,000 steps), c1 the 200^2 centred seed (10,000 steps), c3 the
+2048^2 four-phase ternary (20,000 steps; no single tip: phase fractions and
+solute mass only).  The growing-gap variants of the configs are used
+(microsim_b200/configs.py).
 """
 from __future__ import annotations
 
@@ -16,50 +26,112 @@ import time
 
 import numpy as np
 
-from . import GP_FP32, GP_FP64, Context, analysis as A, configs, load_case
+from . import GP_FP32, GP_FP64, Batch, Context, analysis as A, configs, load_case
 
 
-def run(mesh: int = 1024, steps: int = 50000, every: int = 1000, precision: int = GP_FP64):
-    case = configs.c2(literal=False, steps=steps, mesh=mesh)
-    m, phi, mu = load_case(case)
-    rec = []
-    with Context(m, precision) as c:
-        c.upload(phi, mu)
+def _sample(m, p, st, line):
+    tip = A.tip_position(p[0], 0, line)
+    rad = A.tip_radius(p[0], 0) if line == 0 else float("nan")
+    fr = [float(p[a].mean()) for a in range(m.N)]
+    return [tip, rad, *st["solute"][: m.K1], *fr, st["nonfinite"]]
+
+
+def run_fp32(models, loaded, lines, steps, every):
+    rec = [[] for _ in models]
+    with Batch(models) as b:
+        for i, (_, p, u) in enumerate(loaded):
+            b.upload(i, p, u)
         for s in range(every, steps + 1, every):
-            c.step(every)
-            p, _ = c.download()
-            st = c.stats(allow_nonfinite=True)
-            rec.append([s, A.tip_position(p[0], 0), A.tip_position(p[0], 1), A.tip_radius(p[0], 0),
-                        st["solute"][0], A.solid_fraction(p), st["nonfinite"]])
-    return m, np.array(rec)
+            b.step(every)
+            for i, m in enumerate(models):
+                p, _ = b.download(i)
+                rec[i].append([s, *_sample(m, p, b.stats(i, allow_nonfinite=True), lines[i])])
+    return [np.array(r) for r in rec]
 
 
-def compare(mesh: int = 1024, steps: int = 50000, every: int = 1000) -> dict:
+def run_fp64(models, loaded, lines, steps, every):
+    out = []
+    for (m, phi, mu), line in zip(loaded, lines):
+        rec = []
+        with Context(m, GP_FP64) as c:
+            c.upload(phi, mu)
+            for s in range(every, steps + 1, every):
+                c.step(every)
+                p, _ = c.download()
+                rec.append([s, *_sample(m, p, c.stats(allow_nonfinite=True), line)])
+        out.append(np.array(rec))
+    return out
+
+
+def _rel(a, b):
+    return float(abs(a - b) / abs(b)) if b != 0 else float(abs(a - b))
+
+
+def compare(workload: str = "c2", steps: int | None = None, every: int | None = None, mesh: int | None = None,
+            instances: int | None = None) -> dict:
     t0 = time.time()
-    m, f32 = run(mesh, steps, every, GP_FP32)
-    _, f64 = run(mesh, steps, every, GP_FP64)
-    w = max(3, len(f64) // 5)
-    v64 = A.velocity(f64[:, 0] * m.dt, f64[:, 1], w)
-    v32 = A.velocity(f32[:, 0] * m.dt, f32[:, 1], w)
-    return {
-        "mesh": mesh, "steps": steps, "every": every,
-        "tip_velocity_fp64": v64, "tip_velocity_fp32": v32,
-        "tip_velocity_rel_err": abs(v32 - v64) / abs(v64),
-        "tip_position_rel_err": abs(f32[-1, 1] - f64[-1, 1]) / f64[-1, 1],
-        "tip_radius_rel_err": abs(f32[-1, 3] - f64[-1, 3]) / f64[-1, 3],
-        "solute_rel_diff": abs(f32[-1, 4] - f64[-1, 4]) / abs(f64[-1, 4]),
-        "solid_fraction_fp64": f64[-1, 5], "nonfinite": int(f32[:, 6].max() + f64[:, 6].max()),
-        "wall_s": time.time() - t0,
-    }
+    if workload == "c2":
+        steps, every = steps or 50000, every or 1000
+        cases = [configs.c2(literal=False, steps=steps, mesh=mesh or 1024)]
+    elif workload == "c4":
+        steps, every = steps or 5000, every or 250
+        cases = configs.c4(steps=steps)[: instances or 256]
+    elif workload == "c1":
+        steps, every = steps or 10000, every or 500
+        cases = [configs.c1(literal=False, steps=steps)]
+    elif workload == "c3":
+        steps, every = steps or 20000, every or 1000
+        cases = [configs.c3(steps=steps, mesh=mesh or 2048)]
+    else:
+        raise ValueError(workload)
+    loaded = [load_case(c) for c in cases]
+    models = [m for m, _, _ in loaded]
+    lines = [0 if (c.fills[0][1][1] == 0 and c.fills[0][1][2] == 0) else int(c.fills[0][1][2]) for c in cases]
+    f32 = run_fp32(models, loaded, lines, steps, every)
+    f64 = run_fp64(models, loaded, lines, steps, every)
+    per = []
+    for m, a, b in zip(models, f32, f64):
+        K1, N = m.K1, m.N
+        w = max(3, len(b) // 5)
+        r = {"solute_rel_diff": max(_rel(a[-1, 3 + k], b[-1, 3 + k]) for k in range(K1)),
+             "phase_fraction_abs_diff": float(np.abs(a[-1, 3 + K1:3 + K1 + N] - b[-1, 3 + K1:3 + K1 + N]).max()),
+             "nonfinite": int(a[:, -1].max() + b[:, -1].max())}
+        if workload != "c3":
+            v64 = A.velocity(b[:, 0] * m.dt, b[:, 1], w)
+            v32 = A.velocity(a[:, 0] * m.dt, a[:, 1], w)
+            r.update({"tip_velocity_fp64": v64, "tip_velocity_fp32": v32, "tip_velocity_rel_err": _rel(v32, v64),
+                      "tip_position_rel_err": _rel(a[-1, 1], b[-1, 1])})
+            if not np.isnan(b[-1, 2]):
+                r["tip_radius_rel_err"] = _rel(a[-1, 2], b[-1, 2])
+        per.append(r)
+    out = {"workload": workload, "instances": len(models), "steps": steps, "every": every,
+           "wall_s": time.time() - t0}
+    if len(models) == 1:
+        m = models[0]
+        out["phase_fraction_fp64"] = [float(v) for v in f64[0][-1, 3 + m.K1:3 + m.K1 + m.N]]
+        out["phase_fraction_fp64_start"] = [float(v) for v in f64[0][0, 3 + m.K1:3 + m.K1 + m.N]]
+    keys = sorted({k for r in per for k in r})
+    for k in keys:
+        vals = [r[k] for r in per if k in r and not (isinstance(r[k], float) and np.isnan(r[k]))]
+        if not vals:
+            continue
+        if len(per) == 1:
+            out[k] = vals[0]
+        else:
+            out[k + "_max"] = max(vals)
+            out[k + "_median"] = float(np.median(vals))
+    return out
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mesh", type=int, default=1024)
-    ap.add_argument("--steps", type=int, default=50000)
-    ap.add_argument("--every", type=int, default=1000)
+    ap.add_argument("--workload", default="c2", choices=["c2", "c4", "c1", "c3"])
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--every", type=int, default=None)
+    ap.add_argument("--mesh", type=int, default=None)
+    ap.add_argument("--instances", type=int, default=None)
     a = ap.parse_args()
-    print(json.dumps(compare(a.mesh, a.steps, a.every)))
+    print(json.dumps(compare(a.workload, a.steps, a.every, a.mesh, a.instances)))
 
 
 if __name__ == "__main__":
