@@ -232,6 +232,31 @@ size_t gp_model_sizeof(void);
 /* Text of the last error on this thread. */
 const char *gp_last_error(void);
 
+/* ---- adjoint of the explicit step (binary alloys: N = 2, K-1 = 1) ----------
+ * No counterpart in the reference (it has no adjoint).  A hand-written reverse
+ * of the plain step's model in FP32 (GP_FP32) or FP64 (GP_FP64), with
+ * checkpointing: gp_adj_forward runs nsteps steps from (phi0, mu0), keeping
+ * every checkpoint_every-th state (0: ceil(sqrt(nsteps))), and returns the final
+ * state; gp_adj_backward takes the adjoint of a loss with respect to that final
+ * state (lam_phi [2][mesh_x][mesh_y], lam_mu [mesh_x][mesh_y] or NULL for 0)
+ * and returns the gradient with respect to the GP_ADJ_NPARAM parameters
+ *   grad[0]  mobility M = 1/tau_ab[0][1] (tau scaled with it)
+ *   grad[1]  anisotropy strength dab[0][1]
+ *   grad[2]  interface energy Gamma[0][1]
+ *   grad[3]  liquid diffusivity Diff[1][0][0]
+ * and, when lam_phi0 / lam_mu0 are not NULL, with respect to the initial state.
+ * The segment of checkpoint_every steps is recomputed before it is reversed, so
+ * ceil(nsteps / checkpoint_every) + checkpoint_every states are stored. */
+#define GP_ADJ_NPARAM 4
+typedef struct gp_adj gp_adj;
+int gp_adj_create(const gp_model *m, int precision, gp_adj **out);
+int gp_adj_forward(gp_adj *a, const double *phi0, const double *mu0, int64_t nsteps, int64_t checkpoint_every,
+                   double *phi_out, double *mu_out);
+int gp_adj_backward(gp_adj *a, const double *lam_phi, const double *lam_mu, double *grad, double *lam_phi0,
+                    double *lam_mu0);
+int gp_adj_stored_states(const gp_adj *a, int64_t *states);
+int gp_adj_destroy(gp_adj *a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -118,6 +118,12 @@ _SIGS = {
     "gp_batch_launch_count": (C.c_int64, [C.c_void_p]),
     "gp_batch_cells": (C.c_int64, [C.c_void_p]),
     "gp_last_error": (C.c_char_p, []),
+    "gp_adj_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "gp_adj_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
+                                 C.c_void_p]),
+    "gp_adj_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gp_adj_stored_states": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "gp_adj_destroy": (C.c_int, [C.c_void_p]),
 }
 
 
