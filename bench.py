@@ -21,8 +21,10 @@ outside the events; the batched sweep (301 MB per buffer) is larger than L2
 and is timed as one graph-replayed run.  The same K steps are then replayed
 with per-kernel CUDA events (direct launches) for the roofline of the dominant
 kernel, and the FP64 plain step is timed on the same workload.  Multi-GPU
-(torchrun): every rank runs its own replica of the workload (instances do not
-exchange data), barrier before and after, max over ranks.
+(torchrun): every rank runs its own batch of the sweep (distinct instances,
+drawn from the rank's seed; a single-instance workload is replicated), no
+data-path collective, barrier before and after, max over ranks of the time,
+sum over ranks of the cells (microsim_b200/ranks.py).
 
 The reference arm (--impl reference) times the reference serial solver,
 compiled from its own sources (oracle/_ref/gp_ref_harness), on the host's
@@ -58,15 +60,9 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def workload(name: str):
-    from microsim_b200 import configs
-    if name == "c2":
-        return "dendrite_1024x1024_delta0.02_supersat0.55 (growing gap)", [configs.c2(literal=False, steps=50000)]
-    if name == "c1":
-        return "isotropic_200x200_seed10 (growing gap)", [configs.c1(literal=False, steps=10000)]
-    if name == "c4":
-        return "batched_sweep_256_instances_128-512", configs.c4()
-    raise SystemExit("unknown workload " + name)
+def workload(name: str, rank: int = 0, world: int = 1):
+    from microsim_b200 import ranks
+    return ranks.shard_workload(name, rank, world)
 
 
 class ClockSampler:
@@ -127,13 +123,13 @@ def dist_setup():
 
 
 def allmax(v: float, world: int) -> float:
-    if world == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from microsim_b200 import ranks
+    return ranks.allreduce(v, world, "max")
+
+
+def allsum(v: float, world: int) -> float:
+    from microsim_b200 import ranks
+    return ranks.allreduce(v, world, "sum")
 
 
 def barrier(world: int):
@@ -276,7 +272,7 @@ def fp64_plain_rate(models, fields, steps, warmup, dev, world):
             total_ms += e0.elapsed_time(e1)
             cells += m.mesh_x * m.mesh_y
     total_ms = allmax(total_ms, world)
-    return {"value": world * cells * steps / (total_ms / 1e3), "unit": UNIT, "ms_per_step": total_ms / steps}
+    return {"value": allsum(cells, world) * steps / (total_ms / 1e3), "unit": UNIT, "ms_per_step": total_ms / steps}
 
 
 def run_ours(args, world, rank, local):
@@ -285,7 +281,7 @@ def run_ours(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    wname, cases = workload(args.workload)
+    wname, cases = workload(args.workload, rank, world)
     loaded = [mb.load_case(c) for c in cases]
     models = [m for m, _, _ in loaded]
     prep = args.prep_steps if args.prep_steps >= 0 else {"c2": 25000, "c1": 5000, "c4": 2500}[args.workload]
@@ -327,7 +323,8 @@ def run_ours(args, world, rank, local):
     barrier(world)
     ms = allmax(ms, world)
     step_ms = ms / args.steps
-    value = world * cells * args.steps / (ms / 1e3)
+    cells_all = allsum(cells, world)  # every rank's own instances
+    value = cells_all * args.steps / (ms / 1e3)
 
     # ---- per-kernel CUDA-event timing of the same steps (direct launches)
     lean_tiles, tiles, lean_cells = ctx.lean_stats()
@@ -380,7 +377,7 @@ def run_ours(args, world, rank, local):
         e1.record(stream)
     e1.synchronize()
     e2e_ms = allmax(e0.elapsed_time(e1), world)
-    e2e = world * cells * args.steps / (e2e_ms / 1e3)
+    e2e = cells_all * args.steps / (e2e_ms / 1e3)
     state_bytes = (N + K1) * cells * 8
 
     cpu = None
@@ -397,7 +394,8 @@ def run_ours(args, world, rank, local):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": wname, "precision": "fp32", "instances": len(models), "cells_per_gpu": cells,
                        "state_prepared_steps": prep,
-                       "parallelism": f"replicas{world}" if world > 1 else "single", "l2": l2,
+                       "parallelism": (f"instances sharded over {world} ranks" if len(models) > 1 else
+                                       f"replicas{world}") if world > 1 else "single", "l2": l2,
                        "tile": list(tile), "lean_tiles": lean_tiles, "tiles": tiles},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None, "traffic": traffic,
