@@ -159,6 +159,14 @@ int gp_download(gp_ctx *ctx, double *phi, double *mu);
  * Asynchronous on the context's stream; errors of earlier launches surface here
  * or in gp_sync. */
 int gp_step(gp_ctx *ctx, int64_t nsteps);
+/* nsteps smoothing pre-steps (the reference runs NSMOOTH - 1 of them before its
+ * time loop, microsim_gp.c:97-100; solverloop.h:72-90): the phase-field step
+ * without the driving force and with isotropic gradient energy, the
+ * concentration step without antitrapping current and source, ghost fill.
+ * FP32 contexts run them in FP64 on a copy of their FP32-stored state; the
+ * bit-exact route is an FP64 context (the CLI driver smooths the filled doubles
+ * in FP64 before an FP32 time loop). */
+int gp_smooth(gp_ctx *ctx, int64_t nsteps);
 int gp_sync(gp_ctx *ctx);
 /* FP64 statistics of the current state (max/min/rel-change of the last step,
  * solute and phase sums, NaN watchdog). Synchronous. */

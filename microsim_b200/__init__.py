@@ -118,6 +118,7 @@ _SIGS = {
     "gp_batch_launch_count": (C.c_int64, [C.c_void_p]),
     "gp_batch_cells": (C.c_int64, [C.c_void_p]),
     "gp_last_error": (C.c_char_p, []),
+    "gp_smooth": (C.c_int, [C.c_void_p, C.c_int64]),
     "gp_adj_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "gp_adj_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                                  C.c_void_p]),
@@ -256,6 +257,10 @@ class Context:
 
     def step(self, nsteps: int = 1):
         _check("gp_step", lib().gp_step(self._h, int(nsteps)))
+
+    def smooth(self, nsteps: int):
+        """nsteps smoothing pre-steps (NSMOOTH - 1 in the reference's main)."""
+        _check("gp_smooth", lib().gp_smooth(self._h, int(nsteps)))
 
     def sync(self):
         _check("gp_sync", lib().gp_sync(self._h))

@@ -12,13 +12,14 @@
 #include <string.h>
 
 #include <new>
+#include <vector>
 
 #include "gp_common.cuh"
 
 extern "C" void gp_set_error(const char* fmt, ...);
 
 cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch, int64_t rplane, const double* phi,
-                        const double* mu, double* dphi, double* phi_out, double* mu_out, cudaStream_t s);
+                        const double* mu, double* dphi, double* phi_out, double* mu_out, cudaStream_t s, bool smooth = false);
 struct gp_f32_batch;
 int gp_f32_supported(const gp_model& m);
 cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** out);
@@ -278,6 +279,36 @@ extern "C" int gp_step(gp_ctx* c, int64_t nsteps) {
     c->have_prev = 1;
   }
   return GP_OK;
+}
+
+extern "C" int gp_smooth(gp_ctx* c, int64_t nsteps) {
+  if (!c || nsteps < 0) return GP_E_ARG;
+  if (nsteps == 0) return GP_OK;
+  if (c->precision == GP_FP64) {
+    for (int64_t t = 0; t < nsteps; t++) {
+      const int nxt = 1 - c->cur;
+      GP_CUDA(gp_f64_step(c->m, c->pitch, c->plane, c->rpitch, c->rplane, (const double*)c->phi[c->cur],
+                          (const double*)c->mu[c->cur], c->dphi, (double*)c->phi[nxt], (double*)c->mu[nxt],
+                          c->stream, true));
+      c->launches += 2;
+      c->cur = nxt;
+    }
+    c->have_prev = 0;
+    return GP_OK;
+  }
+  // FP32 context: the pre-steps run in FP64 on a copy of the state
+  const size_t cells = (size_t)c->m.mesh_x * c->m.mesh_y;
+  std::vector<double> phi(cells * c->m.N), mu(cells * c->m.K1);
+  int rc = gp_download(c, phi.data(), mu.data());
+  if (rc != GP_OK) return rc;
+  gp_ctx* d = nullptr;
+  rc = gp_create(&c->m, GP_FP64, &d);
+  if (rc == GP_OK) rc = gp_upload(d, phi.data(), mu.data());
+  if (rc == GP_OK) rc = gp_smooth(d, nsteps);
+  if (rc == GP_OK) rc = gp_download(d, phi.data(), mu.data());
+  if (d) gp_destroy(d);
+  if (rc == GP_OK) rc = gp_upload(c, phi.data(), mu.data());
+  return rc;
 }
 
 extern "C" int gp_sync(gp_ctx* c) {

@@ -213,8 +213,9 @@ __device__ __forceinline__ void make_grads(const gp_model& m, const double (&P)[
 //   isotropic:   functions/function_A_00.h:4-58
 //   anisotropic: functions/function_A_01.h:4-71, 101-219 with functionQ.h:4-72
 template <int N>
-__device__ __forceinline__ double grad_energy_term(const gp_model& m, const double* phi, const Grads<N>& G, int a) {
-  if (!m.anisotropy) {
+__device__ __forceinline__ double grad_energy_term(const gp_model& m, const double* phi, const Grads<N>& G, int a,
+                                                   bool iso = false) {
+  if (!m.anisotropy || iso) {
     double sum = 0.0;
 #pragma unroll
     for (int b = 0; b < N; b++) {
@@ -349,6 +350,36 @@ __device__ __forceinline__ double dwdphi(const gp_model& m, const double* phi, c
   return sum;
 }
 
+// dw/dphi of the smoothing pre-steps with anisotropy: functionW_01.h:41-62,
+// functionW_02.h:35-59 (no sign factors)
+template <int N>
+__device__ __forceinline__ double dwdphi_smooth(const gp_model& m, const double* phi, const double* divphi, int a) {
+  double sum = 0.0;
+  if (m.obstacle) {
+#pragma unroll
+    for (int b = 0; b < N; b++) {
+      if (b == a || !(fabs(divphi[b]) > 0.0)) continue;
+      sum += m.Gamma[a][b] * phi[b];
+    }
+    sum *= m.w_obstacle;
+  } else {
+#pragma unroll
+    for (int b = 0; b < N; b++) {
+      if (b == a || !(fabs(divphi[b]) > 0.0)) continue;
+      sum += 2.0 * m.Gamma[a][b] * (phi[b] * phi[b] * phi[a]);
+    }
+    sum *= 9.0;
+  }
+#pragma unroll
+  for (int b = 0; b < N; b++)
+#pragma unroll
+    for (int c = b + 1; c < N; c++) {
+      if (b == a || c == a) continue;
+      if (fabs(divphi[b]) > 0.0 && fabs(divphi[c]) > 0.0) sum += m.Gamma_abc[a][b][c] * phi[b] * phi[c];
+    }
+  return sum;
+}
+
 // functions/functionTau.h:1-16
 template <int N>
 __device__ __forceinline__ double tau_phi(const gp_model& m, const double* phi) {
@@ -404,10 +435,40 @@ __device__ __forceinline__ void project_simplex(const double* phi, const double*
   }
 }
 
+// projection of the smoothing pre-steps, solverloop/simplex_projection.h:50-91
+template <int N>
+__device__ __forceinline__ void project_simplex_unweighted(const double* phi, const double* divphi, double* dp) {
+  long count = 0;
+#pragma unroll
+  for (int a = 0; a < N; a++)
+    if ((fabs(divphi[a]) > 0.0) && (phi[a] + dp[a]) > 0.0 && (phi[a] + dp[a]) < 1.0) count++;
+  for (int a = 0; a < N; a++) {
+    if (!(fabs(divphi[a]) > 0.0)) continue;
+    if ((phi[a] + dp[a]) > 1.0) {
+      dp[a] = (1.0 - phi[a]);
+#pragma unroll
+      for (int b = 0; b < N; b++)
+        if ((fabs(divphi[b]) > 0.0) && b != a) dp[b] = -phi[b];
+      break;
+    }
+    if ((phi[a] + dp[a]) < 0.0) {
+      const double D = fabs(dp[a] + phi[a]);
+      dp[a] += D;
+#pragma unroll
+      for (int b = 0; b < N; b++)
+        if (((fabs(divphi[b]) > 0.0) && b != a) && (phi[b] + dp[b]) > 0.0 && (phi[b] + dp[b]) < 1.0)
+          dp[b] -= D / (double)(count);
+    }
+  }
+}
+
 // ---------------------------------------------------------------- kernels
 
 // Delta-phi on [-1, mx] x [-1, my] (interior plus the first ghost ring).
-template <int N, int K1>
+// SMOOTH: the smoothing pre-step (calculate_divergence_phasefield.h:63-158):
+// isotropic gradient energy, no dpsi, the unsigned potential when anisotropic,
+// unweighted projection.
+template <int N, int K1, bool SMOOTH>
 __global__ void __launch_bounds__(256) k_dphi(const __grid_constant__ gp_model m, Geo g,
                                               const double* __restrict__ phi, const double* __restrict__ mu,
                                               double* __restrict__ dphi) {
@@ -437,8 +498,12 @@ __global__ void __launch_bounds__(256) k_dphi(const __grid_constant__ gp_model m
   for (int a = 0; a < N; a++) {
     lambda[a] = 0.0;
     if (fabs(divphi[a]) > 0.0) {
-      const double t = grad_energy_term<N>(m, ph, G, a);
-      lambda[a] = m.epsilon * (t) - m.inv_eps * dwdphi<N>(m, ph, divphi, a) - dpsi<N, K1>(m, muc, ph, a);
+      const double t = grad_energy_term<N>(m, ph, G, a, SMOOTH);
+      if (SMOOTH)
+        lambda[a] = m.epsilon * (t) - m.inv_eps * (m.anisotropy ? dwdphi_smooth<N>(m, ph, divphi, a)
+                                                                : dwdphi<N>(m, ph, divphi, a));
+      else
+        lambda[a] = m.epsilon * (t) - m.inv_eps * dwdphi<N>(m, ph, divphi, a) - dpsi<N, K1>(m, muc, ph, a);
       sum_lambda += lambda[a];
       active++;
     }
@@ -450,7 +515,8 @@ __global__ void __launch_bounds__(256) k_dphi(const __grid_constant__ gp_model m
     if (fabs(divphi[a]) > 0.0) dp[a] = m.dt * (lambda[a] - sum_lambda) / (tphi * m.epsilon);
     else dp[a] = 0.0;
   }
-  project_simplex<N>(ph, divphi, dp);
+  if (SMOOTH) project_simplex_unweighted<N>(ph, divphi, dp);
+  else project_simplex<N>(ph, divphi, dp);
   double* out = dphi + (int64_t)(x + 1) * g.rpitch + (y + 1);
 #pragma unroll
   for (int a = 0; a < N; a++) out[a * g.rplane] = dp[a];
@@ -592,8 +658,10 @@ __device__ __forceinline__ void lu_inverse(double (&mm)[K][K], double (&inv)[K][
       }
 }
 
-// mu and phi update of the interior, plus the rel-change terms of the step.
-template <int N, int K1>
+// mu and phi update of the interior.  SMOOTH: the smoothing pre-step
+// (calculate_divergence_concentration.h:154-253): no antitrapping current, no
+// dh/dt source, the LU inverse (matinvnew) for every mu solve.
+template <int N, int K1, bool SMOOTH>
 __global__ void __launch_bounds__(256) k_update(const __grid_constant__ gp_model m, Geo g,
                                                 const double* __restrict__ phi, const double* __restrict__ mu,
                                                 const double* __restrict__ dphi, double* __restrict__ phi_out,
@@ -644,10 +712,13 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ gp_model
   // j_at on the four faces; the y-face at ghosted row MESH_Y-2 carries none
   // (calculate_fluxes_concentration.h:65), i.e. interior row my-5
   double jx_c[K1], jx_b[K1], jy_c[K1], jy_l[K1];
-  jat_face<N, K1>(m, gx_c, cy_c, cy_f, P[1][1], P[2][1], Mc, Mf, Dc, Df, false, jx_c);
-  jat_face<N, K1>(m, gx_b, cy_b, cy_c, P[0][1], P[1][1], Mb, Mc, Db, Dc, false, jx_b);
-  jat_face<N, K1>(m, gy_c, cx_c, cx_r, P[1][1], P[1][2], Mc, Mr, Dc, Dr, (y + 3 == g.my - 2), jy_c);
-  jat_face<N, K1>(m, gy_l, cx_l, cx_c, P[1][0], P[1][1], Ml, Mc, Dl, Dc, (y + 2 == g.my - 2) || (y + 2 == 0), jy_l);
+  if (!SMOOTH) {
+    jat_face<N, K1>(m, gx_c, cy_c, cy_f, P[1][1], P[2][1], Mc, Mf, Dc, Df, false, jx_c);
+    jat_face<N, K1>(m, gx_b, cy_b, cy_c, P[0][1], P[1][1], Mb, Mc, Db, Dc, false, jx_b);
+    jat_face<N, K1>(m, gy_c, cx_c, cx_r, P[1][1], P[1][2], Mc, Mr, Dc, Dr, (y + 3 == g.my - 2), jy_c);
+    jat_face<N, K1>(m, gy_l, cx_l, cx_c, P[1][0], P[1][1], Ml, Mc, Dl, Dc, (y + 2 == g.my - 2) || (y + 2 == 0),
+                    jy_l);
+  }
 
   const double* ph = P[1][1];
   double sum[K1], divflux[K1], divjat[K1], deltac[K1], dcdmu[K1][K1];
@@ -683,8 +754,10 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ gp_model
       divflux[k] += (Dx * gmx - Dxb * gmxb) / m.dx;
       divflux[k] += (Dy * gmy - Dyl * gmyl) / m.dy;
     }
-    divjat[k] = (jx_c[k] - jx_b[k]) * (jscale) / m.dx;
-    divjat[k] += (jy_c[k] - jy_l[k]) * (jscale) / m.dy;
+    if (!SMOOTH) {
+      divjat[k] = (jx_c[k] - jx_b[k]) * (jscale) / m.dx;
+      divjat[k] += (jy_c[k] - jy_l[k]) * (jscale) / m.dy;
+    }
   }
   int bulk = -1;
 #pragma unroll
@@ -699,7 +772,7 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ gp_model
 #pragma unroll
       for (int a = 0; a < N; a++)
         if (a == bulk) co = c_mu<K1>(m, Mc, a, k);
-      cnew[k] = co + m.dt * (divflux[k]) - divjat[k];
+      cnew[k] = SMOOTH ? co + m.dt * (divflux[k]) : co + m.dt * (divflux[k]) - divjat[k];
     }
 #pragma unroll
     for (int k = 0; k < K1; k++) {
@@ -708,6 +781,24 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ gp_model
       for (int a = 0; a < N; a++)
         if (a == bulk) v = Mu<K1>(m, cnew, a, k);
       mnew[k] = v;
+    }
+  } else if (SMOOTH) {
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      deltac[k] = m.dt * (divflux[k]);
+#pragma unroll
+      for (int l = 0; l < K1; l++)
+#pragma unroll
+        for (int a = 0; a < N; a++) dcdmu[k][l] += m.cmu[a][k][l] * hphi<N>(ph, a);
+    }
+    double inv[K1][K1];
+    lu_inverse<K1>(dcdmu, inv);
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      double s = 0;
+#pragma unroll
+      for (int l = 0; l < K1; l++) s = s + inv[k][l] * deltac[l];
+      mnew[k] = s + Mc[k];
     }
   } else {
 #pragma unroll
@@ -762,14 +853,14 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ gp_model
   for (int a = 0; a < N; a++) phi_out[o + a * g.plane] = ph[a] + Dc[a];
 }
 
-template <int N, int K1>
+template <int N, int K1, bool SMOOTH>
 cudaError_t launch_step(const gp_model& m, const Geo& g, const double* phi, const double* mu, double* dphi,
                         double* phi_out, double* mu_out, cudaStream_t s) {
   const dim3 blk(32, 8);
   const dim3 grd_r((g.my + 2 + 31) / 32, (g.mx + 2 + 7) / 8);
-  k_dphi<N, K1><<<grd_r, blk, 0, s>>>(m, g, phi, mu, dphi);
+  k_dphi<N, K1, SMOOTH><<<grd_r, blk, 0, s>>>(m, g, phi, mu, dphi);
   const dim3 grd((g.my + 31) / 32, (g.mx + 7) / 8);
-  k_update<N, K1><<<grd, blk, 0, s>>>(m, g, phi, mu, dphi, phi_out, mu_out);
+  k_update<N, K1, SMOOTH><<<grd, blk, 0, s>>>(m, g, phi, mu, dphi, phi_out, mu_out);
   return cudaGetLastError();
 }
 
@@ -778,7 +869,7 @@ cudaError_t launch_step(const gp_model& m, const Geo& g, const double* phi, cons
 // Host entry used by the C ABI (gp_capi.cu).  Two launches per step.
 cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch, int64_t rplane,
                         const double* phi, const double* mu, double* dphi, double* phi_out, double* mu_out,
-                        cudaStream_t s) {
+                        cudaStream_t s, bool smooth) {
   Geo g;
   g.mx = (int)m.mesh_x;
   g.my = (int)m.mesh_y;
@@ -787,8 +878,10 @@ cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch,
   g.rpitch = rpitch;
   g.rplane = rplane;
   g.bc = gp_bc_of(m);
-#define GP_CASE(NN, KK) \
-  if (m.N == NN && m.K1 == KK) return launch_step<NN, KK>(m, g, phi, mu, dphi, phi_out, mu_out, s);
+#define GP_CASE(NN, KK)                                                                           \
+  if (m.N == NN && m.K1 == KK)                                                                    \
+    return smooth ? launch_step<NN, KK, true>(m, g, phi, mu, dphi, phi_out, mu_out, s)            \
+                  : launch_step<NN, KK, false>(m, g, phi, mu, dphi, phi_out, mu_out, s);
   GP_CASE(2, 1) GP_CASE(2, 2) GP_CASE(2, 3)
   GP_CASE(3, 1) GP_CASE(3, 2) GP_CASE(3, 3)
   GP_CASE(4, 1) GP_CASE(4, 2) GP_CASE(4, 3)

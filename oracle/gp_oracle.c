@@ -350,6 +350,57 @@ static double dwdphi(const gpo_params *p, const double *phi, const double *divph
   return sum;
 }
 
+/* dw/dphi of the smoothing pre-steps: functionW_01.h:41-62 (obstacle) and
+ * functionW_02.h:35-59 (well), without the sign factors */
+static double dwdphi_smooth(const gpo_params *p, const double *phi, const double *divphi, int a) {
+  int b, d, N = p->N;
+  double sum = 0.0;
+  if (p->obstacle) {
+    for (b = 0; b < N; b++) {
+      if (b == a || !(fabs(divphi[b]) > 0.0)) continue;
+      sum += p->Gamma[a * N + b] * phi[b];
+    }
+    sum *= 16.0 / (M_PI * M_PI);
+  } else {
+    for (b = 0; b < N; b++) {
+      if (b == a || !(fabs(divphi[b]) > 0.0)) continue;
+      sum += 2.0 * p->Gamma[a * N + b] * (phi[b] * phi[b] * phi[a]);
+    }
+    sum *= 9.0;
+  }
+  for (b = 0; b < N; b++)
+    for (d = b + 1; d < N; d++) {
+      if (b == a || d == a) continue;
+      if (fabs(divphi[b]) > 0.0 && fabs(divphi[d]) > 0.0) sum += p->Gamma_abc[(a * N + b) * N + d] * phi[b] * phi[d];
+    }
+  return sum;
+}
+
+/* projection of the smoothing pre-steps, solverloop/simplex_projection.h:50-91:
+ * phases in index order; a phase above 1 takes the rest and ends the loop */
+static void project_simplex_unweighted(const gpo_params *p, const double *phi, const double *divphi, double *dp) {
+  int a, b, N = p->N;
+  long count = 0;
+  for (a = 0; a < N; a++)
+    if ((fabs(divphi[a]) > 0.0) && (phi[a] + dp[a]) > 0.0 && (phi[a] + dp[a]) < 1.0) count++;
+  for (a = 0; a < N; a++) {
+    if (!(fabs(divphi[a]) > 0.0)) continue;
+    if ((phi[a] + dp[a]) > 1.0) {
+      dp[a] = (1.0 - phi[a]);
+      for (b = 0; b < N; b++)
+        if ((fabs(divphi[b]) > 0.0) && b != a) dp[b] = -phi[b];
+      break;
+    }
+    if ((phi[a] + dp[a]) < 0.0) {
+      double D = fabs(dp[a] + phi[a]);
+      dp[a] += D;
+      for (b = 0; b < N; b++)
+        if (((fabs(divphi[b]) > 0.0) && b != a) && (phi[b] + dp[b]) > 0.0 && (phi[b] + dp[b]) < 1.0)
+          dp[b] -= D / (count);
+    }
+  }
+}
+
 /* functions/functionTau.h:1-16 */
 static double tau_phi(const gpo_params *p, const double *phi) {
   double sum = 0.0, sum1 = 0.0;
@@ -400,8 +451,11 @@ static void project_simplex(const gpo_params *p, const double *phi, const double
   }
 }
 
-/* Delta-phi of one cell: solverloop/calculate_divergence_phasefield.h:4-62 */
-static void delta_phi_cell(const ctx_t *c, long x, long y, double *dp) {
+/* Delta-phi of one cell: solverloop/calculate_divergence_phasefield.h:4-62;
+ * smooth: the pre-step form of :63-158 (isotropic gradient energy
+ * (function_A_01.h:73-99, 220-260 equal function_A_00's), no dpsi, the
+ * unsigned potential when anisotropic, unweighted projection) */
+static void delta_phi_cell(const ctx_t *c, long x, long y, double *dp, int smooth) {
   const gpo_params *p = c->p;
   int a, N = p->N;
   grad_rec g, gb, gf, gl, gr;
@@ -422,14 +476,18 @@ static void delta_phi_cell(const ctx_t *c, long x, long y, double *dp) {
   for (a = 0; a < N; a++) {
     if (fabs(divphi[a]) > 0.0) {
       double dA, divA;
-      if (p->anisotropy) {
+      if (p->anisotropy && !smooth) {
         dA = dAdphi_aniso(p, phi, &g, a);
         divA = divdA_aniso(p, &g, &gb, &gf, &gl, &gr, a);
       } else {
         dA = dAdphi_iso(p, phi, &g, a);
         divA = divdA_iso(p, &g, &gb, &gl, a);
       }
-      lambda[a] = p->epsilon * (-dA + divA) - (1.0 / p->epsilon) * dwdphi(p, phi, divphi, a) - dpsi(p, mu, phi, a);
+      if (smooth) /* the unsigned potential only with anisotropy (calculate_divergence_phasefield.h:89-97) */
+        lambda[a] = p->epsilon * (-dA + divA) -
+                    (1.0 / p->epsilon) * (p->anisotropy ? dwdphi_smooth(p, phi, divphi, a) : dwdphi(p, phi, divphi, a));
+      else
+        lambda[a] = p->epsilon * (-dA + divA) - (1.0 / p->epsilon) * dwdphi(p, phi, divphi, a) - dpsi(p, mu, phi, a);
       sum_lambda += lambda[a];
       active++;
     }
@@ -439,7 +497,8 @@ static void delta_phi_cell(const ctx_t *c, long x, long y, double *dp) {
     if (fabs(divphi[a]) > 0.0) dp[a] = p->dt * (lambda[a] - sum_lambda) / (tau_phi(p, phi) * p->epsilon);
     else dp[a] = 0.0;
   }
-  project_simplex(p, phi, divphi, dp);
+  if (smooth) project_simplex_unweighted(p, phi, divphi, dp);
+  else project_simplex(p, phi, divphi, dp);
 }
 
 static void cell_vec(const ctx_t *c, const double *base, int n, long x, long y, double *out) {
@@ -632,8 +691,11 @@ void gpo_apply_bc(const gpo_params *p, double *phi, double *mu) {
  * Delta-phi on the ring [2, rows-3]^2, the concentration half step
  * (solverloop.h:35-71 -> calculate_divergence_concentration.h:4-153) updates
  * mu and phi on the interior, then the ghosts are refilled (microsim_gp.c:103-106). */
+/* One time step (solverloop.h:21-71), or with smooth one pre-step
+ * (solverloop.h:72-90: calculate_divergence_concentration.h:154-253, no
+ * antitrapping current and no dh/dt source, the LU inverse for every mu solve). */
 static int one_step(const gpo_params *p, double *phi, double *mu, double *dphi, double *phi_new, double *mu_new,
-                    double *jxa, double *jya, gpo_stats *st) {
+                    double *jxa, double *jya, gpo_stats *st, int smooth) {
   long rx = p->mesh_x + 6, ry = p->mesh_y + 6, n = rx * ry;
   int N = p->N, K1 = p->K1, a, k, l;
   long x, y;
@@ -643,11 +705,11 @@ static int one_step(const gpo_params *p, double *phi, double *mu, double *dphi, 
   for (x = 2; x <= rx - 3; x++)
     for (y = 2; y <= ry - 3; y++) {
       double dp[MAXN];
-      delta_phi_cell(&c, x, y, dp);
+      delta_phi_cell(&c, x, y, dp, smooth);
       for (a = 0; a < N; a++) dphi[a * n + y + x * ry] = dp[a];
     }
   /* antitrapping currents on faces touching the interior */
-  for (x = 2; x <= rx - 4; x++)
+  for (x = 2; x <= rx - 4 && !smooth; x++)
     for (y = 2; y <= ry - 4; y++) {
       double jx[MAXK], jy[MAXK];
       jat_cell(&c, x, y, jx, jy);
@@ -658,7 +720,7 @@ static int one_step(const gpo_params *p, double *phi, double *mu, double *dphi, 
     }
   memcpy(phi_new, phi, sizeof(double) * N * n);
   memcpy(mu_new, mu, sizeof(double) * K1 * n);
-  if (st) {
+  if (st && !smooth) {
     for (a = 0; a < N; a++) st->rel_change_phi[a] = 0.0;
     for (k = 0; k < K1; k++) st->rel_change_mu[k] = 0.0;
   }
@@ -700,9 +762,11 @@ static int one_step(const gpo_params *p, double *phi, double *mu, double *dphi, 
           divflux[k] += (Dx * gmx - Dxb * gmxb) / p->dx;
           divflux[k] += (Dy * gmy - Dyl * gmyl) / p->dy;
         }
-        double jx = jxa[k * n + id], jxb = jxa[k * n + id - ry];
-        double jy = jya[k * n + id], jyl = jya[k * n + id - 1];
-        if (p->obstacle) {
+        double jx = smooth ? 0.0 : jxa[k * n + id], jxb = smooth ? 0.0 : jxa[k * n + id - ry];
+        double jy = smooth ? 0.0 : jya[k * n + id], jyl = smooth ? 0.0 : jya[k * n + id - 1];
+        if (smooth) {
+          divjat[k] = 0.0;
+        } else if (p->obstacle) {
           divjat[k] = (jx - jxb) * (-0.25 * M_PI * p->epsilon) / p->dx;
           divjat[k] += (jy - jyl) * (-0.25 * M_PI * p->epsilon) / p->dy;
         } else {
@@ -714,7 +778,25 @@ static int one_step(const gpo_params *p, double *phi, double *mu, double *dphi, 
       for (a = 0; a < N; a++)
         if (ph[a] == 1.0) { bulk = a; break; }
       double mnew[MAXK];
-      if (bulk >= 0) {
+      if (bulk >= 0 && smooth) {
+        double cnew[MAXK];
+        for (k = 0; k < K1; k++) cnew[k] = c_mu(p, m, bulk, k) + p->dt * (divflux[k]);
+        for (k = 0; k < K1; k++) mnew[k] = Mu(p, cnew, bulk, k);
+      } else if (smooth) {
+        /* deltac = dt divflux; dcdmu^-1 by matinvnew (LU); mu += inv deltac */
+        for (k = 0; k < K1; k++) {
+          deltac[k] = p->dt * (divflux[k]);
+          for (l = 0; l < K1; l++)
+            for (a = 0; a < N; a++) dcdmu[k][l] += p->cmu[(a * K1 + k) * K1 + l] * hphi(p, ph, a);
+        }
+        lu_inverse(dcdmu, inv, K1);
+        for (k = 0; k < K1; k++) {
+          double s = 0;
+          for (l = 0; l < K1; l++) s = s + inv[k][l] * deltac[l];
+          deltamu[k] = s;
+        }
+        for (k = 0; k < K1; k++) mnew[k] = deltamu[k] + m[k];
+      } else if (bulk >= 0) {
         double cnew[MAXK];
         for (k = 0; k < K1; k++) cnew[k] = c_mu(p, m, bulk, k) + p->dt * (divflux[k]) - divjat[k];
         for (k = 0; k < K1; k++) {
@@ -765,13 +847,13 @@ static int one_step(const gpo_params *p, double *phi, double *mu, double *dphi, 
       for (a = 0; a < N; a++) {
         double v = ph[a] + dp[a];
         phi_new[a * n + id] = v;
-        if (st) {
+        if (st && !smooth) {
           if (v > st->phi_max[a]) st->phi_max[a] = v;
           if (v < st->phi_min[a]) st->phi_min[a] = v;
           st->rel_change_phi[a] += dp[a] * dp[a];
         }
       }
-      if (st) {
+      if (st && !smooth) {
         for (k = 0; k < K1; k++) {
           if (mnew[k] > st->mu_max[k]) st->mu_max[k] = mnew[k];
           if (mnew[k] < st->mu_min[k]) st->mu_min[k] = mnew[k];
@@ -807,9 +889,28 @@ int gpo_step(const gpo_params *p, double *phi, double *mu, long nsteps, double *
     for (k = 0; k < p->K1; k++) { st->mu_max[k] = 1.0; st->mu_min[k] = 1.0; st->rel_change_mu[k] = 0.0; }
   }
   for (t = 0; t < nsteps; t++) {
-    one_step(p, phi, mu, dphi, pn, mn, jx, jy, st);
+    one_step(p, phi, mu, dphi, pn, mn, jx, jy, st, 0);
     if (t == 0 && dphi_first) memcpy(dphi_first, dphi, sizeof(double) * p->N * n);
   }
   free(dphi); free(pn); free(mn); free(jx); free(jy);
+  return 0;
+}
+
+/* NSMOOTH - 1 pre-steps (microsim_gp.c:97-100), each followed by the boundary copy */
+int gpo_smooth(const gpo_params *p, double *phi, double *mu, long nsteps) {
+  long rx, ry, n, t;
+  int a;
+  if (p->N < 2 || p->N > MAXN || p->K1 < 1 || p->K1 > MAXK) return -1;
+  if (p->mesh_x < 4 || p->mesh_y < 4) return -1;
+  for (a = 0; a < 4; a++) {
+    if (p->bc_phi[a] != 1 && p->bc_phi[a] != 3) return -1;
+    if (p->bc_mu[a] != 1 && p->bc_mu[a] != 3) return -1;
+  }
+  rx = p->mesh_x + 6; ry = p->mesh_y + 6; n = rx * ry;
+  double *dphi = (double *)calloc((size_t)(p->N * n), sizeof(double));
+  double *pn = (double *)malloc(sizeof(double) * p->N * n);
+  double *mn = (double *)malloc(sizeof(double) * p->K1 * n);
+  for (t = 0; t < nsteps; t++) one_step(p, phi, mu, dphi, pn, mn, NULL, NULL, NULL, 1);
+  free(dphi); free(pn); free(mn);
   return 0;
 }

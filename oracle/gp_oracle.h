@@ -63,6 +63,9 @@ void gpo_apply_bc(const gpo_params *p, double *phi, double *mu);
  * Stats (if not NULL) follow microsim_gp.c's running max/min and the last
  * step's sum of squared changes, over interior cells.  Returns 0, or -1 for
  * unsupported parameters. */
+/* nsteps smoothing pre-steps (the reference runs NSMOOTH - 1 of them before
+ * the time loop), each followed by the boundary copy. */
+int gpo_smooth(const gpo_params *p, double *phi, double *mu, long nsteps);
 int gpo_step(const gpo_params *p, double *phi, double *mu, long nsteps, double *dphi_first,
              gpo_stats *st);
 

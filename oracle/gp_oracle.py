@@ -66,6 +66,8 @@ def lib():
         _lib.gpo_step.restype = C.c_int
         _lib.gpo_apply_bc.argtypes = [C.POINTER(_Params), C.c_void_p, C.c_void_p]
         _lib.gpo_apply_bc.restype = None
+        _lib.gpo_smooth.argtypes = [C.POINTER(_Params), C.c_void_p, C.c_void_p, C.c_long]
+        _lib.gpo_smooth.restype = C.c_int
     return _lib
 
 
@@ -161,6 +163,17 @@ def step(model: OracleModel, phi: np.ndarray, mu: np.ndarray, nsteps: int, want_
         stats = {n: np.array(getattr(st, n)[: (model.N if "phi" in n else model.K1)])
                  for n, _ in _Stats._fields_}
     return dphi, stats
+
+
+def smooth(model: OracleModel, phi: np.ndarray, mu: np.ndarray, nsteps: int) -> None:
+    """nsteps smoothing pre-steps (the reference runs NSMOOTH - 1 of them,
+    microsim_gp.c:97-100) on ghost-padded fields, in place."""
+    assert phi.dtype == np.float64 and phi.flags.c_contiguous
+    assert mu.dtype == np.float64 and mu.flags.c_contiguous
+    p = model.params()
+    rc = lib().gpo_smooth(C.byref(p), phi.ctypes.data, mu.ctypes.data, nsteps)
+    if rc != 0:
+        raise ValueError("oracle rejected the parameters (rc=%d)" % rc)
 
 
 def apply_bc(model: OracleModel, phi: np.ndarray, mu: np.ndarray) -> None:

@@ -47,6 +47,12 @@ def row_digests(phi, mu):
                      for x in range(planes.shape[1])])
 
 
+def presmooth(ctx, g):
+    """Run a fixture's smoothing pre-steps (NSMOOTH - 1) on an uploaded context."""
+    if "nsmooth" in g:
+        ctx.smooth(int(g["nsmooth"]) - 1)
+
+
 def oracle_model(g):
     """Oracle model from a fixture's reference constants."""
     from oracle import gp_oracle as O

@@ -95,6 +95,27 @@ def cases():
                      solver="DILUTE", phases=["a", "b", "l"], components=["X", "Y", "Z"],
                      fills=[("FILLCYLINDER", [0, 7, 10, 0, 0, 4.0]), ("FILLSPHERE", [1, 17, 10, 0, 4.5])])
     out["dilute_three_phase"] = (c, [1, 20, 40])
+    # smoothing pre-steps (NSMOOTH - 1 of them before the time loop): anisotropic obstacle binary
+    c = C.binary_case(32, 28, gap=1.0, supersat=0.5, eps=4.0, delta=0.04, theta=15.0, dt=0.05, tau=1.7776,
+                      seed=(16, 14, 6.0), steps=30)
+    c.nsmooth = 8
+    out["smooth_aniso_obst"] = (c, [1, 15, 30])
+    # smoothing with three phases, well potential, periodic x
+    c = configs.Case(mesh_x=28, mesh_y=24, dx=1.0, dt=0.04, N=3, K=2, ntimesteps=30, epsilon=4.0, tau=1.0,
+                     gamma=[1.0, 1.0, 1.0], tau_ab=[1.5, 1.5, 1.5], aniso=0, dab=[0.0, 0.0, 0.0],
+                     function_w=2, gamma_abc=[5.0],
+                     diffusivity=[(1, 0, 0.0), (1, 1, 0.0), (1, 2, 1.0)], A=[(0, 1.0), (1, 1.0), (2, 1.0)],
+                     ceq=[(0, 0, 0.78), (0, 2, 0.5), (2, 0, 0.5), (1, 1, 0.21), (1, 2, 0.5), (2, 1, 0.5),
+                          (2, 2, 0.5)],
+                     cfill=[(0, 0, 0.78), (0, 2, 0.5), (2, 0, 0.5), (1, 1, 0.21), (1, 2, 0.5), (2, 1, 0.5),
+                            (2, 2, 0.45)],
+                     slopes=[(0, 0, 0.45), (0, 2, 0.45), (2, 0, 0.45), (1, 1, -0.45), (1, 2, -0.45),
+                             (2, 1, -0.45)],
+                     T=0.98, bc_phi=(3, 3, 1, 1), bc_mu=(3, 3, 1, 1), solver="BINARY",
+                     phases=["alpha", "beta", "liquid"], components=["Al", "Cu"],
+                     fills=[("FILLCUBE", [0, 0, 0, 0, 13, 5, 0]), ("FILLCUBE", [1, 14, 0, 0, 27, 5, 0])])
+    c.nsmooth = 6
+    out["smooth_three_phase_well"] = (c, [1, 15, 30])
     return out
 
 
@@ -113,6 +134,10 @@ def run_case(name, case, dump_steps):
         data["phi_0"], data["mu_0"] = phi, mu
         d, _ = O.read_state(os.path.join(dd, "dphi_1.bin"))
         data["dphi_1"] = d
+        if case.nsmooth > 1:  # the state after the NSMOOTH - 1 smoothing pre-steps
+            phi, mu = O.read_state(os.path.join(dd, "smoothed_0.bin"))
+            data["phi_smoothed"], data["mu_smoothed"] = phi, mu
+            data["nsmooth"] = np.array(case.nsmooth)
         for t in dump_steps:
             phi, mu = O.read_state(os.path.join(dd, f"state_{t}.bin"))
             data[f"phi_{t}"], data[f"mu_{t}"] = phi, mu
@@ -124,10 +149,12 @@ def run_case(name, case, dump_steps):
     return data
 
 
-def main():
+def main(only=None):
     if not os.path.exists(O.HARNESS_PATH):
         raise SystemExit("build the reference first: make -C oracle reference")
     for name, (case, steps) in cases().items():
+        if only and name not in only:
+            continue
         d = run_case(name, case, steps)
         size = os.path.getsize(os.path.join(HERE, name + ".npz"))
         print(f"{name}: N={case.N} K={case.K} {case.mesh_x}x{case.mesh_y} steps={steps} -> {size/1024:.1f} KiB")
@@ -135,6 +162,8 @@ def main():
 
 if __name__ == "__main__" and len(sys.argv) == 1:
     main()
+if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "only":
+    main(sys.argv[2:])
 
 
 # ---------------------------------------------------------------------------

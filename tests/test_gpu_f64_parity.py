@@ -12,7 +12,8 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import golden_cases, interior, load_golden, long_cases, oracle_model, row_digests, write_inputs
+from conftest import (golden_cases, interior, load_golden, long_cases, oracle_model, presmooth, row_digests,
+                      write_inputs)
 import microsim_b200 as mb
 from microsim_b200 import configs
 from oracle import gp_oracle as O
@@ -35,10 +36,29 @@ def test_dphi_ring_bitexact(case):
     m, phi, mu = _setup(g)
     with mb.Context(m, mb.GP_FP64) as ctx:
         ctx.upload(phi, mu)
+        presmooth(ctx, g)
         ctx.step(1)
         d = ctx.download_dphi()
     ref = g["dphi_1"][:, 2:-2, 2:-2]
     assert np.array_equal(d, ref), f"max |diff| {np.abs(d - ref).max()}"
+
+
+@pytest.mark.parametrize("case", [c for c in golden_cases() if "nsmooth" in load_golden(c)])
+@pytest.mark.parametrize("precision", [mb.GP_FP64, mb.GP_FP32])
+def test_smoothing_pre_steps_bitexact(case, precision):
+    """NSMOOTH - 1 pre-steps equal the reference's.  An FP32 context runs them in
+    FP64 from its FP32-stored state: within 1e-6 of the reference."""
+    g = load_golden(case)
+    m, phi, mu = _setup(g)
+    with mb.Context(m, precision) as ctx:
+        ctx.upload(phi, mu)
+        ctx.smooth(int(g["nsmooth"]) - 1)
+        p, u = ctx.download()
+    rp, ru = interior(g["phi_smoothed"]), interior(g["mu_smoothed"])
+    if precision == mb.GP_FP64:
+        assert np.array_equal(p, rp) and np.array_equal(u, ru)
+    else:
+        assert np.abs(p - rp).max() <= 1e-6 and np.abs(u - ru).max() <= 1e-6
 
 
 @pytest.mark.parametrize("case", golden_cases())
@@ -47,6 +67,7 @@ def test_states_bitexact(case):
     m, phi, mu = _setup(g)
     with mb.Context(m, mb.GP_FP64) as ctx:
         ctx.upload(phi, mu)
+        presmooth(ctx, g)
         done = 0
         for t in g["dump_steps"]:
             ctx.step(int(t) - done)

@@ -11,11 +11,29 @@ from conftest import golden_cases, interior, load_golden, oracle_model
 from oracle import gp_oracle as O
 
 
+def start_state(g, m):
+    """The fixture's state before its first time step: the filled domain, after
+    the NSMOOTH - 1 smoothing pre-steps when the input asks for them."""
+    phi, mu = g["phi_0"].copy(), g["mu_0"].copy()
+    if "nsmooth" in g:
+        O.smooth(m, phi, mu, int(g["nsmooth"]) - 1)
+    return phi, mu
+
+
+@pytest.mark.parametrize("case", [c for c in golden_cases() if "nsmooth" in load_golden(c)])
+def test_smoothing_pre_steps_bitexact(case):
+    g = load_golden(case)
+    phi, mu = start_state(g, oracle_model(g))
+    assert np.array_equal(interior(phi), interior(g["phi_smoothed"]))
+    assert np.array_equal(interior(mu), interior(g["mu_smoothed"]))
+    assert np.array_equal(phi, g["phi_smoothed"]) and np.array_equal(mu, g["mu_smoothed"])  # ghosts too
+
+
 @pytest.mark.parametrize("case", golden_cases())
 def test_dphi_first_step_bitexact(case):
     g = load_golden(case)
     m = oracle_model(g)
-    phi, mu = g["phi_0"].copy(), g["mu_0"].copy()
+    phi, mu = start_state(g, m)
     dphi, _ = O.step(m, phi, mu, 1, want_dphi=True)
     ring = (slice(None), slice(2, -2), slice(2, -2))
     assert np.array_equal(dphi[ring], g["dphi_1"][ring]), \
@@ -26,7 +44,7 @@ def test_dphi_first_step_bitexact(case):
 def test_states_bitexact(case):
     g = load_golden(case)
     m = oracle_model(g)
-    phi, mu = g["phi_0"].copy(), g["mu_0"].copy()
+    phi, mu = start_state(g, m)
     done = 0
     for t in g["dump_steps"]:
         O.step(m, phi, mu, int(t) - done)
