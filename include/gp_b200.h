@@ -102,6 +102,9 @@ typedef struct gp_model {
   double jat_obst;    /* -0.25*M_PI*epsilon                         */
   double jat_well;    /* -1.0*epsilon                               */
   double s_well;      /* 0.5/sqrt(2.0)                              */
+  /* mu of the liquid rows a moving-frame shift appends: Mu(cfill of the liquid)
+   * at Filling_temperature (functions/shift.h:24-37) */
+  double mu_shift[GP_MAX_K1];
 } gp_model;
 
 /* Parsed Input.in (+ its BOUNDARY lines) and Filling.in. */
@@ -167,6 +170,17 @@ int gp_step(gp_ctx *ctx, int64_t nsteps);
  * bit-exact route is an FP64 context (the CLI driver smooths the filled doubles
  * in FP64 before an FP32 time loop). */
 int gp_smooth(gp_ctx *ctx, int64_t nsteps);
+/* Moving frame (Shift = 1; microsim_gp.c:115-125, functions/shift.h):
+ * gp_interface_y gives the highest row where the liquid fraction crosses 0.5
+ * upwards, in the reference's ghost-padded row index (interior row + 3; 0 when
+ * there is none), as check_SHIFT scans it; gp_shift_y moves the window d rows
+ * along +y, appending liquid rows (mu = gp_model.mu_shift).  The reference
+ * shifts its ghost rows too, and its next phase-field half step reads them
+ * before the boundary copy refreshes them: FP64 contexts keep those rows and
+ * reproduce it bit for bit; FP32 contexts read the boundary map of the shifted
+ * interior. */
+int gp_interface_y(gp_ctx *ctx, int64_t *pos);
+int gp_shift_y(gp_ctx *ctx, int64_t d);
 int gp_sync(gp_ctx *ctx);
 /* FP64 statistics of the current state (max/min/rel-change of the last step,
  * solute and phase sums, NaN watchdog). Synchronous. */

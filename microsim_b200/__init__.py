@@ -54,6 +54,7 @@ class GpModel(C.Structure):
         ("Diff", C.c_double * (_P * _K * _K)),
         ("inv_eps", C.c_double), ("w_obstacle", C.c_double), ("jat_obst", C.c_double),
         ("jat_well", C.c_double), ("s_well", C.c_double),
+        ("mu_shift", C.c_double * _K),
     ]
 
     def arr(self, name):
@@ -119,6 +120,8 @@ _SIGS = {
     "gp_batch_cells": (C.c_int64, [C.c_void_p]),
     "gp_last_error": (C.c_char_p, []),
     "gp_smooth": (C.c_int, [C.c_void_p, C.c_int64]),
+    "gp_interface_y": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "gp_shift_y": (C.c_int, [C.c_void_p, C.c_int64]),
     "gp_adj_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "gp_adj_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                                  C.c_void_p]),
@@ -261,6 +264,16 @@ class Context:
     def smooth(self, nsteps: int):
         """nsteps smoothing pre-steps (NSMOOTH - 1 in the reference's main)."""
         _check("gp_smooth", lib().gp_smooth(self._h, int(nsteps)))
+
+    def interface_y(self) -> int:
+        """Highest upward liquid crossing, ghost-padded row index (check_SHIFT)."""
+        v = C.c_int64()
+        _check("gp_interface_y", lib().gp_interface_y(self._h, C.byref(v)))
+        return v.value
+
+    def shift_y(self, d: int):
+        """Move the window d rows along +y (apply_shiftY)."""
+        _check("gp_shift_y", lib().gp_shift_y(self._h, int(d)))
 
     def sync(self):
         _check("gp_sync", lib().gp_sync(self._h))

@@ -69,6 +69,8 @@ class Case:
     ntimesteps: int = 1000
     savet: int = 1000
     nsmooth: int = 1
+    shift: int = 0                  # moving frame along +y (Shift / Shiftj)
+    shiftj: int = 0
     track: int = 1000
     epsilon: float = 4.0
     tau: float = 1.0                # FunctionTau fallback
@@ -146,8 +148,8 @@ class Case:
         L.append(f"Function_W = {self.function_w};")
         L.append("Gamma_abc = {" + ",".join(fmt(v) for v in self.gamma_abc) + "};")
         L += [
-            "Shift = 0;",
-            "Shiftj = 0;",
+            f"Shift = {self.shift};",
+            f"Shiftj = {self.shiftj};",
             f"Writecomposition = {self.writecomposition};",
             "Noise_phasefield = 0;",
             f"Equilibrium_temperature = {fmt(self.Teq)};",

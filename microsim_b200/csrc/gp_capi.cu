@@ -19,7 +19,7 @@
 extern "C" void gp_set_error(const char* fmt, ...);
 
 cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch, int64_t rplane, const double* phi,
-                        const double* mu, double* dphi, double* phi_out, double* mu_out, cudaStream_t s, bool smooth = false);
+                        const double* mu, double* dphi, double* phi_out, double* mu_out, cudaStream_t s, bool smooth = false, const double* ghost_rows = nullptr);
 struct gp_f32_batch;
 int gp_f32_supported(const gp_model& m);
 cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** out);
@@ -62,6 +62,8 @@ struct gp_ctx {
   void* phi[2];
   void* mu[2];
   double* dphi;    // FP64 form: Delta-phi of the last phase-field half step
+  double* gov;     // FP64 form: the ghost rows a moving-frame shift leaves ([N+K1][mx][6])
+  int gov_pending; // the next phase-field half step reads gov
   gp_f32_batch* f32;  // FP32 form: a batch of one instance over phi/mu
   int cur;         // which buffer holds the current state
   int have_prev;   // buffer 1-cur holds the previous step's state
@@ -169,6 +171,7 @@ extern "C" int gp_destroy(gp_ctx* c) {
     if (c->mu[i]) cudaFree(c->mu[i]);
   }
   if (c->dphi) cudaFree(c->dphi);
+  if (c->gov) cudaFree(c->gov);
   if (c->f32) gp_f32_batch_destroy(c->f32);
   if (c->partials) cudaFree(c->partials);
   if (c->reduced) cudaFree(c->reduced);
@@ -269,7 +272,8 @@ extern "C" int gp_step(gp_ctx* c, int64_t nsteps) {
     if (c->precision == GP_FP64) {
       GP_CUDA(gp_f64_step(c->m, c->pitch, c->plane, c->rpitch, c->rplane, (const double*)c->phi[c->cur],
                           (const double*)c->mu[c->cur], c->dphi, (double*)c->phi[nxt], (double*)c->mu[nxt],
-                          c->stream));
+                          c->stream, false, c->gov_pending ? c->gov : nullptr));
+      c->gov_pending = 0;
       c->launches += 2;
     } else {
       GP_CUDA(gp_f32_batch_launch(c->f32, c->cur, c->stream));
@@ -309,6 +313,119 @@ extern "C" int gp_smooth(gp_ctx* c, int64_t nsteps) {
   if (d) gp_destroy(d);
   if (rc == GP_OK) rc = gp_upload(c, phi.data(), mu.data());
   return rc;
+}
+
+// ------------------------------------------------------------------ moving frame
+
+// Highest row where the liquid fraction crosses 0.5 upwards, in the reference's
+// ghost-padded row index (check_SHIFT, functions/shift.h:43-66): rows y-1, y of
+// every interior column, ghost rows through the boundary map.
+template <typename T>
+__global__ void __launch_bounds__(256) k_interface_y(const T* __restrict__ phiL, int mx, int my, int pitch, int bcy,
+                                                     int* __restrict__ out) {
+  const int x = blockIdx.y, yg = blockIdx.x * blockDim.x + threadIdx.x + 1;  // yg in [1, my + 5]
+  if (yg > my + 5) return;
+  const int yi = yg - 3;
+  const T a = phiL[(int64_t)x * pitch + gp_map(yi - 1, my, bcy)];
+  const T b = phiL[(int64_t)x * pitch + gp_map(yi, my, bcy)];
+  if ((a - ((T)1 - a)) < (T)0 && (b - ((T)1 - b)) > (T)0) atomicMax(out, yg);
+}
+
+// Window shifted by d rows along +y (apply_shiftY, functions/shift.h:4-40): row
+// y takes row y + d (through the boundary map up to the last ghost row), the
+// rows beyond take the liquid (phi of the liquid 1, mu = mu_shift).
+template <typename T>
+__global__ void __launch_bounds__(256) k_shift_y(const T* __restrict__ phi, const T* __restrict__ mu,
+                                                 T* __restrict__ phi_o, T* __restrict__ mu_o, int N, int K1, int mx,
+                                                 int my, int pitch, int64_t plane, gp_bc bc, int d, double f0,
+                                                 double f1, double f2) {
+  const int x = blockIdx.y, y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= my) return;
+  const int64_t o = (int64_t)x * pitch + y;
+  const int src = y + d;
+  if (src <= my + 2) {
+    const int64_t sp = (int64_t)x * pitch + gp_map(src, my, bc.phi_y), sm = (int64_t)x * pitch + gp_map(src, my, bc.mu_y);
+    for (int a = 0; a < N; a++) phi_o[a * plane + o] = phi[a * plane + sp];
+    for (int k = 0; k < K1; k++) mu_o[k * plane + o] = mu[k * plane + sm];
+  } else {
+    for (int a = 0; a < N; a++) phi_o[a * plane + o] = (a == N - 1) ? (T)1 : (T)0;
+    const double f[3] = {f0, f1, f2};
+    for (int k = 0; k < K1; k++) mu_o[k * plane + o] = (T)f[k];
+  }
+}
+
+// The ghost rows y = -3..-1, my..my+2 as the shift leaves them (the reference
+// shifts its ghost rows with the interior): row y takes row y + d of the old
+// state through the boundary map, or the liquid beyond.
+__global__ void k_shift_ghosts(const double* __restrict__ phi, const double* __restrict__ mu,
+                               double* __restrict__ gov, int N, int K1, int mx, int my, int pitch, int64_t plane,
+                               gp_bc bc, int d, double f0, double f1, double f2) {
+  const int x = blockIdx.x, slot = threadIdx.x;
+  if (slot >= 6) return;
+  const int y = slot < 3 ? slot - 3 : my + slot - 3, src = y + d;
+  const double f[3] = {f0, f1, f2};
+  for (int a = 0; a < N; a++)
+    gov[((int64_t)a * mx + x) * 6 + slot] = src <= my + 2 ? phi[a * plane + (int64_t)x * pitch + gp_map(src, my, bc.phi_y)]
+                                                          : (a == N - 1 ? 1.0 : 0.0);
+  for (int k = 0; k < K1; k++)
+    gov[((int64_t)(N + k) * mx + x) * 6 + slot] =
+        src <= my + 2 ? mu[k * plane + (int64_t)x * pitch + gp_map(src, my, bc.mu_y)] : f[k];
+}
+
+extern "C" int gp_interface_y(gp_ctx* c, int64_t* pos) {
+  if (!c || !pos) return GP_E_ARG;
+  const int mx = (int)c->m.mesh_x, my = (int)c->m.mesh_y, L = c->m.N - 1;
+  int* d = nullptr;
+  GP_CUDA(cudaMallocAsync((void**)&d, sizeof(int), c->stream));
+  GP_CUDA(cudaMemsetAsync(d, 0, sizeof(int), c->stream));
+  const dim3 b(256), g((my + 5 + 255) / 256, mx);
+  const int bcy = gp_bc_of(c->m).phi_y;
+  if (c->precision == GP_FP64)
+    k_interface_y<double><<<g, b, 0, c->stream>>>((const double*)c->phi[c->cur] + L * c->plane, mx, my, c->pitch,
+                                                 bcy, d);
+  else
+    k_interface_y<float><<<g, b, 0, c->stream>>>((const float*)c->phi[c->cur] + L * c->plane, mx, my, c->pitch, bcy,
+                                                d);
+  GP_CUDA(cudaGetLastError());
+  c->launches += 1;
+  int h = 0;
+  GP_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  GP_CUDA(cudaFreeAsync(d, c->stream));
+  GP_CUDA(cudaStreamSynchronize(c->stream));
+  *pos = h;
+  return GP_OK;
+}
+
+extern "C" int gp_shift_y(gp_ctx* c, int64_t d) {
+  if (!c || d < 0) return GP_E_ARG;
+  if (d == 0) return GP_OK;
+  const int mx = (int)c->m.mesh_x, my = (int)c->m.mesh_y, nxt = 1 - c->cur;
+  const dim3 b(256), g((my + 255) / 256, mx);
+  const gp_bc bc = gp_bc_of(c->m);
+  const double* f = c->m.mu_shift;
+  if (c->precision == GP_FP64) {
+    if (!c->gov) GP_CUDA(cudaMalloc(&c->gov, sizeof(double) * (c->m.N + c->m.K1) * mx * 6));
+    k_shift_ghosts<<<mx, 32, 0, c->stream>>>((const double*)c->phi[c->cur], (const double*)c->mu[c->cur], c->gov,
+                                             c->m.N, c->m.K1, mx, my, c->pitch, c->plane, bc, (int)d, f[0], f[1],
+                                             f[2]);
+    GP_CUDA(cudaGetLastError());
+    c->gov_pending = 1;
+    c->launches += 1;
+  }
+  if (c->precision == GP_FP64)
+    k_shift_y<double><<<g, b, 0, c->stream>>>((const double*)c->phi[c->cur], (const double*)c->mu[c->cur],
+                                             (double*)c->phi[nxt], (double*)c->mu[nxt], c->m.N, c->m.K1, mx, my,
+                                             c->pitch, c->plane, bc, (int)d, f[0], f[1], f[2]);
+  else
+    k_shift_y<float><<<g, b, 0, c->stream>>>((const float*)c->phi[c->cur], (const float*)c->mu[c->cur],
+                                            (float*)c->phi[nxt], (float*)c->mu[nxt], c->m.N, c->m.K1, mx, my,
+                                            c->pitch, c->plane, bc, (int)d, f[0], f[1], f[2]);
+  GP_CUDA(cudaGetLastError());
+  c->launches += 1;
+  c->cur = nxt;
+  c->have_prev = 0;
+  if (c->f32) GP_CUDA(gp_f32_batch_invalidate(c->f32, c->stream));
+  return GP_OK;
 }
 
 extern "C" int gp_sync(gp_ctx* c) {

@@ -30,10 +30,25 @@ struct Geo {
   int rpitch;      // elements per x-row of the Delta-phi ring array
   int64_t rplane;  // elements per ring plane
   gp_bc bc;
+  // ghost rows y = -3..-1, my..my+2 held explicitly ([N + K1 planes][mx][6]), or
+  // nullptr: ghost reads through the boundary map.  Set for the phase-field half
+  // step right after a moving-frame shift, which reads the shifted ghost rows
+  // before the boundary copy refreshes them (microsim_gp.c:103-125).
+  const double* gov;
 };
+
+__device__ __forceinline__ const double* ghost_row(const Geo& g, int x, int y, int xtype, int q) {
+  const int slot = y < 0 ? y + 3 : y - g.my + 3;
+  return g.gov + ((int64_t)q * g.mx + gp_map(x, g.mx, xtype)) * 6 + slot;
+}
 
 template <int N>
 __device__ __forceinline__ void load_phi(const double* __restrict__ phi, const Geo& g, int x, int y, double* out) {
+  if (g.gov && (y < 0 || y >= g.my)) {
+#pragma unroll
+    for (int a = 0; a < N; a++) out[a] = *ghost_row(g, x, y, g.bc.phi_x, a);
+    return;
+  }
   const int ix = gp_map(x, g.mx, g.bc.phi_x), iy = gp_map(y, g.my, g.bc.phi_y);
   const double* p = phi + (int64_t)ix * g.pitch + iy;
 #pragma unroll
@@ -41,7 +56,13 @@ __device__ __forceinline__ void load_phi(const double* __restrict__ phi, const G
 }
 
 template <int K1>
-__device__ __forceinline__ void load_mu(const double* __restrict__ mu, const Geo& g, int x, int y, double* out) {
+__device__ __forceinline__ void load_mu(const double* __restrict__ mu, const Geo& g, int x, int y, double* out,
+                                        int nphase = 0) {
+  if (g.gov && (y < 0 || y >= g.my)) {
+#pragma unroll
+    for (int k = 0; k < K1; k++) out[k] = *ghost_row(g, x, y, g.bc.mu_x, nphase + k);
+    return;
+  }
   const int ix = gp_map(x, g.mx, g.bc.mu_x), iy = gp_map(y, g.my, g.bc.mu_y);
   const double* p = mu + (int64_t)ix * g.pitch + iy;
 #pragma unroll
@@ -481,7 +502,7 @@ __global__ void __launch_bounds__(256) k_dphi(const __grid_constant__ gp_model m
 #pragma unroll
     for (int j = 0; j < 3; j++) load_phi<N>(phi, g, x + i - 1, y + j - 1, P[i][j]);
   double muc[K1];
-  load_mu<K1>(mu, g, x, y, muc);
+  load_mu<K1>(mu, g, x, y, muc, N);
   const double two_dy = 2.0 * m.dy;
   Grads<N> G;
   make_grads<N>(m, P, two_dy, G);
@@ -860,7 +881,9 @@ cudaError_t launch_step(const gp_model& m, const Geo& g, const double* phi, cons
   const dim3 grd_r((g.my + 2 + 31) / 32, (g.mx + 2 + 7) / 8);
   k_dphi<N, K1, SMOOTH><<<grd_r, blk, 0, s>>>(m, g, phi, mu, dphi);
   const dim3 grd((g.my + 31) / 32, (g.mx + 7) / 8);
-  k_update<N, K1, SMOOTH><<<grd, blk, 0, s>>>(m, g, phi, mu, dphi, phi_out, mu_out);
+  Geo gu = g;
+  gu.gov = nullptr;  // the concentration half step reads refreshed ghosts
+  k_update<N, K1, SMOOTH><<<grd, blk, 0, s>>>(m, gu, phi, mu, dphi, phi_out, mu_out);
   return cudaGetLastError();
 }
 
@@ -869,7 +892,7 @@ cudaError_t launch_step(const gp_model& m, const Geo& g, const double* phi, cons
 // Host entry used by the C ABI (gp_capi.cu).  Two launches per step.
 cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch, int64_t rplane,
                         const double* phi, const double* mu, double* dphi, double* phi_out, double* mu_out,
-                        cudaStream_t s, bool smooth) {
+                        cudaStream_t s, bool smooth, const double* ghost_rows) {
   Geo g;
   g.mx = (int)m.mesh_x;
   g.my = (int)m.mesh_y;
@@ -878,6 +901,7 @@ cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch,
   g.rpitch = rpitch;
   g.rplane = rplane;
   g.bc = gp_bc_of(m);
+  g.gov = ghost_rows;
 #define GP_CASE(NN, KK)                                                                           \
   if (m.N == NN && m.K1 == KK)                                                                    \
     return smooth ? launch_step<NN, KK, true>(m, g, phi, mu, dphi, phi_out, mu_out, s)            \

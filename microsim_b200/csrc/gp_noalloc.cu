@@ -35,7 +35,7 @@ extern "C" void gp_set_error(const char* fmt, ...);
 
 cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch, int64_t rplane,
                         const double* phi, const double* mu, double* dphi, double* phi_out, double* mu_out,
-                        cudaStream_t s, bool smooth = false);
+                        cudaStream_t s, bool smooth = false, const double* ghost_rows = nullptr);
 
 static __device__ __align__(256) double g_noalloc_dphi[GP_NOALLOC_SCRATCH_BYTES / sizeof(double)];
 

@@ -673,6 +673,14 @@ int gp_model_from_input(const gp_input *in, gp_model *m) {
         m->Beff[a][i] = (Beq[a][i] + dBbdT[a][i] * (in->T - in->Teq));
         m->Bfill[a][i] = (Beq[a][i] + dBbdT[a][i] * (in->Teq - in->Teq));
       }
+    /* apply_shiftY's liquid rows, functions/shift.h:24-37 with function_F_01_Mu */
+    for (k = 0; k < K1; k++) {
+      const int L = N - 1;
+      double v = 2.0 * in->A[L][k][k] * in->cfill[L][L][k] + (Beq[L][k] + dBbdT[L][k] * (in->Tfill - in->Teq));
+      for (j = 0; j < K1; j++)
+        if (k != j) v += in->A[L][k][j] * in->cfill[L][L][j];
+      m->mu_shift[k] = v;
+    }
   }
   for (a = 0; a < N; a++)
     for (i = 0; i < K1; i++)

@@ -708,6 +708,10 @@ static int one_step(const gpo_params *p, double *phi, double *mu, double *dphi, 
       delta_phi_cell(&c, x, y, dp, smooth);
       for (a = 0; a < N; a++) dphi[a * n + y + x * ry] = dp[a];
     }
+  /* microsim_gp.c:103-106: the boundary copy between the two half steps (a no-op
+   * unless the ghost rows were left stale, as a moving-frame shift leaves them;
+   * the smoothing pre-step is one sweep, solverloop.h:72-90) */
+  if (!smooth) gpo_apply_bc(p, phi, mu);
   /* antitrapping currents on faces touching the interior */
   for (x = 2; x <= rx - 4 && !smooth; x++)
     for (y = 2; y <= ry - 4; y++) {

@@ -205,6 +205,16 @@ int main(int argc, char *argv[]) {
     if (dumping && t == 1) dump_state(dumpdir, "dphi", 1, 1);
     solverloop_concentration(start, end);
     apply_boundary_conditions(0);
+    /* microsim_gp.c:115-125: the moving frame, every 100 steps */
+    if (t % 100 == 0 && SHIFT) {
+      if (MAX_INTERFACE_POS > shiftj) shift_ON = 1;
+      if (shift_ON) {
+        apply_shiftY(gridinfo, MAX_INTERFACE_POS);
+        shift_OFFSET += (MAX_INTERFACE_POS - shiftj);
+        shift_ON = 0;
+      }
+      printf("shift %ld %ld %ld\n", (long)t, (long)MAX_INTERFACE_POS, (long)shift_OFFSET);
+    }
     if (dumping) {
       for (i = 0; i < ndump; i++) {
         if (dump_at[i] == t) dump_state(dumpdir, "state", t, 0);

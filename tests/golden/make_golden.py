@@ -116,6 +116,11 @@ def cases():
                      fills=[("FILLCUBE", [0, 0, 0, 0, 13, 5, 0]), ("FILLCUBE", [1, 14, 0, 0, 27, 5, 0])])
     c.nsmooth = 6
     out["smooth_three_phase_well"] = (c, [1, 15, 30])
+    # moving frame: a planar solid front growing along +y, the window shifted every 100 steps
+    c = C.binary_case(24, 48, gap=1.0, supersat=0.6, eps=4.0, delta=0.02, dt=0.05, tau=1.7776, steps=400)
+    c.fills = [("FILLCUBE", [0, 0, 0, 0, 23, 14, 0])]
+    c.shift, c.shiftj = 1, 20
+    out["shift_planar"] = (c, [1, 100, 200, 300, 400])
     return out
 
 
@@ -143,6 +148,9 @@ def run_case(name, case, dump_steps):
             data[f"phi_{t}"], data[f"mu_{t}"] = phi, mu
         with open(os.path.join(td, "DATA", "out_0.vtk"), "rb") as f:
             data["vtk_0"] = np.frombuffer(f.read(), dtype=np.uint8)
+        shifts = [[int(v) for v in line.split()[1:]] for line in stdout.splitlines() if line.startswith("shift ")]
+        if shifts:  # (step, interface row, accumulated offset) at every shift check
+            data["shifts"] = np.array(shifts)
         stats = [line.split()[1:] for line in stdout.splitlines() if line.startswith("stat ")]
         data["stats"] = np.array([[float(v) for v in s[1:]] for s in stats])
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **data)

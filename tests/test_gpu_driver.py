@@ -33,3 +33,20 @@ def test_driver_output_matches_reference(case):
     assert np.array_equal(phi, interior(g[f"phi_{t}"]))
     assert np.array_equal(mu, interior(g[f"mu_{t}"]))
     assert np.array_equal(phi0, interior(g["phi_0"]))  # the first file is written before any pre-step
+
+
+def test_driver_moving_frame_matches_reference():
+    """Shift = 1 through the driver: the final file and DATA/shift.dat's offset."""
+    g = load_golden("shift_planar")
+    with tempfile.TemporaryDirectory() as d:
+        ip, fp = write_inputs(g, d)
+        r = subprocess.run([mb.DRIVER_PATH, os.path.basename(ip), os.path.basename(fp), "out"], cwd=d,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        inp = mb.Input(ip, fp)
+        m = inp.model()
+        t = int(g["dump_steps"][-1])
+        phi, mu = inp.read_vtk(m, os.path.join(d, "DATA", f"out_{t}.vtk"))
+        lines = open(os.path.join(d, "DATA", "shift.dat")).read().split()
+    assert np.array_equal(phi, interior(g[f"phi_{t}"])) and np.array_equal(mu, interior(g[f"mu_{t}"]))
+    assert int(lines[-2]) == t and int(lines[-1]) == int(g["shifts"][-1][2])
