@@ -190,6 +190,13 @@ int gp_get_stats(gp_ctx *ctx, gp_stats *out);
 int gp_download_dphi(gp_ctx *ctx, double *dphi);
 /* The CUDA stream (cudaStream_t) the context launches on. */
 void *gp_stream(gp_ctx *ctx);
+/* The current state buffers on the device (valid until the next step, smooth
+ * or shift): phi [N][mesh_x][pitch], mu [K1][mesh_x][pitch], plane = elements
+ * per plane, esize = 8 (FP64) or 4 (FP32).  For callers that exchange rows
+ * between contexts (halo rows of a grid split across GPUs); after writing into
+ * them, call gp_state_changed. */
+int gp_state_device(gp_ctx *ctx, void **phi, void **mu, int64_t *pitch, int64_t *plane, int *esize);
+int gp_state_changed(gp_ctx *ctx);
 /* Number of kernel launches this context issued since creation. */
 int64_t gp_launch_count(const gp_ctx *ctx);
 /* ---------------- batches: many independent instances, FP32 chosen form ---------------- */

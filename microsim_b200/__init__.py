@@ -120,6 +120,9 @@ _SIGS = {
     "gp_batch_cells": (C.c_int64, [C.c_void_p]),
     "gp_last_error": (C.c_char_p, []),
     "gp_smooth": (C.c_int, [C.c_void_p, C.c_int64]),
+    "gp_state_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                  C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
+    "gp_state_changed": (C.c_int, [C.c_void_p]),
     "gp_interface_y": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gp_shift_y": (C.c_int, [C.c_void_p, C.c_int64]),
     "gp_adj_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
@@ -264,6 +267,28 @@ class Context:
     def smooth(self, nsteps: int):
         """nsteps smoothing pre-steps (NSMOOTH - 1 in the reference's main)."""
         _check("gp_smooth", lib().gp_smooth(self._h, int(nsteps)))
+
+    def device_state(self):
+        """(phi, mu) torch views [planes, mesh_x, pitch] of the current device
+        buffers (valid until the next step); call state_changed() after writing."""
+        import torch
+        ph, mu_, pitch, plane, es = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int64(), C.c_int()
+        _check("gp_state_device", lib().gp_state_device(self._h, C.byref(ph), C.byref(mu_), C.byref(pitch),
+                                                          C.byref(plane), C.byref(es)))
+        typestr = "<f8" if es.value == 8 else "<f4"
+        mx = int(self.model.mesh_x)
+
+        class _View:
+            def __init__(self, ptr, planes):
+                self.__cuda_array_interface__ = {"shape": (planes, mx, pitch.value), "typestr": typestr,
+                                                 "data": (ptr, False), "version": 3,
+                                                 "strides": (plane.value * es.value, pitch.value * es.value,
+                                                             es.value)}
+        return (torch.as_tensor(_View(ph.value, int(self.model.N)), device="cuda"),
+                torch.as_tensor(_View(mu_.value, int(self.model.K1)), device="cuda"))
+
+    def state_changed(self):
+        _check("gp_state_changed", lib().gp_state_changed(self._h))
 
     def interface_y(self) -> int:
         """Highest upward liquid crossing, ghost-padded row index (check_SHIFT)."""

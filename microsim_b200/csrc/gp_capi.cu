@@ -437,6 +437,23 @@ extern "C" int gp_sync(gp_ctx* c) {
 extern "C" size_t gp_model_sizeof(void) { return sizeof(gp_model); }
 
 extern "C" void* gp_stream(gp_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" int gp_state_device(gp_ctx* c, void** phi, void** mu, int64_t* pitch, int64_t* plane, int* esize) {
+  if (!c || !phi || !mu || !pitch || !plane || !esize) return GP_E_ARG;
+  *phi = c->phi[c->cur];
+  *mu = c->mu[c->cur];
+  *pitch = c->pitch;
+  *plane = c->plane;
+  *esize = (int)c->esize;
+  return GP_OK;
+}
+
+extern "C" int gp_state_changed(gp_ctx* c) {
+  if (!c) return GP_E_ARG;
+  c->have_prev = 0;
+  if (c->f32) GP_CUDA(gp_f32_batch_invalidate(c->f32, c->stream));
+  return GP_OK;
+}
 extern "C" int64_t gp_launch_count(const gp_ctx* c) { return c ? c->launches : 0; }
 
 // ------------------------------------------------------------------ statistics
