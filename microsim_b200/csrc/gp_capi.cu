@@ -29,6 +29,7 @@ void gp_f32_batch_bind(gp_f32_batch* b, int i, float* phiA, float* muA, float* p
 cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty);
 int gp_f32_batch_tiles(const gp_f32_batch* b);
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s);
+const int* gp_f32_batch_error_word(const gp_f32_batch* b);
 cudaError_t gp_f32_batch_invalidate(gp_f32_batch* b, cudaStream_t s);
 cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s, int64_t* lean,
                                     int64_t* lean_cells);
@@ -48,6 +49,12 @@ void gp_f32_tile_shape(int i, int* tx, int* ty);
       return GP_E_CUDA;                                                                    \
     }                                                                                      \
   } while (0)
+
+// The FP32 form's lean kernel gave up on a staged box (bounded wait expired).
+static int lean_error() {
+  gp_set_error("FP32 lean kernel: a staged mu box did not arrive within one second; results are invalid");
+  return GP_E_CUDA;
+}
 
 struct gp_ctx {
   gp_model m;
@@ -560,9 +567,10 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
 
 // Fixed-order final combine of the block partials (deterministic).
 __global__ void k_stats_final(int N, int K1, const double* __restrict__ partials, int nblocks,
-                              double* __restrict__ out) {
+                              double* __restrict__ out, const int* __restrict__ err) {
   const StatLayout L{N, K1};
   const int s = threadIdx.x;
+  if (s == 63) out[63] = err ? (double)*err : 0.0;  // the FP32 form's lean-kernel error word
   if (s >= L.count()) return;
   double v = partials[s];
   for (int b = 1; b < nblocks; b++) v = combine(L, s, v, partials[(int64_t)b * 64 + s]);
@@ -582,12 +590,14 @@ extern "C" int gp_get_stats(gp_ctx* c, gp_stats* out) {
                                                         (const float*)c->phi[prv], (const float*)c->mu[prv],
                                                         c->have_prev, c->pitch, c->plane, c->partials);
   GP_CUDA(cudaGetLastError());
-  k_stats_final<<<1, 64, 0, c->stream>>>(m.N, m.K1, c->partials, c->red_blocks, c->reduced);
+  k_stats_final<<<1, 64, 0, c->stream>>>(m.N, m.K1, c->partials, c->red_blocks, c->reduced,
+                                         c->f32 ? gp_f32_batch_error_word(c->f32) : nullptr);
   GP_CUDA(cudaGetLastError());
   c->launches += 2;
   double v[64];
   GP_CUDA(cudaMemcpyAsync(v, c->reduced, sizeof v, cudaMemcpyDeviceToHost, c->stream));
   GP_CUDA(cudaStreamSynchronize(c->stream));
+  if (v[63] != 0.0) return lean_error();
   const StatLayout L{m.N, m.K1};
   memset(out, 0, sizeof *out);
   for (int a = 0; a < m.N; a++) {
@@ -808,12 +818,14 @@ extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
       m, b->pool + b->off_phi[cur][i], b->pool + b->off_mu[cur][i], b->pool + b->off_phi[prv][i],
       b->pool + b->off_mu[prv][i], b->have_prev, b->pitch[i], b->plane[i], b->partials);
   GP_CUDA(cudaGetLastError());
-  k_stats_final<<<1, 64, 0, b->stream>>>(m.N, m.K1, b->partials, b->red_blocks, b->reduced);
+  k_stats_final<<<1, 64, 0, b->stream>>>(m.N, m.K1, b->partials, b->red_blocks, b->reduced,
+                                         gp_f32_batch_error_word(b->f32));
   GP_CUDA(cudaGetLastError());
   b->launches += 2;
   double v[64];
   GP_CUDA(cudaMemcpyAsync(v, b->reduced, sizeof v, cudaMemcpyDeviceToHost, b->stream));
   GP_CUDA(cudaStreamSynchronize(b->stream));
+  if (v[63] != 0.0) return lean_error();
   const StatLayout L{m.N, m.K1};
   memset(out, 0, sizeof *out);
   for (int a = 0; a < m.N; a++) {

@@ -20,6 +20,7 @@
 // (calculate_fluxes_concentration.h:65) is kept: it is part of the model the
 // reference integrates.
 
+#include <cuda.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -158,7 +159,7 @@ __device__ __forceinline__ void aniso_terms(float dab, float q0, float q1, float
 // 1/dx of the divergence: sum_l (D_c + D_n)_kl * dt/(2 dx^2) * (mu_n - mu_c)_l
 // (calculate_gradients.h:132-185 with functionD.h; hh = Model::hx or hy).
 template <int K1>
-__device__ __forceinline__ void diff_flux(const Model& m, const float (&Dc)[MK][MK], const float (&Dn)[MK][MK],
+__device__ __forceinline__ void diff_flux(const float (&Dc)[MK][MK], const float (&Dn)[MK][MK],
                                           const float* muc, const float* mun, float hh, float* out) {
 #pragma unroll
   for (int k = 0; k < K1; k++) {
@@ -185,7 +186,7 @@ __device__ __forceinline__ void mobility(const Model& m, const float* ph, float 
 }
 
 // net face flux into a cell (the fluxes carry the 1/dx of the divergence)
-__device__ __forceinline__ float flux_div(const Model& m, float fxp, float fxm, float fyp, float fym) {
+__device__ __forceinline__ float flux_div(float fxp, float fxm, float fyp, float fym) {
   return __fadd_rn(__fsub_rn(fxp, fxm), __fsub_rn(fyp, fym));
 }
 
@@ -465,12 +466,12 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
           mr[k] = MU(k, i1, j1 + 1);
         }
         float fxp[K1], fxm[K1], fyp[K1], fym[K1], dc[K1], mnew[K1];
-        diff_flux<K1>(m, Db, Db, mc, mf, m.hx, fxp);
-        diff_flux<K1>(m, Db, Db, mb, mc, m.hx, fxm);
-        diff_flux<K1>(m, Db, Db, mc, mr, m.hy, fyp);
-        diff_flux<K1>(m, Db, Db, ml, mc, m.hy, fym);
+        diff_flux<K1>(Db, Db, mc, mf, m.hx, fxp);
+        diff_flux<K1>(Db, Db, mb, mc, m.hx, fxm);
+        diff_flux<K1>(Db, Db, mc, mr, m.hy, fyp);
+        diff_flux<K1>(Db, Db, ml, mc, m.hy, fym);
 #pragma unroll
-        for (int k = 0; k < K1; k++) dc[k] = flux_div(m, fxp[k], fxm[k], fyp[k], fym[k]);
+        for (int k = 0; k < K1; k++) dc[k] = flux_div(fxp[k], fxm[k], fyp[k], fym[k]);
         bulk_update<N, K1>(m, b0, mc, dc, mnew);
         const int64_t o = (int64_t)x * I.pitch + y;
 #pragma unroll
@@ -784,7 +785,7 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
     float Dc[MK][MK], Dn[MK][MK];
     mobility<N, K1>(m, pc, Dc);
     mobility<N, K1>(m, pn, Dn);
-    diff_flux<K1>(m, Dc, Dn, muc, mun, xface ? m.hx : m.hy, out);
+    diff_flux<K1>(Dc, Dn, muc, mun, xface ? m.hx : m.hy, out);
     if (skip_at) return;
     float tc[N], tn[N], gn[N];
     bool any = false;
@@ -868,7 +869,7 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
 #pragma unroll
       for (int k = 0; k < K1; k++) {
         mu[k] = MU(k, i1, j1);
-        dc[k] = flux_div(m, sfx[(k * (TX + 1) + ti + 1) * TY + tj], sfx[(k * (TX + 1) + ti) * TY + tj],
+        dc[k] = flux_div(sfx[(k * (TX + 1) + ti + 1) * TY + tj], sfx[(k * (TX + 1) + ti) * TY + tj],
                          sfy[(k * TX + ti) * (TY + 1) + tj + 1], sfy[(k * TX + ti) * (TY + 1) + tj]);
       }
       int bulk = -1;
@@ -1018,120 +1019,174 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 
 // inside phase b; phi stays the one-hot field of b and is written only when
 // the output buffer does not hold it already (its purity word says so).
 //
-// One warp per tile.  A row of the tile is G = TY/4 lanes of four cells each;
-// the warp's 32/G lane groups take RG consecutive rows each and stream them
-// along x: each x-face flux is evaluated once and carried to the next row, the
-// y-faces between a lane's cells once, the lane-boundary faces from the
-// neighbour lane's cell (shuffle) -- the same helper calls on the same operands
-// as the full update's pure path, hence the same bits.  A group's RG + 2 mu
-// rows and its halo columns are staged in the warp's shared-memory buffer by
-// asynchronous copies (cp.async), double-buffered: the next tile's rows are in
-// flight while the current tile is computed.  Rows, halo columns and partial
-// tiles go through the boundary map.
+// A warp updates TPW tiles at a time, LP = 32 / TPW lanes per tile.  A tile's
+// mu rows x0-1 .. x0+TX, columns y0-4 .. y0+TY+3, every plane, arrive in
+// shared memory as one TMA box (a tensor map per instance and buffer; cells
+// outside the grid read as zero, and the ghost row/column of a tile at the
+// grid edge is then written from the boundary map).  Each warp keeps a ring
+// of STAGES stages of TPW boxes: while one stage is computed the next
+// STAGES - 1 are loading.
+//
+// A row of a tile is G = TY/4 lanes of four cells each; the tile's LP/G lane
+// groups take RG consecutive rows each and stream them along x: each x-face
+// flux is evaluated once and carried to the next row, the y-faces from the
+// lane's own cells and the neighbouring float4s of the staged row -- the same
+// helper calls on the same operands as the full update's pure path, hence the
+// same bits.
+#ifndef GP_LEAN_STAGES
+#define GP_LEAN_STAGES 2
+#endif
+#ifndef GP_LEAN_WARPS
+#define GP_LEAN_WARPS 4
+#endif
+#ifndef GP_LEAN_TPW
+#define GP_LEAN_TPW 2
+#endif
+
 template <int N, int K1, int TX, int TY>
 struct Lean {
-  static constexpr int G = TY / 4;     // lanes per tile row
-  static constexpr int NG = 32 / G;    // row groups per warp
-  static constexpr int RG = TX / NG;   // rows per group
-  static constexpr int ROWS = RG + 2;  // rows a group stages
-  static constexpr int HALO = NG * ROWS * K1 * TY;      // offset of the halo columns in a buffer
-  static constexpr int BUF = HALO + NG * RG * K1 * 2;   // floats per buffer
-  static constexpr int WARPS = 4;                       // warps per block
-  static constexpr size_t smem = (size_t)WARPS * 2 * BUF * sizeof(float);
-  static_assert(G * NG == 32 && RG * NG == TX, "tile shape");
-  static_assert(HALO % 4 == 0 && BUF % 4 == 0, "16-byte aligned rows");
+  static constexpr int G = TY / 4;                                      // lanes per tile row
+  static constexpr int TPW = GP_LEAN_TPW < 32 / G ? GP_LEAN_TPW : 32 / G;  // tiles per warp
+  static constexpr int LP = 32 / TPW;                                   // lanes per tile
+  static constexpr int NG = LP / G;                                     // row groups per tile
+  static constexpr int RG = TX / NG;                                    // rows per group
+  static constexpr int R = TX + 2;                                      // staged rows: x0-1 .. x0+TX
+  static constexpr int W = TY + 8;                                      // staged row: y0-4 .. y0+TY+3
+  static constexpr int BYTES = K1 * R * W * 4;                          // one box
+  static constexpr int SLOT = (BYTES + 127) / 128 * 128;
+  static constexpr int STAGES = GP_LEAN_STAGES;
+  static constexpr int WARPS = GP_LEAN_WARPS;                           // warps per block
+  static constexpr int ENT = (8 * STAGES + 15) / 16 * 16;              // ring entries after the barriers
+  static constexpr int CTRL = (ENT + 16 * STAGES * TPW + 127) / 128 * 128;
+  static constexpr int WARP_BYTES = STAGES * TPW * SLOT + CTRL;
+  static constexpr size_t smem = (size_t)WARPS * WARP_BYTES + 128;
+  static_assert(G * NG == LP && RG * NG == TX && TPW * LP == 32, "tile shape");
+  static_assert(W <= 256 && R <= 256 && W * 4 % 16 == 0, "TMA box");
 };
 
-// Issue the copies of tile t's mu rows and halo columns into buffer `buf`.
-template <int N, int K1, int TX, int TY>
-__device__ __forceinline__ void lean_stage(const Inst& Ig, int t, float* buf, int lane) {
-  using S = Lean<N, K1, TX, TY>;
-  constexpr int G = S::G, RG = S::RG, ROWS = S::ROWS;
-  const Inst I = Ig;  // one copy into registers
-  const int lt = t - I.tile_begin, x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
-  const int mx = I.mx, my = I.my, lg = lane % G, grp = lane / G, xs = x0 + grp * RG, yb = y0 + 4 * lg;
-  const int64_t pitch = I.pitch, plane = I.plane;
-  const bool edge = lg == 0 || lg == G - 1;
-  float* hdst = buf + S::HALO + grp * RG * K1 * 2 + (lg ? 1 : 0);
-  if (x0 >= 1 && x0 + TX < mx && y0 >= 1 && y0 + TY < my) {  // every staged cell is in the grid
-    const float* src = I.mu + (int64_t)(xs - 1) * pitch + yb;
-    float* dst = buf + grp * ROWS * K1 * TY + 4 * lg;
-#pragma unroll
-    for (int r = 0; r < ROWS; r++) {
-#pragma unroll
-      for (int k = 0; k < K1; k++) cp_async16(dst + (r * K1 + k) * TY, src + k * plane);
-      src += pitch;
-    }
-    if (edge) {
-      const float* h = I.mu + (int64_t)xs * pitch + (lg == 0 ? y0 - 1 : y0 + TY);
-#pragma unroll
-      for (int r = 0; r < RG; r++) {
-#pragma unroll
-        for (int k = 0; k < K1; k++) cp_async4(hdst + (r * K1 + k) * 2, h + k * plane);
-        h += pitch;
-      }
-    }
-    return;
-  }
-  const bool vec = yb + 3 < my;
-#pragma unroll
-  for (int r = 0; r < ROWS; r++) {
-    const float* row = I.mu + (int64_t)gp_map_any(xs - 1 + r, mx, I.bc.mu_x) * pitch;
-#pragma unroll
-    for (int k = 0; k < K1; k++) {
-      float* dst = buf + ((grp * ROWS + r) * K1 + k) * TY + 4 * lg;
-      if (vec) {
-        cp_async16(dst, row + k * plane + yb);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++) cp_async4(dst + j, row + k * plane + gp_map_any(yb + j, my, I.bc.mu_y));
-      }
-    }
-  }
-  if (edge) {
-    const int col = gp_map_any(lg == 0 ? y0 - 1 : y0 + TY, my, I.bc.mu_y);
-#pragma unroll
-    for (int r = 0; r < RG; r++) {
-      const float* src = I.mu + (int64_t)gp_map_any(xs + r, mx, I.bc.mu_x) * pitch + col;
-#pragma unroll
-      for (int k = 0; k < K1; k++) cp_async4(hdst + (r * K1 + k) * 2, src + k * plane);
-    }
-  }
+// Constants of the lean update of one phase of one instance.
+struct alignas(16) LeanConst {
+  float Db[MK][MK], cm[MK][MK], aa[MK][MK], be[MK], hx, hy;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
-// Update tile t from its staged rows.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait for phase `parity` of the barrier to complete; false after one second.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > 1000000000ull) return false;
+  return true;
+}
+
+// One 3-D box (columns, rows, planes) from the tensor map into shared memory,
+// completing on the barrier.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
+                                            int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Write the ghost row/column of a tile at the grid edge into its staged box:
+// the boundary map's source cell, from the box when it lies there, else from
+// global memory (periodic partners).  Called by the whole warp; `on` says
+// whether the lane's tile needs it, `sub` is the lane's index in its tile.
 template <int N, int K1, int TX, int TY>
-__device__ __forceinline__ void lean_compute(const Inst& Ig, const Model* __restrict__ models,
-                                             uint32_t* __restrict__ flags_out, int t, int b, const float* buf,
-                                             int lane) {
+__device__ __forceinline__ void lean_ghosts(bool on, const Inst& I, int x0, int y0, float* buf, int sub) {
   using S = Lean<N, K1, TX, TY>;
-  constexpr int G = S::G, RG = S::RG, ROWS = S::ROWS;
-  const Inst I = Ig;  // one copy into registers
-  const int lt = t - I.tile_begin, x0 = (lt / I.tiles_y) * TX, y0 = (lt % I.tiles_y) * TY;
-  const int mx = I.mx, my = I.my, lg = lane % G, grp = lane / G, xs = x0 + grp * RG, yb = y0 + 4 * lg;
-  const int xend = min(x0 + TX, mx);
+  constexpr int R = S::R, W = S::W, LP = S::LP;
+  const int mx = I.mx, my = I.my;
+  const int ex = min(TX, mx - x0), ey = min(TY, my - y0);
+  // ghost rows x0 - 1 (box row 0) and x0 + ex (box row ex + 1), over the tile's columns
+  for (int side = 0; side < 2; side++) {
+    const int gx = side ? x0 + ex : x0 - 1;
+    if (on && (side ? gx >= mx : gx < 0)) {
+      const int src = gp_map_any(gx, mx, I.bc.mu_x), sr = src - x0 + 1, dr = gx - x0 + 1;
+      const bool in_box = sr >= 1 && sr <= ex;
+      for (int c = sub; c < ey; c += LP)
+#pragma unroll
+        for (int k = 0; k < K1; k++)
+          buf[(k * R + dr) * W + 4 + c] =
+              in_box ? buf[(k * R + sr) * W + 4 + c] : I.mu[k * I.plane + (int64_t)src * I.pitch + y0 + c];
+    }
+  }
+  __syncwarp();
+  // ghost columns y0 - 1 (box column 3) and y0 + ey (box column ey + 4), over the tile's rows
+  for (int side = 0; side < 2; side++) {
+    const int gy = side ? y0 + ey : y0 - 1;
+    if (on && (side ? gy >= my : gy < 0)) {
+      const int src = gp_map_any(gy, my, I.bc.mu_y), sc = src - y0 + 4, dc = gy - y0 + 4;
+      const bool in_box = sc >= 4 && sc < 4 + ey;
+      for (int r = sub; r < ex; r += LP)
+#pragma unroll
+        for (int k = 0; k < K1; k++)
+          buf[(k * R + r + 1) * W + dc] =
+              in_box ? buf[(k * R + r + 1) * W + sc] : I.mu[k * I.plane + (int64_t)(x0 + r) * I.pitch + src];
+    }
+  }
+  __syncwarp();
+}
+
+// Update tile (x0, y0) of instance I from its staged box (`sub`: the lane's
+// index in the tile).  A tile inside the grid stores its rows without bounds
+// tests; an edge tile tests rows and columns.  The phi of a tile whose output
+// buffer does not hold the one-hot field of b yet is written in a second pass.
+template <int N, int K1, int TX, int TY>
+__device__ __forceinline__ void lean_compute(const Inst& I, const LeanConst& C, bool write_phi, int b, int x0, int y0,
+                                             const float* buf, int sub) {
+  using S = Lean<N, K1, TX, TY>;
+  constexpr int G = S::G, RG = S::RG, R = S::R, W = S::W;
+  const int lg = sub % G, grp = sub / G, xs = x0 + grp * RG, yb = y0 + 4 * lg;
+  const int mx = I.mx, my = I.my;
+  const bool full = x0 + TX <= mx && y0 + TY <= my;
   const int64_t pitch = I.pitch, plane = I.plane;
-  float* const mu_out = I.mu_out;
-  float* const phi_out = I.phi_out;
-  const bool vec = yb + 3 < my;
-  // the phase's constants, once per tile into registers
-  const Model& m = models[I.model];
-  const float hx = m.hx, hy = m.hy;
+  float* const out = I.mu_out + (int64_t)xs * pitch + yb;
+  const float* const sb = buf + grp * RG * W + 4 + 4 * lg;  // the group's first staged row, the lane's first cell
+  const float hx = C.hx, hy = C.hy;
   float Db[MK][MK], cm[MK][MK], be[MK], aa[MK][MK];
 #pragma unroll
-  for (int a = 0; a < N; a++)
-    if (a == b) {
+  for (int k = 0; k < K1; k++) {
+    be[k] = C.be[k];
 #pragma unroll
-      for (int k = 0; k < K1; k++)
-#pragma unroll
-        for (int l = 0; l < K1; l++) Db[k][l] = m.DC[a][k][l];
+    for (int l = 0; l < K1; l++) {
+      Db[k][l] = C.Db[k][l];
+      cm[k][l] = C.cm[k][l];
+      aa[k][l] = C.aa[k][l];
     }
-  phase_consts<N, K1>(m, b, cm, be, aa);
-  const bool write_phi = pf(flags_out[t], PF_CORE) != 1 + b;
+  }
   auto row = [&](int r, float (&v)[4][K1]) {
 #pragma unroll
     for (int k = 0; k < K1; k++) {
-      const float4 q = *reinterpret_cast<const float4*>(buf + ((grp * ROWS + r) * K1 + k) * TY + 4 * lg);
+      const float4 q = *reinterpret_cast<const float4*>(sb + (k * R + r) * W);
       v[0][k] = q.x;
       v[1][k] = q.y;
       v[2][k] = q.z;
@@ -1144,115 +1199,193 @@ __device__ __forceinline__ void lean_compute(const Inst& Ig, const Model* __rest
     row(0, prev);
     row(1, cur);
 #pragma unroll
-    for (int j = 0; j < 4; j++) diff_flux<K1>(m, Db, Db, prev[j], cur[j], hx, fxm[j]);
+    for (int j = 0; j < 4; j++) diff_flux<K1>(Db, Db, prev[j], cur[j], hx, fxm[j]);
   }
-#pragma unroll
-  for (int r = 0; r < RG; r++) {
-    const int x = xs + r;
+  // the new mu of the lane's four cells in group row r (box row r + 1); advances cur and fxm
+  auto step = [&](int r, float (&mnew)[4][K1]) {
     float nx[4][K1], left[K1], right[K1], fy[5][K1];
     row(r + 2, nx);
 #pragma unroll
     for (int k = 0; k < K1; k++) {
-      const float up = __shfl_up_sync(0xffffffffu, cur[3][k], 1, G);
-      const float dn = __shfl_down_sync(0xffffffffu, cur[0][k], 1, G);
-      const float h = buf[S::HALO + ((grp * RG + r) * K1 + k) * 2 + (lg ? 1 : 0)];
-      left[k] = lg == 0 ? h : up;
-      right[k] = lg == G - 1 ? h : dn;
+      left[k] = sb[(k * R + r + 1) * W - 1];
+      right[k] = sb[(k * R + r + 1) * W + 4];
     }
-    diff_flux<K1>(m, Db, Db, left, cur[0], hy, fy[0]);
+    diff_flux<K1>(Db, Db, left, cur[0], hy, fy[0]);
 #pragma unroll
-    for (int j = 0; j < 3; j++) diff_flux<K1>(m, Db, Db, cur[j], cur[j + 1], hy, fy[j + 1]);
-    diff_flux<K1>(m, Db, Db, cur[3], right, hy, fy[4]);
-    float mnew[4][K1];
+    for (int j = 0; j < 3; j++) diff_flux<K1>(Db, Db, cur[j], cur[j + 1], hy, fy[j + 1]);
+    diff_flux<K1>(Db, Db, cur[3], right, hy, fy[4]);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       float fxp[K1], dc[K1];
-      diff_flux<K1>(m, Db, Db, cur[j], nx[j], hx, fxp);
+      diff_flux<K1>(Db, Db, cur[j], nx[j], hx, fxp);
 #pragma unroll
       for (int k = 0; k < K1; k++) {
-        dc[k] = flux_div(m, fxp[k], fxm[j][k], fy[j + 1][k], fy[j][k]);
+        dc[k] = flux_div(fxp[k], fxm[j][k], fy[j + 1][k], fy[j][k]);
         fxm[j][k] = fxp[k];
       }
       bulk_update_v<K1>(cm, be, aa, cur[j], dc, mnew[j]);
-    }
-    if (x < xend) {
-      const int64_t o = (int64_t)x * pitch + yb;
-      if (vec) {
-#pragma unroll
-        for (int k = 0; k < K1; k++)
-          *reinterpret_cast<float4*>(mu_out + o + k * plane) =
-              make_float4(mnew[0][k], mnew[1][k], mnew[2][k], mnew[3][k]);
-        if (write_phi) {
-#pragma unroll
-          for (int a = 0; a < N; a++) {
-            const float v = a == b ? 1.f : 0.f;
-            *reinterpret_cast<float4*>(phi_out + o + a * plane) = make_float4(v, v, v, v);
-          }
-        }
-      } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (yb + j < my) {
-#pragma unroll
-            for (int k = 0; k < K1; k++) mu_out[o + j + k * plane] = mnew[j][k];
-            if (write_phi) {
-#pragma unroll
-              for (int a = 0; a < N; a++) phi_out[o + j + a * plane] = a == b ? 1.f : 0.f;
-            }
-          }
-      }
     }
 #pragma unroll
     for (int j = 0; j < 4; j++)
 #pragma unroll
       for (int k = 0; k < K1; k++) cur[j][k] = nx[j][k];
+  };
+  if (full) {
+#pragma unroll
+    for (int r = 0; r < RG; r++) {
+      float mnew[4][K1];
+      step(r, mnew);
+#pragma unroll
+      for (int k = 0; k < K1; k++)
+        __stwb(reinterpret_cast<float4*>(out + r * pitch + k * plane),
+               make_float4(mnew[0][k], mnew[1][k], mnew[2][k], mnew[3][k]));
+    }
+  } else {
+    const bool vec = yb + 3 < my;
+#pragma unroll
+    for (int r = 0; r < RG; r++) {
+      float mnew[4][K1];
+      step(r, mnew);
+      if (xs + r < mx) {
+        if (vec) {
+#pragma unroll
+          for (int k = 0; k < K1; k++)
+            __stwb(reinterpret_cast<float4*>(out + r * pitch + k * plane),
+                   make_float4(mnew[0][k], mnew[1][k], mnew[2][k], mnew[3][k]));
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (yb + j < my) {
+#pragma unroll
+              for (int k = 0; k < K1; k++) out[r * pitch + k * plane + j] = mnew[j][k];
+            }
+        }
+      }
+    }
   }
-  __syncwarp();
-  if (lane == 0) flags_out[t] = pf_all(1 + b);
+  if (write_phi) {
+    float* const po = I.phi_out + (int64_t)xs * pitch + yb;
+    for (int r = 0; r < RG && xs + r < mx; r++)
+#pragma unroll
+      for (int a = 0; a < N; a++) {
+        const float v = a == b ? 1.f : 0.f;
+        if (yb + 3 < my) {
+          *reinterpret_cast<float4*>(po + r * pitch + a * plane) = make_float4(v, v, v, v);
+        } else {
+          for (int j = 0; j < 4 && yb + j < my; j++) po[r * pitch + a * plane + j] = v;
+        }
+      }
+  }
 }
 
 // The lean tiles of one step.  Warps scan the tiles w, w + W, w + 2W, ...
 // (W = warps of the grid), 32 candidates per ballot, and update the accepted
-// ones, staging the next tile while computing the current one.
+// ones TPW at a time through the ring of staged boxes.  With `reverse` the
+// scan runs from the last tile down: steps alternate the direction, so a step
+// starts on the tiles the previous step wrote last, whose mu is still in L2.  A stage whose boxes
+// have not arrived after one second sets *err; the warp then waits (bounded)
+// for its other boxes and returns.
 template <int N, int K1, int TX, int TY>
-__global__ void __launch_bounds__(128) k_lean32(const Inst* __restrict__ insts, const Model* __restrict__ models,
-                                                const int* __restrict__ tile_inst,
-                                                const uint32_t* __restrict__ flags_in,
-                                                uint32_t* __restrict__ flags_out, int total) {
+__global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
+    k_lean32(const Inst* __restrict__ insts, const LeanConst* __restrict__ lconst,
+             const CUtensorMap* __restrict__ tmaps, const int* __restrict__ tile_inst,
+             const uint32_t* __restrict__ flags_in, uint32_t* __restrict__ flags_out, int total, int reverse,
+             int* __restrict__ err) {
   using S = Lean<N, K1, TX, TY>;
-  extern __shared__ __align__(16) float lsm[];
-  const int lane = threadIdx.x & 31;
-  float* wbuf = lsm + (threadIdx.x >> 5) * 2 * S::BUF;
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  constexpr int STAGES = S::STAGES, TPW = S::TPW, LP = S::LP;
+  static_assert(STAGES >= 2, "a stage loads while another is computed");
+  extern __shared__ __align__(16) unsigned char lsm_raw[];
+  unsigned char* lsm = lsm_raw + ((128 - (smem_u32(lsm_raw) & 127)) & 127);
+  const int lane = threadIdx.x & 31, q = lane / LP, sub = lane % LP;
+  unsigned char* wsm = lsm + (threadIdx.x >> 5) * S::WARP_BYTES;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(wsm);          // [STAGES]
+  int4* ent = reinterpret_cast<int4*>(wsm + S::ENT);         // [STAGES][TPW] {tile, inst * 8 + phase, x0, y0}
+  float* slots = reinterpret_cast<float*>(wsm + S::CTRL);    // [STAGES][TPW][SLOT / 4]
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t base = gw; base < total; base += 32 * nwarp) {
-    const int64_t tc = base + lane * nwarp;
-    int bc = -1;
-    if (tc < total) bc = lean_phase(flags_in, insts[tile_inst[tc]], (int)tc, TX, TY);
-    unsigned todo = __ballot_sync(0xffffffffu, bc >= 0);
-    if (!todo) continue;
-    int src = __ffs(todo) - 1;
-    todo &= todo - 1;
-    int t = (int)(base + src * nwarp), b = __shfl_sync(0xffffffffu, bc, src);
-    lean_stage<N, K1, TX, TY>(insts[tile_inst[t]], t, wbuf, lane);
-    cp_async_commit();
-    for (int i = 0; t >= 0; i++) {
-      int tn = -1, bn = -1;
-      if (todo) {
-        src = __ffs(todo) - 1;
-        todo &= todo - 1;
-        tn = (int)(base + src * nwarp);
-        bn = __shfl_sync(0xffffffffu, bc, src);
-        lean_stage<N, K1, TX, TY>(insts[tile_inst[tn]], tn, wbuf + ((i + 1) & 1) * S::BUF, lane);
+  int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) - 32 * nwarp;
+  unsigned todo = 0;
+  int mine = -1, mx0 = 0, my0 = 0;  // this lane's candidate: inst * 8 + phase (or -1), its origin
+  if (lane == 0) {
+    for (int s = 0; s < STAGES; s++) mbar_init(&bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncwarp();
+  // the next accepted tile of this warp (warp-uniform), tile -1 when none is left
+  auto next = [&]() -> int4 {
+    while (!todo) {
+      base += 32 * nwarp;
+      if (base >= total) return make_int4(-1, 0, 0, 0);
+      int64_t tc = base + lane * nwarp;
+      if (reverse) tc = total - 1 - tc;
+      mine = -1;
+      if (tc >= 0 && tc < total) {
+        const int inst = tile_inst[tc];
+        const Inst& I = insts[inst];
+        const int bc = lean_phase(flags_in, I, (int)tc, TX, TY);
+        if (bc >= 0) {
+          const int lt = (int)tc - I.tile_begin, ny = I.tiles_y;
+          mine = inst * 8 + bc;
+          mx0 = (lt / ny) * TX;
+          my0 = (lt % ny) * TY;
+        }
       }
-      cp_async_commit();
-      cp_async_wait_prev();  // all but the copies just issued: tile t is staged
-      __syncwarp();
-      lean_compute<N, K1, TX, TY>(insts[tile_inst[t]], models, flags_out, t, b, wbuf + (i & 1) * S::BUF, lane);
-      __syncwarp();  // buffer (i & 1) is reused by the copies issued in iteration i + 1
-      t = tn;
-      b = bn;
+      todo = __ballot_sync(0xffffffffu, mine >= 0);
     }
+    const int src = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const int t = (int)(base + src * nwarp);
+    return make_int4(reverse ? total - 1 - t : t, __shfl_sync(0xffffffffu, mine, src),
+                     __shfl_sync(0xffffffffu, mx0, src), __shfl_sync(0xffffffffu, my0, src));
+  };
+  // record the next TPW tiles in stage s and start their boxes
+  auto fill = [&](int s) {
+    int4 e[TPW];
+    int nv = 0;
+#pragma unroll
+    for (int j = 0; j < TPW; j++) {
+      e[j] = next();
+      nv += e[j].x >= 0;
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int j = 0; j < TPW; j++) ent[s * TPW + j] = e[j];
+      if (nv) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(&bar[s], nv * S::BYTES);
+#pragma unroll
+        for (int j = 0; j < TPW; j++)
+          if (e[j].x >= 0)
+            tma_load_3d(slots + (s * TPW + j) * (S::SLOT / 4), &tmaps[e[j].y >> 3], &bar[s], e[j].w - 4,
+                        e[j].z - 1, 0);
+      }
+    }
+  };
+  for (int s = 0; s < STAGES - 1; s++) fill(s);
+  __syncwarp();
+  uint32_t phase = 0;  // bit s: parity of stage s's next completion
+  for (int s = 0;; s = s + 1 == STAGES ? 0 : s + 1) {
+    if (ent[s * TPW].x < 0) break;  // stages fill in order: nothing is left
+    const int4 e = ent[s * TPW + q];
+    fill(s == 0 ? STAGES - 1 : s - 1);  // the stage computed in the previous pass
+    const bool own = e.x >= 0;
+    const int inst = own ? e.y >> 3 : 0, b = e.y & 7;
+    const Inst I = insts[inst];
+    const LeanConst C = lconst[inst * N + b];
+    const bool write_phi = own && pf(flags_out[e.x], PF_CORE) != 1 + b;
+    if (!mbar_wait(&bar[s], (phase >> s) & 1)) {
+      if (lane == 0) atomicExch(err, 1);
+      __syncwarp();
+      for (int j = 0; j < STAGES; j++)  // every stage with boxes in flight
+        if (ent[j * TPW].x >= 0) mbar_wait(&bar[j], (phase >> j) & 1);
+      return;
+    }
+    phase ^= 1u << s;
+    float* buf = slots + (s * TPW + q) * (S::SLOT / 4);
+    const bool edge = own && (e.z == 0 || e.z + TX >= I.mx || e.w == 0 || e.w + TY >= I.my);
+    if (__any_sync(0xffffffffu, edge)) lean_ghosts<N, K1, TX, TY>(edge, I, e.z, e.w, buf, sub);
+    if (own) lean_compute<N, K1, TX, TY>(I, C, write_phi, b, e.z, e.w, buf, sub);
+    __syncwarp();
+    if (own && sub == 0) flags_out[e.x] = pf_all(1 + b);
   }
 }
 
@@ -1334,7 +1467,8 @@ using namespace gp32;
 // Kernels of one (N, K1, anisotropy, tile shape).
 struct KernelSet {
   void (*general)(const Inst*, const Model*, const int*, const int*, int*, uint32_t*);
-  void (*lean)(const Inst*, const Model*, const int*, const uint32_t*, uint32_t*, int);
+  void (*lean)(const Inst*, const LeanConst*, const CUtensorMap*, const int*, const uint32_t*, uint32_t*, int, int,
+               int*);
   void (*list)(const Inst*, const int*, const uint32_t*, int, int*, int*);
   size_t smem_general, smem_lean;
 };
@@ -1392,6 +1526,9 @@ struct gp_f32_batch {
   std::vector<Inst> hinst[2];  // [buffer parity]
   Inst* dinst[2] = {nullptr, nullptr};
   Model* dmodel = nullptr;
+  LeanConst* dlconst = nullptr;                 // [n][N] lean-update constants of each phase
+  CUtensorMap* dtmap[2] = {nullptr, nullptr};  // [parity][n] mu boxes of the lean kernel
+  int* derr = nullptr;                          // lean kernel: a staged box did not arrive
   int total_tiles = 0;
   KernelSet ks;
   uint32_t* dflags = nullptr;  // [2][total_tiles] purity words of the state in buffer p
@@ -1435,8 +1572,29 @@ cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** ou
   b->gm.assign(models, models + n);
   std::vector<Model> hm(n);
   for (int i = 0; i < n; i++) hm[i] = make_model(models[i]);
+  std::vector<LeanConst> hl((size_t)n * b->N);
+  for (int i = 0; i < n; i++)
+    for (int a = 0; a < b->N; a++) {
+      LeanConst& L = hl[(size_t)i * b->N + a];
+      memset(&L, 0, sizeof L);
+      for (int k = 0; k < MK; k++) {
+        L.be[k] = hm[i].Beff[a][k];
+        for (int l = 0; l < MK; l++) {
+          L.Db[k][l] = hm[i].DC[a][k][l];
+          L.cm[k][l] = hm[i].cmu[a][k][l];
+          L.aa[k][l] = hm[i].A[a][k][l];
+        }
+      }
+      L.hx = hm[i].hx;
+      L.hy = hm[i].hy;
+    }
   cudaError_t e = cudaMalloc(&b->dmodel, sizeof(Model) * n);
   if (e == cudaSuccess) e = cudaMemcpy(b->dmodel, hm.data(), sizeof(Model) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dlconst, sizeof(LeanConst) * hl.size());
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->dlconst, hl.data(), sizeof(LeanConst) * hl.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&b->derr, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->derr, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&b->dcnt, 4 * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(b->dcnt, 0, 4 * sizeof(int));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
@@ -1445,6 +1603,7 @@ cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** ou
   for (int p = 0; e == cudaSuccess && p < 2; p++) {
     b->hinst[p].resize(n);
     e = cudaMalloc(&b->dinst[p], sizeof(Inst) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&b->dtmap[p], sizeof(CUtensorMap) * n);
   }
   if (e != cudaSuccess) {
     gp_f32_batch_destroy(b);
@@ -1460,6 +1619,10 @@ void gp_f32_batch_destroy(gp_f32_batch* b) {
   cudaFree(b->dmodel);
   cudaFree(b->dinst[0]);
   cudaFree(b->dinst[1]);
+  cudaFree(b->dtmap[0]);
+  cudaFree(b->dtmap[1]);
+  cudaFree(b->dlconst);
+  cudaFree(b->derr);
   free_tiles(b);
   cudaFree(b->dcnt);
   for (cudaEvent_t ev : b->tev) cudaEventDestroy(ev);
@@ -1496,6 +1659,44 @@ cudaError_t gp_f32_batch_invalidate(gp_f32_batch* b, cudaStream_t s) {
 
 void gp_f32_batch_set_narrowband(gp_f32_batch* b, int on) { b->narrowband = on ? 1 : 0; }
 
+// cuTensorMapEncodeTiled, from the driver (the runtime does not wrap it).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)f;
+  }
+  return fn;
+}
+
+// The lean kernel's mu box of every instance read at parity p: a 3-D tensor
+// (columns, rows, planes) over the instance's input mu, box (TY + 8) x (TX + 2)
+// x K1 starting at (y0 - 4, x0 - 1, 0); cells outside the grid read as zero.
+static cudaError_t encode_boxes(gp_f32_batch* b, int p) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return cudaErrorNotSupported;
+  std::vector<CUtensorMap> maps(b->n);
+  for (int i = 0; i < b->n; i++) {
+    const Inst& I = b->hinst[p][i];
+    const cuuint64_t dim[3] = {(cuuint64_t)I.my, (cuuint64_t)I.mx, (cuuint64_t)b->K1};
+    const cuuint64_t stride[2] = {(cuuint64_t)I.pitch * 4, (cuuint64_t)I.plane * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)b->ty + 8, (cuuint32_t)b->tx + 2, (cuuint32_t)b->K1};
+    const cuuint32_t estride[3] = {1, 1, 1};
+    if (enc(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)I.mu, dim, stride, box, estride,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return cudaErrorInvalidValue;
+  }
+  return cudaMemcpy(b->dtmap[p], maps.data(), sizeof(CUtensorMap) * b->n, cudaMemcpyHostToDevice);
+}
+
 // Recompute the tile decomposition for shape (tx, ty) and upload the instance tables.
 cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   KernelSet ks;
@@ -1518,6 +1719,7 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   b->total_tiles = t;
   for (int p = 0; p < 2; p++) {
     cudaError_t e = cudaMemcpy(b->dinst[p], b->hinst[p].data(), sizeof(Inst) * b->n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = encode_boxes(b, p);
     if (e != cudaSuccess) return e;
   }
   free_tiles(b);
@@ -1535,7 +1737,8 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   e = cudaFuncSetAttribute(ks.general, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_general);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, ks.general, 256, ks.smem_general);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(ks.lean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_lean);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, ks.lean, 128, ks.smem_lean);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, ks.lean, 32 * GP_LEAN_WARPS, ks.smem_lean);
   if (e != cudaSuccess) return e;
   b->grid_general = sms * (occ_g > 0 ? occ_g : 1);
   b->grid_lean = sms * (occ_l > 0 ? occ_l : 1);
@@ -1625,8 +1828,8 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
     if ((e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess) return e;
   }
   if (E && ((e = cudaEventRecord(E[0], ls)) != cudaSuccess)) return e;
-  k.lean<<<b->grid_lean, 128, k.smem_lean, ls>>>(b->dinst[p], b->dmodel, b->dtile_inst, flags_in, flags_out,
-                                                 b->total_tiles);
+  k.lean<<<b->grid_lean, 32 * GP_LEAN_WARPS, k.smem_lean, ls>>>(b->dinst[p], b->dlconst, b->dtmap[p], b->dtile_inst, flags_in,
+                                                 flags_out, b->total_tiles, p, b->derr);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E && ((e = cudaEventRecord(E[1], ls)) != cudaSuccess)) return e;
   if (E && ((e = cudaEventRecord(E[2], s)) != cudaSuccess)) return e;
@@ -1667,6 +1870,9 @@ cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s,
   *lean_cells = c;
   return cudaSuccess;
 }
+
+// device word set by a lean kernel whose staged box did not arrive (0 = none)
+const int* gp_f32_batch_error_word(const gp_f32_batch* b) { return b->derr; }
 
 // kernel launches one gp_f32_batch_launch issues
 int gp_f32_batch_launches_per_step(const gp_f32_batch* b) { return b->narrowband ? 3 : 1; }

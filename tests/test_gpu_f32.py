@@ -172,7 +172,8 @@ def test_tip_velocity_within_half_percent_of_fp64():
 def test_narrow_band_is_bit_identical_to_the_full_kernel():
     """Tiles sent to the lean pure-phase kernel get the same bits as from the
     full kernel, for every tile shape: Neumann borders (mirrored rings), a
-    periodic batch member (wrapped rings are never trusted), partial edge tiles
+    periodic batch member (wrapped rings are never trusted), a periodic mu under
+    Neumann phi (ghosts of lean edge tiles from the far side), partial edge tiles
     with fewer than three cells on an axis, the skipped phi writes, and a
     re-upload in mid-run (purity words reset)."""
     cases = [configs.binary_case(200, 150, gap=1.0, supersat=0.55, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
@@ -182,6 +183,12 @@ def test_narrow_band_is_bit_identical_to_the_full_kernel():
              configs.binary_case(98, 130, gap=1.0, supersat=0.5, eps=4.0, delta=0.01, dt=0.05, tau=1.7776,
                                  seed=(49, 65, 7.0))]
     loaded = [mb.load_case(c) for c in cases]
+    # Neumann phi with a periodic mu: the lean tiles' ghost rows/columns come from the far side
+    m4, p4, u4 = mb.load_case(cases[0])
+    m4 = m4.copy()
+    for i in range(4):
+        m4.bc_mu[i] = 3
+    loaded.append((m4, p4, u4))
     models = [m for m, _, _ in loaded]
 
     def run(on, tile, reupload=False):
