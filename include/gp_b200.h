@@ -225,6 +225,12 @@ int gp_batch_set_narrowband(gp_batch *b, int on);
  * the interior cells of those lean tiles (diagnostics; synchronises the
  * batch's stream). */
 int gp_batch_lean_tiles(gp_batch *b, int64_t *lean, int64_t *total, int64_t *lean_cells);
+/* Blocks per SM of the two persistent grids (lean kernel, full kernel); 0 =
+ * as many as fit.  The kernels run concurrently, so a lean grid below its
+ * occupancy leaves every SM room for full-kernel blocks beside it.
+ * gp_batch_get_grids also reports the occupancies. */
+int gp_batch_set_grids(gp_batch *b, int lean_per_sm, int general_per_sm);
+int gp_batch_get_grids(gp_batch *b, int *lean_per_sm, int *general_per_sm, int *occ_lean, int *occ_general);
 /* Per-kernel timing (diagnostics): while on, steps launch directly (no graph
  * replay), their kernels one after the other on the batch's stream, and record
  * CUDA events around each kernel; gp_batch_kernel_ms gives
@@ -232,9 +238,10 @@ int gp_batch_lean_tiles(gp_batch *b, int64_t *lean, int64_t *total, int64_t *lea
  * full kernel (ms3[0..2]) over the steps since timing was switched on. */
 int gp_batch_set_timing(gp_batch *b, int on);
 int gp_batch_kernel_ms(gp_batch *b, double *ms3, int64_t *steps);
-/* Measured sweep over the tile shapes on the batch's own state (restored
- * afterwards); the winner is cached in cache_path (may be NULL) per batch
- * signature and read back on the next call. */
+/* Measured sweep over the tile shapes, each with the lean grid at its
+ * occupancy and one block per SM below it, on the batch's own state (restored
+ * afterwards); the winner is applied and cached in cache_path (may be NULL)
+ * per batch signature, read back on the next call. */
 int gp_batch_autotune(gp_batch *b, const char *cache_path, int *tx, int *ty);
 void *gp_batch_stream(gp_batch *b);
 int64_t gp_batch_launch_count(const gp_batch *b);

@@ -110,6 +110,9 @@ _SIGS = {
     "gp_batch_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(GpStats)]),
     "gp_batch_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gp_batch_set_narrowband": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_batch_set_grids": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "gp_batch_get_grids": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int)]),
     "gp_batch_lean_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                       C.POINTER(C.c_int64)]),
     "gp_batch_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
@@ -386,6 +389,16 @@ class Batch:
 
     def set_narrowband(self, on: bool):
         _check("gp_batch_set_narrowband", lib().gp_batch_set_narrowband(self._h, 1 if on else 0))
+
+    def set_grids(self, lean_per_sm: int = 0, general_per_sm: int = 0):
+        """Blocks per SM of the lean and full persistent grids (0: as many as fit)."""
+        _check("gp_batch_set_grids", lib().gp_batch_set_grids(self._h, lean_per_sm, general_per_sm))
+
+    def grids(self):
+        """(lean blocks per SM, full blocks per SM, lean occupancy, full occupancy)."""
+        v = [C.c_int() for _ in range(4)]
+        _check("gp_batch_get_grids", lib().gp_batch_get_grids(self._h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
 
     def lean_tiles(self):
         """(tiles the next step updates with the lean kernel, all tiles)."""

@@ -30,6 +30,9 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty);
 int gp_f32_batch_tiles(const gp_f32_batch* b);
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s);
 const int* gp_f32_batch_error_word(const gp_f32_batch* b);
+void gp_f32_batch_set_grids(gp_f32_batch* b, int lean_per_sm, int general_per_sm);
+void gp_f32_batch_get_grids(const gp_f32_batch* b, int* lean_per_sm, int* general_per_sm, int* occ_lean,
+                            int* occ_general);
 cudaError_t gp_f32_batch_invalidate(gp_f32_batch* b, cudaStream_t s);
 cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s, int64_t* lean,
                                     int64_t* lean_cells);
@@ -871,15 +874,16 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
     if (f) {
       char line[256];
       while (fgets(line, sizeof line, f)) {
-        int N, K1, an, n, tx, ty;
+        int N, K1, an, n, tx, ty, lp;
         long long c;
         double ms;
-        if (sscanf(line, "%d %d %d %lld %d %d %d %lf", &N, &K1, &an, &c, &n, &tx, &ty, &ms) == 8 && N == m0.N &&
-            K1 == m0.K1 && an == m0.anisotropy && c == cells && n == b->n) {
+        if (sscanf(line, "%d %d %d %lld %d %d %d %d %lf", &N, &K1, &an, &c, &n, &tx, &ty, &lp, &ms) == 9 &&
+            N == m0.N && K1 == m0.K1 && an == m0.anisotropy && c == cells && n == b->n) {
           fclose(f);
           if (tx_out) *tx_out = tx;
           if (ty_out) *ty_out = ty;
-          return gp_batch_set_tile(b, tx, ty);
+          int rc = gp_batch_set_tile(b, tx, ty);
+          return rc == GP_OK ? gp_batch_set_grids(b, lp, 0) : rc;
         }
       }
       fclose(f);
@@ -893,25 +897,34 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   cudaEvent_t e0, e1;
   GP_CUDA(cudaEventCreate(&e0));
   GP_CUDA(cudaEventCreate(&e1));
-  int best_tx = b->tx, best_ty = b->ty;
+  int best_tx = b->tx, best_ty = b->ty, best_lp = 0;
   float best = 1e30f;
   for (int s = 0; s < gp_f32_tile_shape_count(); s++) {
     int tx, ty;
     gp_f32_tile_shape(s, &tx, &ty);
     if (gp_batch_set_tile(b, tx, ty) != GP_OK) continue;
-    for (int w = 0; w < 3; w++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (w & 1), b->stream));
-    GP_CUDA(cudaEventRecord(e0, b->stream));
-    for (int r = 0; r < 10; r++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (r & 1), b->stream));
-    GP_CUDA(cudaEventRecord(e1, b->stream));
-    GP_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    GP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    b->launches += 13 * gp_f32_batch_launches_per_step(b->f32);
-    if (ms < best) {
-      best = ms;
-      best_tx = tx;
-      best_ty = ty;
+    int lp0, gp0, occ_l, occ_g;
+    gp_f32_batch_get_grids(b->f32, &lp0, &gp0, &occ_l, &occ_g);
+    // lean grid at occupancy, or one block per SM short of it (room for full-kernel blocks)
+    for (int c = 0; c < (occ_l > 1 ? 2 : 1); c++) {
+      const int lp = c ? occ_l - 1 : 0;
+      gp_f32_batch_set_grids(b->f32, lp, 0);
+      for (int w = 0; w < 3; w++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (w & 1), b->stream));
+      GP_CUDA(cudaEventRecord(e0, b->stream));
+      for (int r = 0; r < 10; r++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (r & 1), b->stream));
+      GP_CUDA(cudaEventRecord(e1, b->stream));
+      GP_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      GP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      b->launches += 13 * gp_f32_batch_launches_per_step(b->f32);
+      if (ms < best) {
+        best = ms;
+        best_tx = tx;
+        best_ty = ty;
+        best_lp = lp;
+      }
     }
+    gp_f32_batch_set_grids(b->f32, 0, 0);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -920,11 +933,12 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   b->parity = saved_parity;
   b->have_prev = saved_prev;
   int rc = gp_batch_set_tile(b, best_tx, best_ty);
+  if (rc == GP_OK) rc = gp_batch_set_grids(b, best_lp, 0);
   if (rc != GP_OK) return rc;
   if (cache_path) {
     FILE* f = fopen(cache_path, "a");
     if (f) {
-      fprintf(f, "%s %d %d %.6f\n", key, best_tx, best_ty, best / 10.0f);
+      fprintf(f, "%s %d %d %d %.6f\n", key, best_tx, best_ty, best_lp, best / 10.0f);
       fclose(f);
     }
   }
@@ -938,6 +952,21 @@ extern "C" int gp_batch_set_narrowband(gp_batch* b, int on) {
   GP_CUDA(cudaStreamSynchronize(b->stream));
   gp_f32_batch_set_narrowband(b->f32, on);
   batch_drop_graphs(b);
+  return GP_OK;
+}
+
+extern "C" int gp_batch_set_grids(gp_batch* b, int lean_per_sm, int general_per_sm) {
+  if (!b || lean_per_sm < 0 || general_per_sm < 0) return GP_E_ARG;
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  gp_f32_batch_set_grids(b->f32, lean_per_sm, general_per_sm);
+  batch_drop_graphs(b);
+  return GP_OK;
+}
+
+extern "C" int gp_batch_get_grids(gp_batch* b, int* lean_per_sm, int* general_per_sm, int* occ_lean,
+                                  int* occ_general) {
+  if (!b || !lean_per_sm || !general_per_sm || !occ_lean || !occ_general) return GP_E_ARG;
+  gp_f32_batch_get_grids(b->f32, lean_per_sm, general_per_sm, occ_lean, occ_general);
   return GP_OK;
 }
 

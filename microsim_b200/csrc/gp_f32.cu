@@ -1536,6 +1536,9 @@ struct gp_f32_batch {
   int* dglist = nullptr;       // [total_tiles] tiles of the full kernel
   int* dcnt = nullptr;         // [4] list count, queue head, finished blocks
   int grid_general = 0, grid_lean = 0;
+  int occ_general = 0, occ_lean = 0;         // resident blocks per SM at full occupancy
+  int lean_per_sm = 0, general_per_sm = 0;   // blocks per SM of the persistent grids (0: occupancy)
+  int sms = 0;
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // per-kernel timing (off by default): a ring of event sets, one per step
@@ -1697,6 +1700,29 @@ static cudaError_t encode_boxes(gp_f32_batch* b, int p) {
   return cudaMemcpy(b->dtmap[p], maps.data(), sizeof(CUtensorMap) * b->n, cudaMemcpyHostToDevice);
 }
 
+// Persistent grid sizes: blocks per SM as set (clamped to the occupancy), else the occupancy.
+// Fewer lean blocks than fit leave room on every SM for full-kernel blocks to run beside them.
+static void set_grids(gp_f32_batch* b) {
+  const int l = b->lean_per_sm > 0 && b->lean_per_sm < b->occ_lean ? b->lean_per_sm : b->occ_lean;
+  const int g = b->general_per_sm > 0 && b->general_per_sm < b->occ_general ? b->general_per_sm : b->occ_general;
+  b->grid_lean = b->sms * l;
+  b->grid_general = b->sms * g;
+}
+
+void gp_f32_batch_set_grids(gp_f32_batch* b, int lean_per_sm, int general_per_sm) {
+  b->lean_per_sm = lean_per_sm;
+  b->general_per_sm = general_per_sm;
+  if (b->sms) set_grids(b);
+}
+
+void gp_f32_batch_get_grids(const gp_f32_batch* b, int* lean_per_sm, int* general_per_sm, int* occ_lean,
+                            int* occ_general) {
+  *lean_per_sm = b->sms ? b->grid_lean / b->sms : 0;
+  *general_per_sm = b->sms ? b->grid_general / b->sms : 0;
+  *occ_lean = b->occ_lean;
+  *occ_general = b->occ_general;
+}
+
 // Recompute the tile decomposition for shape (tx, ty) and upload the instance tables.
 cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   KernelSet ks;
@@ -1734,14 +1760,22 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   int dev = 0, sms = 0, occ_g = 0, occ_l = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // one shared-memory carve-out for the three kernels of a step: no L1/shared reconfiguration
+  // between them, and lean and full blocks can share an SM
+  for (const void* f : {(const void*)ks.general, (const void*)ks.lean, (const void*)ks.list}) {
+    e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+  }
   e = cudaFuncSetAttribute(ks.general, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_general);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, ks.general, 256, ks.smem_general);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(ks.lean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_lean);
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, ks.lean, 32 * GP_LEAN_WARPS, ks.smem_lean);
   if (e != cudaSuccess) return e;
-  b->grid_general = sms * (occ_g > 0 ? occ_g : 1);
-  b->grid_lean = sms * (occ_l > 0 ? occ_l : 1);
+  b->sms = sms;
+  b->occ_general = occ_g > 0 ? occ_g : 1;
+  b->occ_lean = occ_l > 0 ? occ_l : 1;
+  set_grids(b);
   return cudaDeviceSynchronize();  // the flag reset above must land before any stream uses them
 }
 

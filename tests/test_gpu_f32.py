@@ -152,7 +152,7 @@ def test_autotune_restores_state_and_caches(tmp_path):
         after = b.download(0)
         assert (tx, ty) in [(16, 32), (8, 32), (32, 32), (16, 64)]
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
-        assert os.path.exists(cache) and len(open(cache).read().split()) == 8
+        assert os.path.exists(cache) and len(open(cache).read().split()) == 9
         assert b.autotune(cache) == (tx, ty)  # read back from the cache
 
 
