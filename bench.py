@@ -295,7 +295,7 @@ def run_ours(args, world, rank, local):
     ctx = mb.Batch(models)
     for i, f in enumerate(fields):
         ctx.upload(i, *f)
-    tile = ctx.autotune(None) if not args.no_autotune else (16, 32)
+    tile = ctx.autotune(args.tune_cache) if not args.no_autotune else (16, 32)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     state_mb = cells * (N + K1) * 4 / 1e6
     with ClockSampler(local) as clk:
@@ -433,6 +433,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--tune-cache", default=None,
+                    help="autotuner cache file: a profiled rerun reads back the plain run's choice")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
