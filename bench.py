@@ -296,6 +296,7 @@ def run_ours(args, world, rank, local):
     for i, f in enumerate(fields):
         ctx.upload(i, *f)
     tile = ctx.autotune(args.tune_cache) if not args.no_autotune else (16, 32)
+    ctx.prepare()  # graph capture is set-up, not part of a step
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     state_mb = cells * (N + K1) * 4 / 1e6
     with ClockSampler(local) as clk:

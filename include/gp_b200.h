@@ -212,6 +212,9 @@ int gp_batch_destroy(gp_batch *b);
 int gp_batch_upload(gp_batch *b, int i, const double *phi, const double *mu);
 int gp_batch_download(gp_batch *b, int i, double *phi, double *mu);
 int gp_batch_step(gp_batch *b, int64_t nsteps);
+/* Capture the step graphs of both buffer parities now, without stepping (the
+ * first gp_batch_step would otherwise capture them). */
+int gp_batch_prepare(gp_batch *b);
 int gp_batch_sync(gp_batch *b);
 int gp_batch_get_stats(gp_batch *b, int i, gp_stats *out);
 /* Tile shape of the fused kernel (tx along x, ty along y): 16x32, 8x32, 32x32, 16x64. */

@@ -111,6 +111,7 @@ _SIGS = {
     "gp_batch_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gp_batch_set_narrowband": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_batch_set_grids": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "gp_batch_prepare": (C.c_int, [C.c_void_p]),
     "gp_batch_get_grids": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
     "gp_batch_lean_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
@@ -389,6 +390,10 @@ class Batch:
 
     def set_narrowband(self, on: bool):
         _check("gp_batch_set_narrowband", lib().gp_batch_set_narrowband(self._h, 1 if on else 0))
+
+    def prepare(self):
+        """Capture the step graphs now (no step is taken)."""
+        _check("gp_batch_prepare", lib().gp_batch_prepare(self._h))
 
     def set_grids(self, lean_per_sm: int = 0, general_per_sm: int = 0):
         """Blocks per SM of the lean and full persistent grids (0: as many as fit)."""

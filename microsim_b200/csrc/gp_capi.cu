@@ -807,6 +807,19 @@ extern "C" int gp_batch_step(gp_batch* b, int64_t nsteps) {
   return GP_OK;
 }
 
+// Capture and instantiate the step graphs of both buffer parities now (no step
+// is taken), so that the first gp_batch_step calls do not pay for them.
+extern "C" int gp_batch_prepare(gp_batch* b) {
+  if (!b) return GP_E_ARG;
+  if (gp_f32_batch_timing(b->f32)) return GP_OK;  // timed steps launch directly
+  for (int p = 0; p < 2; p++)
+    if (!b->graph[p]) {
+      int rc = batch_capture(b, p);
+      if (rc != GP_OK) return rc;
+    }
+  return GP_OK;
+}
+
 extern "C" int gp_batch_sync(gp_batch* b) {
   if (!b) return GP_E_ARG;
   GP_CUDA(cudaStreamSynchronize(b->stream));
