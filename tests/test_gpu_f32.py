@@ -226,6 +226,31 @@ def test_narrow_band_is_bit_identical_to_the_full_kernel():
     assert np.array_equal(a[0], c[0]) and np.array_equal(a[1], c[1])
 
 
+def test_grid_split_and_prepared_graphs_are_bit_identical():
+    """The persistent grids' blocks per SM (lean and full kernels, run
+    concurrently) and graph capture ahead of time change no bits; prepare()
+    takes no step."""
+    m, phi, mu = mb.load_case(BINARY["aniso_corner"])
+    res = []
+    for grids, prep in [((0, 0), False), ((1, 1), True), ((2, 3), True), ((0, 2), False)]:
+        with mb.Batch([m, m]) as b:
+            b.set_grids(*grids)
+            lp, gp, occ_l, occ_g = b.grids()
+            assert lp == (grids[0] if 0 < grids[0] < occ_l else occ_l)
+            assert gp == (grids[1] if 0 < grids[1] < occ_g else occ_g)
+            b.upload(0, phi, mu)
+            b.upload(1, phi, mu)
+            if prep:
+                before = b.download(0)
+                b.prepare()
+                after = b.download(0)
+                assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+            b.step(37)
+            res.append(b.download(1))
+    for p, u in res[1:]:
+        assert np.array_equal(p, res[0][0]) and np.array_equal(u, res[0][1])
+
+
 def test_moving_frame_within_tolerance_of_reference():
     """Shift = 1 in the FP32 form: same interface rows and offsets as the
     reference, fields within the 2-phase tolerances (the first step after a
