@@ -292,6 +292,23 @@ enum { PF_CORE = 0, PF_XLO = 4, PF_XHI = 8, PF_YLO = 12, PF_YHI = 16 };
 __host__ __device__ __forceinline__ int pf(uint32_t w, int f) { return (int)((w >> f) & 15u); }
 __host__ __device__ __forceinline__ uint32_t pf_all(int c) { return (uint32_t)c * 0x11111u; }
 
+// Static facts of tile t used by lean_phase, one word: tiles along y (the
+// index stride of the x-neighbours), which of the four neighbours exist, and
+// whether the tile is never lean (its two-cell ring leaves the grid where it
+// is not a trusted mirror: a periodic wrap, or fewer than 3 cells on that axis).
+enum : uint32_t { TG_NY = 0xFFFFFFu, TG_XM = 1u << 24, TG_XP = 1u << 25, TG_YM = 1u << 26, TG_YP = 1u << 27,
+                  TG_REJECT = 1u << 28 };
+
+inline uint32_t tile_geo(const Inst& I, int t, int TX, int TY) {
+  const int ny = I.tiles_y, lt = t - I.tile_begin, tx = lt / ny, ty = lt % ny;
+  const int ex = I.mx - tx * TX < TX ? I.mx - tx * TX : TX, ey = I.my - ty * TY < TY ? I.my - ty * TY : TY;
+  const bool xm = tx > 0, xp = tx + 1 < I.tiles_x, ym = ty > 0, yp = ty + 1 < ny;
+  const bool reject = ((!xm || !xp) && !(I.bc.phi_x == GP_BC_NEUMANN && ex >= 3)) ||
+                      ((!ym || !yp) && !(I.bc.phi_y == GP_BC_NEUMANN && ey >= 3));
+  return (uint32_t)ny | (xm ? TG_XM : 0u) | (xp ? TG_XP : 0u) | (ym ? TG_YM : 0u) | (yp ? TG_YP : 0u) |
+         (reject ? TG_REJECT : 0u);
+}
+
 // Phase b >= 0 when tile t may take the lean update: in the input, the tile
 // and the two-cell ring the full update reads around it (tile +- 2, the phi
 // region it stages) hold the one-hot field of phase b, known from the purity
@@ -299,37 +316,28 @@ __host__ __device__ __forceinline__ uint32_t pf_all(int c) { return (uint32_t)c 
 // it is the Neumann mirror of the tile's own cells (rows 1, 2 and M-2, M-3:
 // the tile needs 3 cells on that axis); a periodic wrap is not trusted.
 // The full update of such a tile is its pure-phase path, so the lean update
-// gives the same bits.  -1 otherwise.
-__host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ F, const Inst& I, int t, int TX,
-                                                   int TY) {
-  const int c = pf(F[t], PF_CORE);
-  if (!c) return -1;
-  const int ny = I.tiles_y, lt = t - I.tile_begin, tx = lt / ny, ty = lt % ny;
-  const int ex = I.mx - tx * TX < TX ? I.mx - tx * TX : TX, ey = I.my - ty * TY < TY ? I.my - ty * TY : TY;
-  const bool xm = tx > 0, xp = tx + 1 < I.tiles_x, ym = ty > 0, yp = ty + 1 < ny;
-  if ((!xm || !xp) && !(I.bc.phi_x == GP_BC_NEUMANN && ex >= 3)) return -1;
-  if ((!ym || !yp) && !(I.bc.phi_y == GP_BC_NEUMANN && ey >= 3)) return -1;
-  if (xm && pf(F[t - ny], PF_XHI) != c) return -1;
-  if (xp && pf(F[t + ny], PF_XLO) != c) return -1;
-  if (ym && pf(F[t - 1], PF_YHI) != c) return -1;
-  if (yp && pf(F[t + 1], PF_YLO) != c) return -1;
-  if (xm && ym) {
-    const uint32_t v = F[t - ny - 1];
-    if (pf(v, PF_XHI) != c && pf(v, PF_YHI) != c) return -1;
-  }
-  if (xm && yp) {
-    const uint32_t v = F[t - ny + 1];
-    if (pf(v, PF_XHI) != c && pf(v, PF_YLO) != c) return -1;
-  }
-  if (xp && ym) {
-    const uint32_t v = F[t + ny - 1];
-    if (pf(v, PF_XLO) != c && pf(v, PF_YHI) != c) return -1;
-  }
-  if (xp && yp) {
-    const uint32_t v = F[t + ny + 1];
-    if (pf(v, PF_XLO) != c && pf(v, PF_YLO) != c) return -1;
-  }
-  return c - 1;
+// gives the same bits.  -1 otherwise.  The nine words are loaded at once (a
+// missing neighbour reads the tile's own word, unused).
+__host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ F, uint32_t geo, int t) {
+  if (geo & TG_REJECT) return -1;
+  const int ny = (int)(geo & TG_NY);
+  const bool xm = geo & TG_XM, xp = geo & TG_XP, ym = geo & TG_YM, yp = geo & TG_YP;
+  const uint32_t w = F[t];
+  const uint32_t wxm = F[xm ? t - ny : t], wxp = F[xp ? t + ny : t], wym = F[ym ? t - 1 : t],
+                 wyp = F[yp ? t + 1 : t];
+  const uint32_t wmm = F[xm && ym ? t - ny - 1 : t], wmp = F[xm && yp ? t - ny + 1 : t],
+                 wpm = F[xp && ym ? t + ny - 1 : t], wpp = F[xp && yp ? t + ny + 1 : t];
+  const int c = pf(w, PF_CORE);
+  bool ok = c != 0;
+  ok &= !xm || pf(wxm, PF_XHI) == c;
+  ok &= !xp || pf(wxp, PF_XLO) == c;
+  ok &= !ym || pf(wym, PF_YHI) == c;
+  ok &= !yp || pf(wyp, PF_YLO) == c;
+  ok &= !(xm && ym) || pf(wmm, PF_XHI) == c || pf(wmm, PF_YHI) == c;
+  ok &= !(xm && yp) || pf(wmp, PF_XHI) == c || pf(wmp, PF_YLO) == c;
+  ok &= !(xp && ym) || pf(wpm, PF_XLO) == c || pf(wpm, PF_YHI) == c;
+  ok &= !(xp && yp) || pf(wpp, PF_XLO) == c || pf(wpp, PF_YLO) == c;
+  return ok ? c - 1 : -1;
 }
 
 // Full update of the tiles.  With glist == nullptr block k takes tile k (grid
@@ -1288,7 +1296,7 @@ __device__ __forceinline__ void lean_compute(const Inst& I, const LeanConst& C, 
 template <int N, int K1, int TX, int TY>
 __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
     k_lean32(const Inst* __restrict__ insts, const LeanConst* __restrict__ lconst,
-             const CUtensorMap* __restrict__ tmaps, const int* __restrict__ tile_inst,
+             const CUtensorMap* __restrict__ tmaps, const int4* __restrict__ tile_desc,
              const uint32_t* __restrict__ flags_in, uint32_t* __restrict__ flags_out, int total, int reverse,
              int* __restrict__ err) {
   using S = Lean<N, K1, TX, TY>;
@@ -1319,14 +1327,12 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
       if (reverse) tc = total - 1 - tc;
       mine = -1;
       if (tc >= 0 && tc < total) {
-        const int inst = tile_inst[tc];
-        const Inst& I = insts[inst];
-        const int bc = lean_phase(flags_in, I, (int)tc, TX, TY);
+        const int4 d = tile_desc[tc];  // {instance, x0, y0, tile_geo}
+        const int bc = lean_phase(flags_in, (uint32_t)d.w, (int)tc);
         if (bc >= 0) {
-          const int lt = (int)tc - I.tile_begin, ny = I.tiles_y;
-          mine = inst * 8 + bc;
-          mx0 = (lt / ny) * TX;
-          my0 = (lt % ny) * TY;
+          mine = d.x * 8 + bc;
+          mx0 = d.y;
+          my0 = d.z;
         }
       }
       todo = __ballot_sync(0xffffffffu, mine >= 0);
@@ -1392,12 +1398,11 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
 // The tiles of one step that lean_phase rejects, appended to glist (count in
 // cnt[0]) for the full kernel.
 template <int TX, int TY>
-__global__ void __launch_bounds__(256) k_general_list(const Inst* __restrict__ insts,
-                                                      const int* __restrict__ tile_inst,
+__global__ void __launch_bounds__(256) k_general_list(const int4* __restrict__ tile_desc,
                                                       const uint32_t* __restrict__ flags_in, int total,
                                                       int* __restrict__ glist, int* __restrict__ cnt) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool gen = t < total && lean_phase(flags_in, insts[tile_inst[t]], t, TX, TY) < 0;
+  const bool gen = t < total && lean_phase(flags_in, (uint32_t)tile_desc[t].w, t) < 0;
   const unsigned bal = __ballot_sync(0xffffffffu, gen);
   const int lane = threadIdx.x & 31;
   int base = 0;
@@ -1467,9 +1472,9 @@ using namespace gp32;
 // Kernels of one (N, K1, anisotropy, tile shape).
 struct KernelSet {
   void (*general)(const Inst*, const Model*, const int*, const int*, int*, uint32_t*);
-  void (*lean)(const Inst*, const LeanConst*, const CUtensorMap*, const int*, const uint32_t*, uint32_t*, int, int,
+  void (*lean)(const Inst*, const LeanConst*, const CUtensorMap*, const int4*, const uint32_t*, uint32_t*, int, int,
                int*);
-  void (*list)(const Inst*, const int*, const uint32_t*, int, int*, int*);
+  void (*list)(const int4*, const uint32_t*, int, int*, int*);
   size_t smem_general, smem_lean;
 };
 
@@ -1533,6 +1538,8 @@ struct gp_f32_batch {
   KernelSet ks;
   uint32_t* dflags = nullptr;  // [2][total_tiles] purity words of the state in buffer p
   int* dtile_inst = nullptr;   // [total_tiles] instance of each tile
+  int4* dtile_desc = nullptr;  // [total_tiles] {instance, x0, y0, tile_geo}
+  std::vector<int4> htile_desc;
   int* dglist = nullptr;       // [total_tiles] tiles of the full kernel
   int* dcnt = nullptr;         // [4] list count, queue head, finished blocks
   int grid_general = 0, grid_lean = 0;
@@ -1554,9 +1561,11 @@ void gp_f32_batch_destroy(gp_f32_batch* b);
 static void free_tiles(gp_f32_batch* b) {
   cudaFree(b->dflags);
   cudaFree(b->dtile_inst);
+  cudaFree(b->dtile_desc);
   cudaFree(b->dglist);
   b->dflags = nullptr;
   b->dtile_inst = nullptr;
+  b->dtile_desc = nullptr;
   b->dglist = nullptr;
 }
 
@@ -1732,6 +1741,7 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   b->ks = ks;
   int t = 0;
   std::vector<int> tile_inst;
+  b->htile_desc.clear();
   for (int i = 0; i < b->n; i++) {
     const int txs = (int)((b->gm[i].mesh_x + tx - 1) / tx), tys = (int)((b->gm[i].mesh_y + ty - 1) / ty);
     for (int p = 0; p < 2; p++) {
@@ -1739,6 +1749,8 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
       b->hinst[p][i].tiles_y = tys;
       b->hinst[p][i].tile_begin = t;
     }
+    for (int k = 0; k < txs * tys; k++)
+      b->htile_desc.push_back(make_int4(i, (k / tys) * tx, (k % tys) * ty, (int)tile_geo(b->hinst[0][i], t + k, tx, ty)));
     t += txs * tys;
     tile_inst.insert(tile_inst.end(), (size_t)txs * tys, i);
   }
@@ -1753,6 +1765,9 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   if (e == cudaSuccess) e = cudaMemset(b->dflags, 0, 2 * sizeof(uint32_t) * (size_t)t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dtile_inst, sizeof(int) * t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dglist, sizeof(int) * t);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dtile_desc, sizeof(int4) * t);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->dtile_desc, b->htile_desc.data(), sizeof(int4) * t, cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(b->dtile_inst, tile_inst.data(), sizeof(int) * t, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return e;
@@ -1862,12 +1877,12 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
     if ((e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess) return e;
   }
   if (E && ((e = cudaEventRecord(E[0], ls)) != cudaSuccess)) return e;
-  k.lean<<<b->grid_lean, 32 * GP_LEAN_WARPS, k.smem_lean, ls>>>(b->dinst[p], b->dlconst, b->dtmap[p], b->dtile_inst, flags_in,
+  k.lean<<<b->grid_lean, 32 * GP_LEAN_WARPS, k.smem_lean, ls>>>(b->dinst[p], b->dlconst, b->dtmap[p], b->dtile_desc, flags_in,
                                                  flags_out, b->total_tiles, p, b->derr);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E && ((e = cudaEventRecord(E[1], ls)) != cudaSuccess)) return e;
   if (E && ((e = cudaEventRecord(E[2], s)) != cudaSuccess)) return e;
-  k.list<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dinst[p], b->dtile_inst, flags_in, b->total_tiles, b->dglist,
+  k.list<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dtile_desc, flags_in, b->total_tiles, b->dglist,
                                                       b->dcnt);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
@@ -1894,7 +1909,7 @@ cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s,
   for (int i = 0; i < b->n && b->narrowband; i++) {
     const Inst& I = b->hinst[parity & 1][i];
     for (int t = I.tile_begin; t < I.tile_begin + I.tiles_x * I.tiles_y; t++)
-      if (lean_phase(F.data(), I, t, b->tx, b->ty) >= 0) {
+      if (lean_phase(F.data(), (uint32_t)b->htile_desc[t].w, t) >= 0) {
         const int lt = t - I.tile_begin, x0 = (lt / I.tiles_y) * b->tx, y0 = (lt % I.tiles_y) * b->ty;
         n++;
         c += (int64_t)(I.mx - x0 < b->tx ? I.mx - x0 : b->tx) * (I.my - y0 < b->ty ? I.my - y0 : b->ty);
