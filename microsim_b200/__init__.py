@@ -138,6 +138,15 @@ _SIGS = {
 }
 
 
+def _out(a, shape):
+    """A C-contiguous float64 output array of `shape`: `a` itself when given."""
+    if a is None:
+        return np.empty(shape)
+    if a.dtype != np.float64 or a.shape != tuple(shape) or not a.flags.c_contiguous or not a.flags.writeable:
+        raise ValueError(f"output array must be writeable C-contiguous float64 of shape {tuple(shape)}")
+    return a
+
+
 def lib():
     """Load libgp_b200.so (raises if it has not been built)."""
     global _lib
@@ -252,10 +261,11 @@ class Context:
         mu = np.ascontiguousarray(mu, dtype=np.float64)
         _check("gp_upload", lib().gp_upload(self._h, _ptr(phi), _ptr(mu)))
 
-    def download(self):
+    def download(self, phi: np.ndarray | None = None, mu: np.ndarray | None = None):
+        """The state as float64 arrays (into phi / mu when given)."""
         m = self.model
-        phi = np.empty((m.N, m.mesh_x, m.mesh_y))
-        mu = np.empty((m.K1, m.mesh_x, m.mesh_y))
+        phi = _out(phi, (m.N, m.mesh_x, m.mesh_y))
+        mu = _out(mu, (m.K1, m.mesh_x, m.mesh_y))
         _check("gp_download", lib().gp_download(self._h, _ptr(phi), _ptr(mu)))
         return phi, mu
 
@@ -365,10 +375,12 @@ class Batch:
         mu = np.ascontiguousarray(mu, dtype=np.float64)
         _check("gp_batch_upload", lib().gp_batch_upload(self._h, i, _ptr(phi), _ptr(mu)))
 
-    def download(self, i: int):
+    def download(self, i: int, phi: np.ndarray | None = None, mu: np.ndarray | None = None):
+        """Instance i's state as float64 arrays (into phi / mu when given: C-contiguous
+        float64 of the instance's shapes, e.g. views of pinned host memory)."""
         m = self.models[i]
-        phi = np.empty((m.N, m.mesh_x, m.mesh_y))
-        mu = np.empty((m.K1, m.mesh_x, m.mesh_y))
+        phi = _out(phi, (m.N, m.mesh_x, m.mesh_y))
+        mu = _out(mu, (m.K1, m.mesh_x, m.mesh_y))
         _check("gp_batch_download", lib().gp_batch_download(self._h, i, _ptr(phi), _ptr(mu)))
         return phi, mu
 

@@ -53,6 +53,23 @@ void gp_f32_tile_shape(int i, int* tx, int* ty);
     }                                                                                      \
   } while (0)
 
+// A device staging buffer of at least `need` bytes, kept for later copies (a
+// fresh allocation per copy costs more than the copy for small instances).
+// Copies on `s` that used the old buffer are ordered before its release.
+static cudaError_t ensure_stage(double** buf, size_t* have, size_t need, cudaStream_t s) {
+  if (*have >= need) return cudaSuccess;
+  if (*buf) {
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    cudaFree(*buf);
+    *buf = nullptr;
+    *have = 0;
+  }
+  cudaError_t e = cudaMalloc((void**)buf, need);
+  if (e == cudaSuccess) *have = need;
+  return e;
+}
+
 // The FP32 form's lean kernel gave up on a staged box (bounded wait expired).
 static int lean_error() {
   gp_set_error("FP32 lean kernel: a staged mu box did not arrive within one second; results are invalid");
@@ -78,6 +95,8 @@ struct gp_ctx {
   int cur;         // which buffer holds the current state
   int have_prev;   // buffer 1-cur holds the previous step's state
   double* partials;  // statistics: per-block partial results
+  double* stage = nullptr;  // FP32 form: device staging of FP64 host fields (kept between copies)
+  size_t stage_bytes = 0;
   double* reduced;   // statistics: final values (device)
   int red_blocks;
   int64_t launches;
@@ -184,6 +203,7 @@ extern "C" int gp_destroy(gp_ctx* c) {
   if (c->gov) cudaFree(c->gov);
   if (c->f32) gp_f32_batch_destroy(c->f32);
   if (c->partials) cudaFree(c->partials);
+  if (c->stage) cudaFree(c->stage);
   if (c->reduced) cudaFree(c->reduced);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -229,9 +249,9 @@ static int copy_planes(gp_ctx* c, const double* host, void* dev, int nplanes, bo
     return GP_OK;
   }
   // FP32: stage doubles on the device, convert with a kernel
-  double* stage = nullptr;
   const size_t bytes = (size_t)nplanes * mx * my * sizeof(double);
-  GP_CUDA(cudaMallocAsync((void**)&stage, bytes, c->stream));
+  GP_CUDA(ensure_stage(&c->stage, &c->stage_bytes, bytes, c->stream));
+  double* const stage = c->stage;
   if (up) {
     GP_CUDA(cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, c->stream));
     k_pack<float><<<592, 256, 0, c->stream>>>(stage, (float*)dev, (int)mx, (int)my, c->pitch, c->plane, nplanes);
@@ -242,7 +262,6 @@ static int copy_planes(gp_ctx* c, const double* host, void* dev, int nplanes, bo
   }
   c->launches++;
   GP_CUDA(cudaGetLastError());
-  GP_CUDA(cudaFreeAsync(stage, c->stream));
   return GP_OK;
 }
 
@@ -645,6 +664,8 @@ struct gp_batch {
   int graph_steps = 16;
   double* partials = nullptr;
   double* reduced = nullptr;
+  double* stage = nullptr;  // device staging of FP64 host fields (kept between copies)
+  size_t stage_bytes = 0;
   int red_blocks = 296;
   int64_t launches = 0;
   int tx = 16, ty = 32;
@@ -665,6 +686,7 @@ extern "C" int gp_batch_destroy(gp_batch* b) {
   if (b->f32) gp_f32_batch_destroy(b->f32);
   if (b->pool) cudaFree(b->pool);
   if (b->partials) cudaFree(b->partials);
+  if (b->stage) cudaFree(b->stage);
   if (b->reduced) cudaFree(b->reduced);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -730,9 +752,9 @@ static int batch_copy(gp_batch* b, int i, const double* host, int nplanes, bool 
   const gp_model& m = b->models[i];
   const int64_t mx = m.mesh_x, my = m.mesh_y;
   float* dev = b->pool + (is_phi ? b->off_phi[b->parity][i] : b->off_mu[b->parity][i]);
-  double* stage = nullptr;
   const size_t bytes = (size_t)nplanes * mx * my * sizeof(double);
-  GP_CUDA(cudaMallocAsync((void**)&stage, bytes, b->stream));
+  GP_CUDA(ensure_stage(&b->stage, &b->stage_bytes, bytes, b->stream));
+  double* const stage = b->stage;
   if (up) {
     GP_CUDA(cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, b->stream));
     k_pack<float><<<592, 256, 0, b->stream>>>(stage, dev, (int)mx, (int)my, b->pitch[i], b->plane[i], nplanes);
@@ -742,7 +764,6 @@ static int batch_copy(gp_batch* b, int i, const double* host, int nplanes, bool 
   }
   b->launches++;
   GP_CUDA(cudaGetLastError());
-  GP_CUDA(cudaFreeAsync(stage, b->stream));
   return GP_OK;
 }
 

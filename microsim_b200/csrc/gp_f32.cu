@@ -346,8 +346,11 @@ __host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ 
 // cnt[1]); the last block to finish resets the counters (cnt[2] counts
 // finished blocks) for the next step.
 // Every tile writes the purity word of its output.
+#ifndef GP_STEP_BLOCKS_BINARY
+#define GP_STEP_BLOCKS_BINARY 4  // resident full-kernel blocks per SM for binary alloys
+#endif
 template <int N, int K1, bool ANISO, int TX, int TY>
-__global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? 4 : (K1 >= 3 ? 1 : 2))
+__global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? GP_STEP_BLOCKS_BINARY : (K1 >= 3 ? 1 : 2))
     k_step32(const Inst* __restrict__ insts, const Model* __restrict__ models, const int* __restrict__ tile_inst,
              const int* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out) {
   using T = Tile<N, K1, ANISO, TX, TY>;
