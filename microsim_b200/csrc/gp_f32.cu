@@ -352,7 +352,7 @@ __host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ 
 template <int N, int K1, bool ANISO, int TX, int TY>
 __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? GP_STEP_BLOCKS_BINARY : (K1 >= 3 ? 1 : 2))
     k_step32(const Inst* __restrict__ insts, const Model* __restrict__ models, const int* __restrict__ tile_inst,
-             const int* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out) {
+             const int2* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out) {
   using T = Tile<N, K1, ANISO, TX, TY>;
   constexpr int X2 = T::X2, Y2 = T::Y2, X1 = T::X1, Y1 = T::Y1, W = T::W, Q = T::Q;
   constexpr int L = N - 1;
@@ -370,16 +370,17 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? GP_STEP_BLOCKS_BINA
   for (int iter = 0;; iter++) {
   __syncthreads();  // the previous tile's shared state is no longer read
   if (threadIdx.x == 0) {
-    int t = -1;
+    int2 e = make_int2(-1, 0);
     if (glist) {  // block k starts with entry k, then takes entries grid, grid + 1, ... from the queue
+      // (claimed when the block is free: the blocks whose first tiles finish early take the rest)
       const int i = iter == 0 ? (int)blockIdx.x : (int)gridDim.x + atomicAdd(&cnt[1], 1);
-      if (i < cnt[0]) t = glist[i];
+      if (i < cnt[0]) e = glist[i];
     } else if (iter == 0) {
-      t = blockIdx.x;
+      e = make_int2((int)blockIdx.x, tile_inst[blockIdx.x]);
     }
-    s_tile = t;
-    if (t >= 0) {
-      sInst = insts[tile_inst[t]];
+    s_tile = e.x;
+    if (e.x >= 0) {
+      sInst = insts[e.y];
       s_reload = sInst.model != s_model;
       s_model = sInst.model;
       s_bad = 0u;
@@ -388,10 +389,10 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? GP_STEP_BLOCKS_BINA
   __syncthreads();
   const int tile = s_tile;
   if (tile < 0) break;
-  if (s_reload) {  // the instance's model constants into shared memory
+  if (s_reload) {  // the instance's model constants into shared memory, loaded with the staged fields
     const float4* src = reinterpret_cast<const float4*>(models + sInst.model);
     float4* dst = reinterpret_cast<float4*>(&sModel);
-    for (int e = threadIdx.x; e < (int)(sizeof(Model) / 16); e += nt) dst[e] = __ldg(src + e);
+    for (int e = threadIdx.x; e < (int)(sizeof(Model) / 16); e += nt) cp_async16(dst + e, src + e);
   }
   const Inst& I = sInst;
   const Model& m = sModel;
@@ -1403,15 +1404,17 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
 template <int TX, int TY>
 __global__ void __launch_bounds__(256) k_general_list(const int4* __restrict__ tile_desc,
                                                       const uint32_t* __restrict__ flags_in, int total,
-                                                      int* __restrict__ glist, int* __restrict__ cnt) {
+                                                      int2* __restrict__ glist, int* __restrict__ cnt) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool gen = t < total && lean_phase(flags_in, (uint32_t)tile_desc[t].w, t) < 0;
+  int4 d = make_int4(0, 0, 0, 0);
+  if (t < total) d = tile_desc[t];
+  const bool gen = t < total && lean_phase(flags_in, (uint32_t)d.w, t) < 0;
   const unsigned bal = __ballot_sync(0xffffffffu, gen);
   const int lane = threadIdx.x & 31;
   int base = 0;
   if (lane == 0 && bal) base = atomicAdd(&cnt[0], __popc(bal));
   base = __shfl_sync(0xffffffffu, base, 0);
-  if (gen) glist[base + __popc(bal & ((1u << lane) - 1u))] = t;
+  if (gen) glist[base + __popc(bal & ((1u << lane) - 1u))] = make_int2(t, d.x);
 }
 
 // ---------------------------------------------------------------- host side
@@ -1474,10 +1477,10 @@ using namespace gp32;
 
 // Kernels of one (N, K1, anisotropy, tile shape).
 struct KernelSet {
-  void (*general)(const Inst*, const Model*, const int*, const int*, int*, uint32_t*);
+  void (*general)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*);
   void (*lean)(const Inst*, const LeanConst*, const CUtensorMap*, const int4*, const uint32_t*, uint32_t*, int, int,
                int*);
-  void (*list)(const int4*, const uint32_t*, int, int*, int*);
+  void (*list)(const int4*, const uint32_t*, int, int2*, int*);
   size_t smem_general, smem_lean;
 };
 
@@ -1543,7 +1546,7 @@ struct gp_f32_batch {
   int* dtile_inst = nullptr;   // [total_tiles] instance of each tile
   int4* dtile_desc = nullptr;  // [total_tiles] {instance, x0, y0, tile_geo}
   std::vector<int4> htile_desc;
-  int* dglist = nullptr;       // [total_tiles] tiles of the full kernel
+  int2* dglist = nullptr;      // [total_tiles] {tile, instance} of the full kernel's tiles
   int* dcnt = nullptr;         // [4] list count, queue head, finished blocks
   int grid_general = 0, grid_lean = 0;
   int occ_general = 0, occ_lean = 0;         // resident blocks per SM at full occupancy
@@ -1767,7 +1770,7 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   cudaError_t e = cudaMalloc(&b->dflags, 2 * sizeof(uint32_t) * (size_t)t);
   if (e == cudaSuccess) e = cudaMemset(b->dflags, 0, 2 * sizeof(uint32_t) * (size_t)t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dtile_inst, sizeof(int) * t);
-  if (e == cudaSuccess) e = cudaMalloc(&b->dglist, sizeof(int) * t);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dglist, sizeof(int2) * t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dtile_desc, sizeof(int4) * t);
   if (e == cudaSuccess)
     e = cudaMemcpy(b->dtile_desc, b->htile_desc.data(), sizeof(int4) * t, cudaMemcpyHostToDevice);
