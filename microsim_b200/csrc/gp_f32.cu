@@ -341,8 +341,11 @@ __host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ 
 }
 
 // Full update of the tiles.  With glist == nullptr block k takes tile k (grid
-// = all tiles).  Otherwise the blocks are persistent and take the cnt[0]
-// tiles of glist: block k entry k first, then entries grid + (queue head
+// = all tiles).  Otherwise the blocks are persistent and take the entries of
+// glist: first the cnt[0] tiles with interface cells of their own (glist[0..]),
+// then the cnt[3] tiles that are pure inside and only border an interface
+// (stored from glist[total - 1] down), cheaper, so that they fill the second
+// round; block k takes entry k first, then entries grid + (queue head
 // cnt[1]); the last block to finish resets the counters (cnt[2] counts
 // finished blocks) for the next step.
 // Every tile writes the purity word of its output.
@@ -352,7 +355,7 @@ __host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ 
 template <int N, int K1, bool ANISO, int TX, int TY>
 __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? GP_STEP_BLOCKS_BINARY : (K1 >= 3 ? 1 : 2))
     k_step32(const Inst* __restrict__ insts, const Model* __restrict__ models, const int* __restrict__ tile_inst,
-             const int2* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out) {
+             const int2* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out, int total) {
   using T = Tile<N, K1, ANISO, TX, TY>;
   constexpr int X2 = T::X2, Y2 = T::Y2, X1 = T::X1, Y1 = T::Y1, W = T::W, Q = T::Q;
   constexpr int L = N - 1;
@@ -374,7 +377,9 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? GP_STEP_BLOCKS_BINA
     if (glist) {  // block k starts with entry k, then takes entries grid, grid + 1, ... from the queue
       // (claimed when the block is free: the blocks whose first tiles finish early take the rest)
       const int i = iter == 0 ? (int)blockIdx.x : (int)gridDim.x + atomicAdd(&cnt[1], 1);
-      if (i < cnt[0]) e = glist[i];
+      const int n0 = cnt[0];
+      if (i < n0) e = glist[i];
+      else if (i < n0 + cnt[3]) e = glist[total - 1 - (i - n0)];
     } else if (iter == 0) {
       e = make_int2((int)blockIdx.x, tile_inst[blockIdx.x]);
     }
@@ -1023,6 +1028,7 @@ __global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? GP_STEP_BLOCKS_BINA
       cnt[0] = 0;
       cnt[1] = 0;
       cnt[2] = 0;
+      cnt[3] = 0;
     }
   }
 }
@@ -1399,8 +1405,10 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
   }
 }
 
-// The tiles of one step that lean_phase rejects, appended to glist (count in
-// cnt[0]) for the full kernel.
+// The tiles of one step that lean_phase rejects, listed for the full kernel:
+// tiles whose own cells are not all one pure phase from glist[0] up (count in
+// cnt[0]), the others (an interface only in their ring) from glist[total - 1]
+// down (count in cnt[3]).
 template <int TX, int TY>
 __global__ void __launch_bounds__(256) k_general_list(const int4* __restrict__ tile_desc,
                                                       const uint32_t* __restrict__ flags_in, int total,
@@ -1409,12 +1417,17 @@ __global__ void __launch_bounds__(256) k_general_list(const int4* __restrict__ t
   int4 d = make_int4(0, 0, 0, 0);
   if (t < total) d = tile_desc[t];
   const bool gen = t < total && lean_phase(flags_in, (uint32_t)d.w, t) < 0;
-  const unsigned bal = __ballot_sync(0xffffffffu, gen);
+  const bool ring = gen && pf(flags_in[t], PF_CORE) != 0;  // pure inside
+  const unsigned bal = __ballot_sync(0xffffffffu, gen && !ring), balr = __ballot_sync(0xffffffffu, ring);
   const int lane = threadIdx.x & 31;
-  int base = 0;
+  int base = 0, baser = 0;
   if (lane == 0 && bal) base = atomicAdd(&cnt[0], __popc(bal));
+  if (lane == 0 && balr) baser = atomicAdd(&cnt[3], __popc(balr));
   base = __shfl_sync(0xffffffffu, base, 0);
-  if (gen) glist[base + __popc(bal & ((1u << lane) - 1u))] = make_int2(t, d.x);
+  baser = __shfl_sync(0xffffffffu, baser, 0);
+  const unsigned below = (1u << lane) - 1u;
+  if (gen && !ring) glist[base + __popc(bal & below)] = make_int2(t, d.x);
+  if (ring) glist[total - 1 - (baser + __popc(balr & below))] = make_int2(t, d.x);
 }
 
 // ---------------------------------------------------------------- host side
@@ -1477,7 +1490,7 @@ using namespace gp32;
 
 // Kernels of one (N, K1, anisotropy, tile shape).
 struct KernelSet {
-  void (*general)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*);
+  void (*general)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*, int);
   void (*lean)(const Inst*, const LeanConst*, const CUtensorMap*, const int4*, const uint32_t*, uint32_t*, int, int,
                int*);
   void (*list)(const int4*, const uint32_t*, int, int2*, int*);
@@ -1867,7 +1880,7 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   if (!b->narrowband) {
     if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
     k.general<<<b->total_tiles, 256, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr,
-                                                          flags_out);
+                                                          flags_out, b->total_tiles);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (E) {
       if ((e = cudaEventRecord(E[4], s)) != cudaSuccess) return e;
@@ -1893,7 +1906,7 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
   k.general<<<b->grid_general, 256, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, b->dglist, b->dcnt,
-                                                         flags_out);
+                                                         flags_out, b->total_tiles);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E) return cudaEventRecord(E[4], s);
   if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess) return e;
