@@ -233,6 +233,11 @@ int gp_batch_lean_tiles(gp_batch *b, int64_t *lean, int64_t *total, int64_t *lea
  * occupancy leaves every SM room for full-kernel blocks beside it.
  * gp_batch_get_grids also reports the occupancies. */
 int gp_batch_set_grids(gp_batch *b, int lean_per_sm, int general_per_sm);
+/* Failure-detection test (no counterpart in the reference): the next step's
+ * lean kernel leaves one staged tile box unissued; its wait gives up after one
+ * second, the kernel returns, and the next gp_batch_get_stats reports GP_E_CUDA.
+ * The batch's results are invalid from then on. */
+int gp_batch_test_lose_box(gp_batch *b);
 int gp_batch_get_grids(gp_batch *b, int *lean_per_sm, int *general_per_sm, int *occ_lean, int *occ_general);
 /* Per-kernel timing (diagnostics): while on, steps launch directly (no graph
  * replay), their kernels one after the other on the batch's stream, and record

@@ -112,6 +112,7 @@ _SIGS = {
     "gp_batch_set_narrowband": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_batch_set_grids": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gp_batch_prepare": (C.c_int, [C.c_void_p]),
+    "gp_batch_test_lose_box": (C.c_int, [C.c_void_p]),
     "gp_batch_get_grids": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
     "gp_batch_lean_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),

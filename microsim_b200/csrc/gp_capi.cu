@@ -30,6 +30,7 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty);
 int gp_f32_batch_tiles(const gp_f32_batch* b);
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s);
 const int* gp_f32_batch_error_word(const gp_f32_batch* b);
+void gp_f32_batch_test_lose_box(gp_f32_batch* b);
 void gp_f32_batch_set_grids(gp_f32_batch* b, int lean_per_sm, int general_per_sm);
 void gp_f32_batch_get_grids(const gp_f32_batch* b, int* lean_per_sm, int* general_per_sm, int* occ_lean,
                             int* occ_general);
@@ -987,6 +988,12 @@ extern "C" int gp_batch_set_narrowband(gp_batch* b, int on) {
   GP_CUDA(cudaStreamSynchronize(b->stream));
   gp_f32_batch_set_narrowband(b->f32, on);
   batch_drop_graphs(b);
+  return GP_OK;
+}
+
+extern "C" int gp_batch_test_lose_box(gp_batch* b) {
+  if (!b) return GP_E_ARG;
+  gp_f32_batch_test_lose_box(b->f32);
   return GP_OK;
 }
 

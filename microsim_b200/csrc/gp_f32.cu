@@ -1308,7 +1308,7 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
     k_lean32(const Inst* __restrict__ insts, const LeanConst* __restrict__ lconst,
              const CUtensorMap* __restrict__ tmaps, const int4* __restrict__ tile_desc,
              const uint32_t* __restrict__ flags_in, uint32_t* __restrict__ flags_out, int total, int reverse,
-             int* __restrict__ err) {
+             int lose_box, int* __restrict__ err) {
   using S = Lean<N, K1, TX, TY>;
   constexpr int STAGES = S::STAGES, TPW = S::TPW, LP = S::LP;
   static_assert(STAGES >= 2, "a stage loads while another is computed");
@@ -1354,6 +1354,8 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
                      __shfl_sync(0xffffffffu, mx0, src), __shfl_sync(0xffffffffu, my0, src));
   };
   // record the next TPW tiles in stage s and start their boxes
+  // failure-detection test: the first warp to take the token err[1] issues none of that
+  // stage's boxes, so its wait expires
   auto fill = [&](int s) {
     int4 e[TPW];
     int nv = 0;
@@ -1366,11 +1368,12 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
 #pragma unroll
       for (int j = 0; j < TPW; j++) ent[s * TPW + j] = e[j];
       if (nv) {
+        const bool lose = lose_box && atomicExch(&err[1], 0) != 0;
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_expect_tx(&bar[s], nv * S::BYTES);
 #pragma unroll
         for (int j = 0; j < TPW; j++)
-          if (e[j].x >= 0)
+          if (e[j].x >= 0 && !lose)
             tma_load_3d(slots + (s * TPW + j) * (S::SLOT / 4), &tmaps[e[j].y >> 3], &bar[s], e[j].w - 4,
                         e[j].z - 1, 0);
       }
@@ -1492,7 +1495,7 @@ using namespace gp32;
 struct KernelSet {
   void (*general)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*, int);
   void (*lean)(const Inst*, const LeanConst*, const CUtensorMap*, const int4*, const uint32_t*, uint32_t*, int, int,
-               int*);
+               int, int*);
   void (*list)(const int4*, const uint32_t*, int, int2*, int*);
   size_t smem_general, smem_lean;
 };
@@ -1546,6 +1549,7 @@ struct gp_f32_batch {
   int n = 0, N = 0, K1 = 0, aniso = 0;
   int tx = 16, ty = 32;  // tile shape (autotuned)
   int narrowband = 1;    // send the tiles lean_phase accepts to the lean kernel
+  int lose_box = 0;      // failure-detection test: the next lean launch loses one stage's boxes
   std::vector<gp_model> gm;
   std::vector<Inst> hinst[2];  // [buffer parity]
   Inst* dinst[2] = {nullptr, nullptr};
@@ -1624,8 +1628,8 @@ cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** ou
   if (e == cudaSuccess) e = cudaMalloc(&b->dlconst, sizeof(LeanConst) * hl.size());
   if (e == cudaSuccess)
     e = cudaMemcpy(b->dlconst, hl.data(), sizeof(LeanConst) * hl.size(), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMalloc(&b->derr, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(b->derr, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->derr, 2 * sizeof(int));  // error word, test token
+  if (e == cudaSuccess) e = cudaMemset(b->derr, 0, 2 * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&b->dcnt, 4 * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(b->dcnt, 0, 4 * sizeof(int));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
@@ -1896,8 +1900,11 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
     if ((e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess) return e;
   }
   if (E && ((e = cudaEventRecord(E[0], ls)) != cudaSuccess)) return e;
+  if (b->lose_box)  // failure-detection test: a nonzero token, taken by one warp
+    if ((e = cudaMemsetAsync(b->derr + 1, 1, sizeof(int), ls)) != cudaSuccess) return e;
   k.lean<<<b->grid_lean, 32 * GP_LEAN_WARPS, k.smem_lean, ls>>>(b->dinst[p], b->dlconst, b->dtmap[p], b->dtile_desc, flags_in,
-                                                 flags_out, b->total_tiles, p, b->derr);
+                                                 flags_out, b->total_tiles, p, b->lose_box, b->derr);
+  b->lose_box = 0;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E && ((e = cudaEventRecord(E[1], ls)) != cudaSuccess)) return e;
   if (E && ((e = cudaEventRecord(E[2], s)) != cudaSuccess)) return e;
@@ -1938,6 +1945,10 @@ cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s,
   *lean_cells = c;
   return cudaSuccess;
 }
+
+// Failure-detection test: the next lean-kernel launch leaves one staged box
+// unissued, so that its bounded wait expires and the error word is set.
+void gp_f32_batch_test_lose_box(gp_f32_batch* b) { b->lose_box = 1; }
 
 // device word set by a lean kernel whose staged box did not arrive (0 = none)
 const int* gp_f32_batch_error_word(const gp_f32_batch* b) { return b->derr; }
