@@ -176,6 +176,9 @@ extern "C" int gp_create(const gp_model* m, int precision, gp_ctx** out) {
   }
   if (ok) ok = cudaMalloc(&c->partials, (size_t)c->red_blocks * 64 * sizeof(double)) == cudaSuccess &&
                cudaMalloc(&c->reduced, 64 * sizeof(double)) == cudaSuccess;
+  // the zero fills above run on the legacy stream, which the context's non-blocking stream does not
+  // wait for: they must have landed before an upload on that stream can follow
+  if (ok) ok = cudaDeviceSynchronize() == cudaSuccess;
   if (ok && precision == GP_FP32) {
     ok = gp_f32_batch_create(m, 1, &c->f32) == cudaSuccess;
     if (ok) {
