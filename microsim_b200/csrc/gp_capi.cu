@@ -673,6 +673,7 @@ struct gp_batch {
   int red_blocks = 296;
   int64_t launches = 0;
   int tx = 16, ty = 32;
+  int lose_pending = 0;  // failure-detection test armed for the next step
 };
 
 static void batch_drop_graphs(gp_batch* b) {
@@ -813,6 +814,15 @@ static int batch_capture(gp_batch* b, int parity) {
 
 extern "C" int gp_batch_step(gp_batch* b, int64_t nsteps) {
   if (!b || nsteps < 0) return GP_E_ARG;
+  if (b->lose_pending && nsteps > 0) {  // failure-detection test: one direct step that loses a box
+    b->lose_pending = 0;
+    gp_f32_batch_test_lose_box(b->f32);
+    GP_CUDA(gp_f32_batch_launch(b->f32, b->parity, b->stream));
+    b->launches += gp_f32_batch_launches_per_step(b->f32);
+    b->parity ^= 1;
+    b->have_prev = 1;
+    nsteps--;
+  }
   while (nsteps >= b->graph_steps && !gp_f32_batch_timing(b->f32)) {  // timed steps launch directly
     if (!b->graph[b->parity]) {
       int rc = batch_capture(b, b->parity);
@@ -996,7 +1006,7 @@ extern "C" int gp_batch_set_narrowband(gp_batch* b, int on) {
 
 extern "C" int gp_batch_test_lose_box(gp_batch* b) {
   if (!b) return GP_E_ARG;
-  gp_f32_batch_test_lose_box(b->f32);
+  b->lose_pending = 1;  // taken by the next step, launched directly (never into a graph)
   return GP_OK;
 }
 

@@ -1882,6 +1882,7 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
     E = &b->tev[5 * (b->tn++ % gp_f32_batch::kTimingSlots)];
   }
   if (!b->narrowband) {
+    b->lose_box = 0;  // no lean kernel, no staged boxes to lose
     if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
     k.general<<<b->total_tiles, 256, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr,
                                                           flags_out, b->total_tiles);
