@@ -233,6 +233,11 @@ int gp_batch_lean_tiles(gp_batch *b, int64_t *lean, int64_t *total, int64_t *lea
  * occupancy leaves every SM room for full-kernel blocks beside it.
  * gp_batch_get_grids also reports the occupancies. */
 int gp_batch_set_grids(gp_batch *b, int lean_per_sm, int general_per_sm);
+/* Threads per full-kernel block (one interface tile per block): 256, or 512
+ * for binary alloys (shorter chains per thread, half the resident blocks:
+ * faster when few tiles hold an interface).  The autotuner chooses it too. */
+int gp_batch_set_block(gp_batch *b, int threads);
+int gp_batch_get_block(gp_batch *b);
 /* Failure-detection test (no counterpart in the reference): the next step's
  * lean kernel leaves one staged tile box unissued; its wait gives up after one
  * second, the kernel returns, and the next gp_batch_get_stats reports GP_E_CUDA.
@@ -246,8 +251,9 @@ int gp_batch_get_grids(gp_batch *b, int *lean_per_sm, int *general_per_sm, int *
  * full kernel (ms3[0..2]) over the steps since timing was switched on. */
 int gp_batch_set_timing(gp_batch *b, int on);
 int gp_batch_kernel_ms(gp_batch *b, double *ms3, int64_t *steps);
-/* Measured sweep over the tile shapes, each with the lean grid at its
- * occupancy and one block per SM below it, on the batch's own state (restored
+/* Measured sweep over the tile shapes, each with full-kernel blocks of 256
+ * and (binary alloys) 512 threads and the lean grid at its occupancy and one
+ * block per SM below it, on the batch's own state (restored
  * afterwards); the winner is applied and cached in cache_path (may be NULL)
  * per batch signature, read back on the next call. */
 int gp_batch_autotune(gp_batch *b, const char *cache_path, int *tx, int *ty);

@@ -112,6 +112,8 @@ _SIGS = {
     "gp_batch_set_narrowband": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_batch_set_grids": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gp_batch_prepare": (C.c_int, [C.c_void_p]),
+    "gp_batch_set_block": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_batch_get_block": (C.c_int, [C.c_void_p]),
     "gp_batch_test_lose_box": (C.c_int, [C.c_void_p]),
     "gp_batch_get_grids": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
@@ -403,6 +405,13 @@ class Batch:
 
     def set_narrowband(self, on: bool):
         _check("gp_batch_set_narrowband", lib().gp_batch_set_narrowband(self._h, 1 if on else 0))
+
+    def set_block(self, threads: int):
+        """Threads per full-kernel block: 256, or 512 for binary alloys."""
+        _check("gp_batch_set_block", lib().gp_batch_set_block(self._h, threads))
+
+    def block(self) -> int:
+        return lib().gp_batch_get_block(self._h)
 
     def prepare(self):
         """Capture the step graphs now (no step is taken)."""

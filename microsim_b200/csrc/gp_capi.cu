@@ -31,6 +31,9 @@ int gp_f32_batch_tiles(const gp_f32_batch* b);
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s);
 const int* gp_f32_batch_error_word(const gp_f32_batch* b);
 void gp_f32_batch_test_lose_box(gp_f32_batch* b);
+bool gp_f32_batch_set_step_threads(gp_f32_batch* b, int threads);
+int gp_f32_batch_step_threads(const gp_f32_batch* b);
+bool gp_f32_batch_has_wide_step(const gp_f32_batch* b);
 void gp_f32_batch_set_grids(gp_f32_batch* b, int lean_per_sm, int general_per_sm);
 void gp_f32_batch_get_grids(const gp_f32_batch* b, int* lean_per_sm, int* general_per_sm, int* occ_lean,
                             int* occ_general);
@@ -922,15 +925,16 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
     if (f) {
       char line[256];
       while (fgets(line, sizeof line, f)) {
-        int N, K1, an, n, tx, ty, lp;
+        int N, K1, an, n, tx, ty, lp, th;
         long long c;
         double ms;
-        if (sscanf(line, "%d %d %d %lld %d %d %d %d %lf", &N, &K1, &an, &c, &n, &tx, &ty, &lp, &ms) == 9 &&
+        if (sscanf(line, "%d %d %d %lld %d %d %d %d %d %lf", &N, &K1, &an, &c, &n, &tx, &ty, &lp, &th, &ms) == 10 &&
             N == m0.N && K1 == m0.K1 && an == m0.anisotropy && c == cells && n == b->n) {
           fclose(f);
           if (tx_out) *tx_out = tx;
           if (ty_out) *ty_out = ty;
           int rc = gp_batch_set_tile(b, tx, ty);
+          if (rc == GP_OK) rc = gp_batch_set_block(b, th);
           return rc == GP_OK ? gp_batch_set_grids(b, lp, 0) : rc;
         }
       }
@@ -945,7 +949,7 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   cudaEvent_t e0, e1;
   GP_CUDA(cudaEventCreate(&e0));
   GP_CUDA(cudaEventCreate(&e1));
-  int best_tx = b->tx, best_ty = b->ty, best_lp = 0;
+  int best_tx = b->tx, best_ty = b->ty, best_lp = 0, best_th = 256;
   float best = 1e30f;
   for (int s = 0; s < gp_f32_tile_shape_count(); s++) {
     int tx, ty;
@@ -953,9 +957,12 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
     if (gp_batch_set_tile(b, tx, ty) != GP_OK) continue;
     int lp0, gp0, occ_l, occ_g;
     gp_f32_batch_get_grids(b->f32, &lp0, &gp0, &occ_l, &occ_g);
-    // lean grid at occupancy, or one block per SM short of it (room for full-kernel blocks)
-    for (int c = 0; c < (occ_l > 1 ? 2 : 1); c++) {
+    // full-kernel blocks of 256 and (binary alloys) 512 threads; lean grid at occupancy, or
+    // one block per SM short of it (room for full-kernel blocks)
+    for (int v = 0; v < (occ_l > 1 ? 2 : 1) * (gp_f32_batch_has_wide_step(b->f32) ? 2 : 1); v++) {
+      const int c = v % 2 == 1 && occ_l > 1, th = (occ_l > 1 ? v / 2 : v) ? 512 : 256;
       const int lp = c ? occ_l - 1 : 0;
+      gp_f32_batch_set_step_threads(b->f32, th);
       gp_f32_batch_set_grids(b->f32, lp, 0);
       for (int w = 0; w < 3; w++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (w & 1), b->stream));
       GP_CUDA(cudaEventRecord(e0, b->stream));
@@ -971,9 +978,11 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
         best_tx = tx;
         best_ty = ty;
         best_lp = lp;
+        best_th = th;
       }
     }
     gp_f32_batch_set_grids(b->f32, 0, 0);
+    gp_f32_batch_set_step_threads(b->f32, 256);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -982,12 +991,13 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   b->parity = saved_parity;
   b->have_prev = saved_prev;
   int rc = gp_batch_set_tile(b, best_tx, best_ty);
+  if (rc == GP_OK) rc = gp_batch_set_block(b, best_th);
   if (rc == GP_OK) rc = gp_batch_set_grids(b, best_lp, 0);
   if (rc != GP_OK) return rc;
   if (cache_path) {
     FILE* f = fopen(cache_path, "a");
     if (f) {
-      fprintf(f, "%s %d %d %d %.6f\n", key, best_tx, best_ty, best_lp, best / 10.0f);
+      fprintf(f, "%s %d %d %d %d %.6f\n", key, best_tx, best_ty, best_lp, best_th, best / 10.0f);
       fclose(f);
     }
   }
@@ -1003,6 +1013,20 @@ extern "C" int gp_batch_set_narrowband(gp_batch* b, int on) {
   batch_drop_graphs(b);
   return GP_OK;
 }
+
+extern "C" int gp_batch_set_block(gp_batch* b, int threads) {
+  if (!b) return GP_E_ARG;
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  if (!gp_f32_batch_set_step_threads(b->f32, threads)) {
+    gp_set_error("gp_batch_set_block: %d threads per full-kernel block not available (256; 512 for binary alloys)",
+                 threads);
+    return GP_E_ARG;
+  }
+  batch_drop_graphs(b);
+  return GP_OK;
+}
+
+extern "C" int gp_batch_get_block(gp_batch* b) { return b ? gp_f32_batch_step_threads(b->f32) : 0; }
 
 extern "C" int gp_batch_test_lose_box(gp_batch* b) {
   if (!b) return GP_E_ARG;

@@ -349,11 +349,10 @@ __host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ 
 // cnt[1]); the last block to finish resets the counters (cnt[2] counts
 // finished blocks) for the next step.
 // Every tile writes the purity word of its output.
-#ifndef GP_STEP_BLOCKS_BINARY
-#define GP_STEP_BLOCKS_BINARY 4  // resident full-kernel blocks per SM for binary alloys
-#endif
-template <int N, int K1, bool ANISO, int TX, int TY>
-__global__ void __launch_bounds__(256, (N == 2 && K1 == 1) ? GP_STEP_BLOCKS_BINARY : (K1 >= 3 ? 1 : 2))
+// THREADS per block (one tile): 256, or 512 for binary alloys (shorter per-thread chains, half
+// the resident blocks: faster when there are few interface tiles); the autotuner picks.
+template <int N, int K1, bool ANISO, int TX, int TY, int THREADS = 256>
+__global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS : (K1 >= 3 || THREADS > 256 ? 1 : 2))
     k_step32(const Inst* __restrict__ insts, const Model* __restrict__ models, const int* __restrict__ tile_inst,
              const int2* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out, int total) {
   using T = Tile<N, K1, ANISO, TX, TY>;
@@ -1494,6 +1493,7 @@ using namespace gp32;
 // Kernels of one (N, K1, anisotropy, tile shape).
 struct KernelSet {
   void (*general)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*, int);
+  void (*general_wide)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*, int);  // 512 threads
   void (*lean)(const Inst*, const LeanConst*, const CUtensorMap*, const int4*, const uint32_t*, uint32_t*, int, int,
                int, int*);
   void (*list)(const int4*, const uint32_t*, int, int2*, int*);
@@ -1504,6 +1504,8 @@ template <int N, int K1, bool AN, int TX, int TY>
 static KernelSet make_set() {
   KernelSet k;
   k.general = k_step32<N, K1, AN, TX, TY>;
+  k.general_wide = nullptr;
+  if constexpr (N == 2 && K1 == 1) k.general_wide = k_step32<N, K1, AN, TX, TY, 512>;
   k.lean = k_lean32<N, K1, TX, TY>;
   k.list = k_general_list<TX, TY>;
   k.smem_general = Tile<N, K1, AN, TX, TY>::bytes;
@@ -1567,6 +1569,8 @@ struct gp_f32_batch {
   int* dcnt = nullptr;         // [4] list count, queue head, finished blocks
   int grid_general = 0, grid_lean = 0;
   int occ_general = 0, occ_lean = 0;         // resident blocks per SM at full occupancy
+  int step_threads = 256;                    // full-kernel block size: 256 or 512
+  int occ_general_by[2] = {0, 0};            // occupancy of the 256- and 512-thread full kernels
   int lean_per_sm = 0, general_per_sm = 0;   // blocks per SM of the persistent grids (0: occupancy)
   int sms = 0;
   cudaStream_t side = nullptr;
@@ -1747,6 +1751,20 @@ void gp_f32_batch_set_grids(gp_f32_batch* b, int lean_per_sm, int general_per_sm
   if (b->sms) set_grids(b);
 }
 
+// Full-kernel block size (256, or 512 where the 512-thread kernel exists); false if unavailable.
+bool gp_f32_batch_set_step_threads(gp_f32_batch* b, int threads) {
+  if (threads != 256 && !(threads == 512 && b->ks.general_wide)) return false;
+  b->step_threads = threads;
+  if (b->sms) {
+    b->occ_general = b->occ_general_by[threads == 512];
+    set_grids(b);
+  }
+  return true;
+}
+
+int gp_f32_batch_step_threads(const gp_f32_batch* b) { return b->step_threads; }
+bool gp_f32_batch_has_wide_step(const gp_f32_batch* b) { return b->ks.general_wide != nullptr; }
+
 void gp_f32_batch_get_grids(const gp_f32_batch* b, int* lean_per_sm, int* general_per_sm, int* occ_lean,
                             int* occ_general) {
   *lean_per_sm = b->sms ? b->grid_lean / b->sms : 0;
@@ -1806,12 +1824,23 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   }
   e = cudaFuncSetAttribute(ks.general, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_general);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, ks.general, 256, ks.smem_general);
+  int occ_w = 0;
+  if (e == cudaSuccess && ks.general_wide) {
+    e = cudaFuncSetAttribute(ks.general_wide, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(ks.general_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_general);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_w, ks.general_wide, 512, ks.smem_general);
+  }
   if (e == cudaSuccess) e = cudaFuncSetAttribute(ks.lean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_lean);
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, ks.lean, 32 * GP_LEAN_WARPS, ks.smem_lean);
   if (e != cudaSuccess) return e;
   b->sms = sms;
-  b->occ_general = occ_g > 0 ? occ_g : 1;
+  b->occ_general_by[0] = occ_g > 0 ? occ_g : 1;
+  b->occ_general_by[1] = occ_w > 0 ? occ_w : 1;
+  if (!ks.general_wide) b->step_threads = 256;
+  b->occ_general = b->occ_general_by[b->step_threads == 512];
   b->occ_lean = occ_l > 0 ? occ_l : 1;
   set_grids(b);
   return cudaDeviceSynchronize();  // the flag reset above must land before any stream uses them
@@ -1884,7 +1913,7 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   if (!b->narrowband) {
     b->lose_box = 0;  // no lean kernel, no staged boxes to lose
     if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
-    k.general<<<b->total_tiles, 256, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr,
+    (b->step_threads == 512 ? k.general_wide : k.general)<<<b->total_tiles, b->step_threads, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr,
                                                           flags_out, b->total_tiles);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (E) {
@@ -1913,7 +1942,7 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
                                                       b->dcnt);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
-  k.general<<<b->grid_general, 256, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, b->dglist, b->dcnt,
+  (b->step_threads == 512 ? k.general_wide : k.general)<<<b->grid_general, b->step_threads, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, b->dglist, b->dcnt,
                                                          flags_out, b->total_tiles);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E) return cudaEventRecord(E[4], s);

@@ -152,7 +152,7 @@ def test_autotune_restores_state_and_caches(tmp_path):
         after = b.download(0)
         assert (tx, ty) in [(16, 32), (8, 32), (32, 32), (16, 64)]
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
-        assert os.path.exists(cache) and len(open(cache).read().split()) == 9
+        assert os.path.exists(cache) and len(open(cache).read().split()) == 10
         assert b.autotune(cache) == (tx, ty)  # read back from the cache
 
 
@@ -228,12 +228,14 @@ def test_narrow_band_is_bit_identical_to_the_full_kernel():
 
 def test_grid_split_and_prepared_graphs_are_bit_identical():
     """The persistent grids' blocks per SM (lean and full kernels, run
-    concurrently) and graph capture ahead of time change no bits; prepare()
-    takes no step."""
+    concurrently), the full kernel's block size and graph capture ahead of time
+    change no bits; prepare() takes no step."""
     m, phi, mu = mb.load_case(BINARY["aniso_corner"])
     res = []
-    for grids, prep in [((0, 0), False), ((1, 1), True), ((2, 3), True), ((0, 2), False)]:
+    for grids, prep, block in [((0, 0), False, 256), ((1, 1), True, 512), ((2, 3), True, 256), ((0, 2), False, 512)]:
         with mb.Batch([m, m]) as b:
+            b.set_block(block)
+            assert b.block() == block
             b.set_grids(*grids)
             lp, gp, occ_l, occ_g = b.grids()
             assert lp == (grids[0] if 0 < grids[0] < occ_l else occ_l)
