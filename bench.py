@@ -118,6 +118,8 @@ def dist_setup():
         import torch.distributed as dist
         from datetime import timedelta
         torch.cuda.set_device(local)
+        import microsim_b200 as mb
+        mb.set_device(local)  # the library's own CUDA runtime
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     return world, rank, local
 

@@ -277,6 +277,11 @@ int64_t gp_batch_cells(const gp_batch *b);
 #define GP_NOALLOC_SCRATCH_BYTES (8u << 20)
 int gp_step_f64_noalloc(const gp_model *m, const double *phi, const double *mu, double *phi_out, double *mu_out,
                         int64_t pitch, void *stream);
+/* The GPU that contexts, batches and adjoints created next on this thread use.
+ * The library carries its own CUDA runtime, so the host program's own choice of
+ * device (e.g. torch.cuda.set_device) does not reach it; one process per GPU
+ * calls this once with its local rank. */
+int gp_set_device(int device);
 /* sizeof(gp_model) as compiled into the library (binding layout check). */
 size_t gp_model_sizeof(void);
 /* Text of the last error on this thread. */

@@ -126,6 +126,7 @@ _SIGS = {
     "gp_batch_launch_count": (C.c_int64, [C.c_void_p]),
     "gp_batch_cells": (C.c_int64, [C.c_void_p]),
     "gp_last_error": (C.c_char_p, []),
+    "gp_set_device": (C.c_int, [C.c_int]),
     "gp_smooth": (C.c_int, [C.c_void_p, C.c_int64]),
     "gp_state_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
@@ -177,6 +178,12 @@ class GpError(RuntimeError):
 def _check(what, rc):
     if rc != GP_OK:
         raise GpError(what, rc)
+
+
+def set_device(device: int):
+    """The GPU the library's contexts and batches created next on this thread use
+    (the library's CUDA runtime is its own: torch.cuda.set_device does not reach it)."""
+    _check("gp_set_device", lib().gp_set_device(int(device)))
 
 
 def _ptr(a: np.ndarray):

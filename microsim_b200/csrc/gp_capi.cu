@@ -472,6 +472,17 @@ extern "C" int gp_sync(gp_ctx* c) {
 
 extern "C" size_t gp_model_sizeof(void) { return sizeof(gp_model); }
 
+extern "C" int gp_set_device(int device) {
+  int n = 0;
+  GP_CUDA(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) {
+    gp_set_error("gp_set_device: device %d of %d", device, n);
+    return GP_E_ARG;
+  }
+  GP_CUDA(cudaSetDevice(device));
+  return GP_OK;
+}
+
 extern "C" void* gp_stream(gp_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 extern "C" int gp_state_device(gp_ctx* c, void** phi, void** mu, int64_t* pitch, int64_t* plane, int* esize) {

@@ -48,3 +48,11 @@ def test_lost_box_expires_its_wait_and_is_reported():
             b.stats(0)
     again = _run(m, phi, mu, 5)  # the context still works
     assert np.array_equal(again[0], ref[0]) and np.array_equal(again[1], ref[1])
+
+
+def test_set_device_checks_its_range():
+    mb.set_device(0)
+    with pytest.raises(mb.GpError) as err:
+        mb.set_device(4096)
+    assert err.value.rc == mb.GP_E_ARG
+    mb.set_device(0)
