@@ -158,7 +158,8 @@ def exchange_local(ctxs, copies):
 
 def exchange_nccl(ctx, copies, rank: int):
     """Halo rows of this rank's context with the other ranks (torch.distributed
-    over NCCL; one process per GPU)."""
+    over NCCL; one process per GPU, the context created after
+    microsim_b200.set_device(local rank))."""
     import torch
     import torch.distributed as dist
     ctx.sync()
