@@ -238,6 +238,12 @@ int gp_batch_set_grids(gp_batch *b, int lean_per_sm, int general_per_sm);
  * faster when few tiles hold an interface).  The autotuner chooses it too. */
 int gp_batch_set_block(gp_batch *b, int threads);
 int gp_batch_get_block(gp_batch *b);
+/* How the full kernel finds the tiles the lean kernel rejects: 0 = a list
+ * kernel collects them into a queue (best with many interface tiles), 1 = each
+ * full-kernel block scans its own interleaved share of the tiles (one launch
+ * fewer per step, best with few).  The autotuner chooses it too. */
+int gp_batch_set_scan(gp_batch *b, int on);
+int gp_batch_get_scan(gp_batch *b);
 /* Failure-detection test (no counterpart in the reference): the next step's
  * lean kernel leaves one staged tile box unissued; its wait gives up after one
  * second, the kernel returns, and the next gp_batch_get_stats reports GP_E_CUDA.
@@ -252,8 +258,9 @@ int gp_batch_get_grids(gp_batch *b, int *lean_per_sm, int *general_per_sm, int *
 int gp_batch_set_timing(gp_batch *b, int on);
 int gp_batch_kernel_ms(gp_batch *b, double *ms3, int64_t *steps);
 /* Measured sweep over the tile shapes, each with full-kernel blocks of 256
- * and (binary alloys) 512 threads and the lean grid at its occupancy and one
- * block per SM below it, on the batch's own state (restored
+ * and (binary alloys) 512 threads, the list or scan way of finding the
+ * interface tiles, and the lean grid at its occupancy and one block per SM
+ * below it, on the batch's own state (restored
  * afterwards); the winner is applied and cached in cache_path (may be NULL)
  * per batch signature, read back on the next call. */
 int gp_batch_autotune(gp_batch *b, const char *cache_path, int *tx, int *ty);

@@ -114,6 +114,8 @@ _SIGS = {
     "gp_batch_prepare": (C.c_int, [C.c_void_p]),
     "gp_batch_set_block": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_batch_get_block": (C.c_int, [C.c_void_p]),
+    "gp_batch_set_scan": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_batch_get_scan": (C.c_int, [C.c_void_p]),
     "gp_batch_test_lose_box": (C.c_int, [C.c_void_p]),
     "gp_batch_get_grids": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
@@ -419,6 +421,13 @@ class Batch:
 
     def block(self) -> int:
         return lib().gp_batch_get_block(self._h)
+
+    def set_scan(self, on: bool):
+        """Full-kernel blocks find their own interface tiles (True) or take them from the list."""
+        _check("gp_batch_set_scan", lib().gp_batch_set_scan(self._h, 1 if on else 0))
+
+    def scan(self) -> bool:
+        return bool(lib().gp_batch_get_scan(self._h))
 
     def prepare(self):
         """Capture the step graphs now (no step is taken)."""

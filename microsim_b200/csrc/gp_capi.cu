@@ -34,6 +34,8 @@ void gp_f32_batch_test_lose_box(gp_f32_batch* b);
 bool gp_f32_batch_set_step_threads(gp_f32_batch* b, int threads);
 int gp_f32_batch_step_threads(const gp_f32_batch* b);
 bool gp_f32_batch_has_wide_step(const gp_f32_batch* b);
+void gp_f32_batch_set_scan(gp_f32_batch* b, int on);
+int gp_f32_batch_scan(const gp_f32_batch* b);
 void gp_f32_batch_set_grids(gp_f32_batch* b, int lean_per_sm, int general_per_sm);
 void gp_f32_batch_get_grids(const gp_f32_batch* b, int* lean_per_sm, int* general_per_sm, int* occ_lean,
                             int* occ_general);
@@ -936,16 +938,18 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
     if (f) {
       char line[256];
       while (fgets(line, sizeof line, f)) {
-        int N, K1, an, n, tx, ty, lp, th;
+        int N, K1, an, n, tx, ty, lp, th, sc;
         long long c;
         double ms;
-        if (sscanf(line, "%d %d %d %lld %d %d %d %d %d %lf", &N, &K1, &an, &c, &n, &tx, &ty, &lp, &th, &ms) == 10 &&
+        if (sscanf(line, "%d %d %d %lld %d %d %d %d %d %d %lf", &N, &K1, &an, &c, &n, &tx, &ty, &lp, &th, &sc, &ms) ==
+                11 &&
             N == m0.N && K1 == m0.K1 && an == m0.anisotropy && c == cells && n == b->n) {
           fclose(f);
           if (tx_out) *tx_out = tx;
           if (ty_out) *ty_out = ty;
           int rc = gp_batch_set_tile(b, tx, ty);
           if (rc == GP_OK) rc = gp_batch_set_block(b, th);
+          if (rc == GP_OK) rc = gp_batch_set_scan(b, sc);
           return rc == GP_OK ? gp_batch_set_grids(b, lp, 0) : rc;
         }
       }
@@ -960,7 +964,7 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   cudaEvent_t e0, e1;
   GP_CUDA(cudaEventCreate(&e0));
   GP_CUDA(cudaEventCreate(&e1));
-  int best_tx = b->tx, best_ty = b->ty, best_lp = 0, best_th = 256;
+  int best_tx = b->tx, best_ty = b->ty, best_lp = 0, best_th = 256, best_sc = 0;
   float best = 1e30f;
   for (int s = 0; s < gp_f32_tile_shape_count(); s++) {
     int tx, ty;
@@ -969,12 +973,16 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
     int lp0, gp0, occ_l, occ_g;
     gp_f32_batch_get_grids(b->f32, &lp0, &gp0, &occ_l, &occ_g);
     // full-kernel blocks of 256 and (binary alloys) 512 threads; lean grid at occupancy, or
-    // one block per SM short of it (room for full-kernel blocks)
-    for (int v = 0; v < (occ_l > 1 ? 2 : 1) * (gp_f32_batch_has_wide_step(b->f32) ? 2 : 1); v++) {
-      const int c = v % 2 == 1 && occ_l > 1, th = (occ_l > 1 ? v / 2 : v) ? 512 : 256;
+    // one block per SM short of it (room for full-kernel blocks); the interface tiles listed by
+    // the list kernel, or found by the full kernel's blocks themselves
+    for (int v = 0; v < 8; v++) {
+      const int th = v & 1 ? 512 : 256, c = (v >> 1) & 1, sc = v >> 2;
+      if (th == 512 && !gp_f32_batch_has_wide_step(b->f32)) continue;
+      if (c && occ_l < 2) continue;
       const int lp = c ? occ_l - 1 : 0;
       gp_f32_batch_set_step_threads(b->f32, th);
       gp_f32_batch_set_grids(b->f32, lp, 0);
+      gp_f32_batch_set_scan(b->f32, sc);
       for (int w = 0; w < 3; w++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (w & 1), b->stream));
       GP_CUDA(cudaEventRecord(e0, b->stream));
       for (int r = 0; r < 10; r++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (r & 1), b->stream));
@@ -990,10 +998,12 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
         best_ty = ty;
         best_lp = lp;
         best_th = th;
+        best_sc = sc;
       }
     }
     gp_f32_batch_set_grids(b->f32, 0, 0);
     gp_f32_batch_set_step_threads(b->f32, 256);
+    gp_f32_batch_set_scan(b->f32, 0);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1003,12 +1013,13 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   b->have_prev = saved_prev;
   int rc = gp_batch_set_tile(b, best_tx, best_ty);
   if (rc == GP_OK) rc = gp_batch_set_block(b, best_th);
+  if (rc == GP_OK) rc = gp_batch_set_scan(b, best_sc);
   if (rc == GP_OK) rc = gp_batch_set_grids(b, best_lp, 0);
   if (rc != GP_OK) return rc;
   if (cache_path) {
     FILE* f = fopen(cache_path, "a");
     if (f) {
-      fprintf(f, "%s %d %d %d %d %.6f\n", key, best_tx, best_ty, best_lp, best_th, best / 10.0f);
+      fprintf(f, "%s %d %d %d %d %d %.6f\n", key, best_tx, best_ty, best_lp, best_th, best_sc, best / 10.0f);
       fclose(f);
     }
   }
@@ -1038,6 +1049,16 @@ extern "C" int gp_batch_set_block(gp_batch* b, int threads) {
 }
 
 extern "C" int gp_batch_get_block(gp_batch* b) { return b ? gp_f32_batch_step_threads(b->f32) : 0; }
+
+extern "C" int gp_batch_set_scan(gp_batch* b, int on) {
+  if (!b) return GP_E_ARG;
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  gp_f32_batch_set_scan(b->f32, on);
+  batch_drop_graphs(b);
+  return GP_OK;
+}
+
+extern "C" int gp_batch_get_scan(gp_batch* b) { return b ? gp_f32_batch_scan(b->f32) : 0; }
 
 extern "C" int gp_batch_test_lose_box(gp_batch* b) {
   if (!b) return GP_E_ARG;

@@ -354,7 +354,8 @@ __host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ 
 template <int N, int K1, bool ANISO, int TX, int TY, int THREADS = 256>
 __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS : (K1 >= 3 || THREADS > 256 ? 1 : 2))
     k_step32(const Inst* __restrict__ insts, const Model* __restrict__ models, const int* __restrict__ tile_inst,
-             const int2* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out, int total) {
+             const int2* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out, int total,
+             const int4* __restrict__ tile_desc, const uint32_t* __restrict__ flags_in) {
   using T = Tile<N, K1, ANISO, TX, TY>;
   constexpr int X2 = T::X2, Y2 = T::Y2, X1 = T::X1, Y1 = T::Y1, W = T::W, Q = T::Q;
   constexpr int L = N - 1;
@@ -366,14 +367,46 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
   __shared__ __align__(16) Inst sInst;
   __shared__ int s_tile, s_model, s_reload;
   __shared__ unsigned s_bad;
+  // scan mode (tile_desc given): the block's own tiles blockIdx.x + grid * j, scanned THREADS
+  // candidates at a time; the ones lean_phase rejects are listed here and updated in turn
+  __shared__ int2 s_scan[THREADS];
+  __shared__ int s_scan_n, s_scan_k, s_chunk, s_scan_done;
   const int nt = blockDim.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = nt >> 5;
-  if (threadIdx.x == 0) s_model = -1;
+  if (threadIdx.x == 0) {
+    s_model = -1;
+    s_scan_n = s_scan_k = s_chunk = 0;
+    s_scan_done = (int)blockIdx.x >= total;
+  }
 
   for (int iter = 0;; iter++) {
   __syncthreads();  // the previous tile's shared state is no longer read
+  if (tile_desc) {
+    while (s_scan_k >= s_scan_n && !s_scan_done) {  // block-uniform: shared values read after a barrier
+      __syncthreads();
+      if (threadIdx.x == 0) s_scan_n = s_scan_k = 0;
+      __syncthreads();
+      const int64_t t = blockIdx.x + (int64_t)gridDim.x * ((int64_t)s_chunk * nt + threadIdx.x);
+      int4 d = make_int4(0, 0, 0, 0);
+      if (t < total) d = tile_desc[t];
+      const bool gen = t < total && lean_phase(flags_in, (uint32_t)d.w, (int)t) < 0;
+      const unsigned bal = __ballot_sync(0xffffffffu, gen);
+      int base = 0;
+      if (lane == 0 && bal) base = atomicAdd(&s_scan_n, __popc(bal));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (gen) s_scan[base + __popc(bal & ((1u << lane) - 1u))] = make_int2((int)t, d.x);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        s_chunk++;
+        s_scan_done = blockIdx.x + (int64_t)gridDim.x * ((int64_t)s_chunk * nt) >= total;
+      }
+      __syncthreads();
+    }
+  }
   if (threadIdx.x == 0) {
     int2 e = make_int2(-1, 0);
-    if (glist) {  // block k starts with entry k, then takes entries grid, grid + 1, ... from the queue
+    if (tile_desc) {
+      if (s_scan_k < s_scan_n) e = s_scan[s_scan_k++];
+    } else if (glist) {  // block k starts with entry k, then takes entries grid, grid + 1, ... from the queue
       // (claimed when the block is free: the blocks whose first tiles finish early take the rest)
       const int i = iter == 0 ? (int)blockIdx.x : (int)gridDim.x + atomicAdd(&cnt[1], 1);
       const int n0 = cnt[0];
@@ -1492,8 +1525,10 @@ using namespace gp32;
 
 // Kernels of one (N, K1, anisotropy, tile shape).
 struct KernelSet {
-  void (*general)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*, int);
-  void (*general_wide)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*, int);  // 512 threads
+  void (*general)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*, int, const int4*,
+                  const uint32_t*);
+  void (*general_wide)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*, int, const int4*,
+                       const uint32_t*);  // 512 threads
   void (*lean)(const Inst*, const LeanConst*, const CUtensorMap*, const int4*, const uint32_t*, uint32_t*, int, int,
                int, int*);
   void (*list)(const int4*, const uint32_t*, int, int2*, int*);
@@ -1570,6 +1605,7 @@ struct gp_f32_batch {
   int grid_general = 0, grid_lean = 0;
   int occ_general = 0, occ_lean = 0;         // resident blocks per SM at full occupancy
   int step_threads = 256;                    // full-kernel block size: 256 or 512
+  int scan = 0;                              // full-kernel blocks scan their own tiles (no list kernel)
   int occ_general_by[2] = {0, 0};            // occupancy of the 256- and 512-thread full kernels
   int lean_per_sm = 0, general_per_sm = 0;   // blocks per SM of the persistent grids (0: occupancy)
   int sms = 0;
@@ -1763,6 +1799,8 @@ bool gp_f32_batch_set_step_threads(gp_f32_batch* b, int threads) {
 }
 
 int gp_f32_batch_step_threads(const gp_f32_batch* b) { return b->step_threads; }
+void gp_f32_batch_set_scan(gp_f32_batch* b, int on) { b->scan = on ? 1 : 0; }
+int gp_f32_batch_scan(const gp_f32_batch* b) { return b->scan; }
 bool gp_f32_batch_has_wide_step(const gp_f32_batch* b) { return b->ks.general_wide != nullptr; }
 
 void gp_f32_batch_get_grids(const gp_f32_batch* b, int* lean_per_sm, int* general_per_sm, int* occ_lean,
@@ -1913,8 +1951,8 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   if (!b->narrowband) {
     b->lose_box = 0;  // no lean kernel, no staged boxes to lose
     if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
-    (b->step_threads == 512 ? k.general_wide : k.general)<<<b->total_tiles, b->step_threads, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr,
-                                                          flags_out, b->total_tiles);
+    (b->step_threads == 512 ? k.general_wide : k.general)<<<b->total_tiles, b->step_threads, k.smem_general, s>>>(
+        b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr, flags_out, b->total_tiles, nullptr, nullptr);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (E) {
       if ((e = cudaEventRecord(E[4], s)) != cudaSuccess) return e;
@@ -1938,12 +1976,15 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E && ((e = cudaEventRecord(E[1], ls)) != cudaSuccess)) return e;
   if (E && ((e = cudaEventRecord(E[2], s)) != cudaSuccess)) return e;
-  k.list<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dtile_desc, flags_in, b->total_tiles, b->dglist,
-                                                      b->dcnt);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (!b->scan) {
+    k.list<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dtile_desc, flags_in, b->total_tiles, b->dglist,
+                                                        b->dcnt);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
-  (b->step_threads == 512 ? k.general_wide : k.general)<<<b->grid_general, b->step_threads, k.smem_general, s>>>(b->dinst[p], b->dmodel, b->dtile_inst, b->dglist, b->dcnt,
-                                                         flags_out, b->total_tiles);
+  (b->step_threads == 512 ? k.general_wide : k.general)<<<b->grid_general, b->step_threads, k.smem_general, s>>>(
+      b->dinst[p], b->dmodel, b->dtile_inst, b->scan ? nullptr : b->dglist, b->scan ? nullptr : b->dcnt, flags_out,
+      b->total_tiles, b->scan ? b->dtile_desc : nullptr, b->scan ? flags_in : nullptr);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E) return cudaEventRecord(E[4], s);
   if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess) return e;
@@ -1984,4 +2025,4 @@ void gp_f32_batch_test_lose_box(gp_f32_batch* b) { b->lose_box = 1; }
 const int* gp_f32_batch_error_word(const gp_f32_batch* b) { return b->derr; }
 
 // kernel launches one gp_f32_batch_launch issues
-int gp_f32_batch_launches_per_step(const gp_f32_batch* b) { return b->narrowband ? 3 : 1; }
+int gp_f32_batch_launches_per_step(const gp_f32_batch* b) { return b->narrowband ? (b->scan ? 2 : 3) : 1; }

@@ -152,7 +152,7 @@ def test_autotune_restores_state_and_caches(tmp_path):
         after = b.download(0)
         assert (tx, ty) in [(16, 32), (8, 32), (32, 32), (16, 64)]
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
-        assert os.path.exists(cache) and len(open(cache).read().split()) == 10
+        assert os.path.exists(cache) and len(open(cache).read().split()) == 11
         assert b.autotune(cache) == (tx, ty)  # read back from the cache
 
 
@@ -191,10 +191,11 @@ def test_narrow_band_is_bit_identical_to_the_full_kernel():
     loaded.append((m4, p4, u4))
     models = [m for m, _, _ in loaded]
 
-    def run(on, tile, reupload=False):
+    def run(on, tile, reupload=False, scan=False):
         with mb.Batch(models) as b:
             b.set_tile(*tile)
             b.set_narrowband(on)
+            b.set_scan(scan)
             for i, (_, p, u) in enumerate(loaded):
                 b.upload(i, p, u)
             b.step(150)  # graph replays and direct launches, both buffer parities
@@ -207,8 +208,9 @@ def test_narrow_band_is_bit_identical_to_the_full_kernel():
 
     ref, (lean0, _) = run(False, (16, 32))
     assert lean0 == 0
-    for tile in [(16, 32), (8, 32), (32, 32), (16, 64)]:
-        got, (lean, total) = run(True, tile, reupload=tile == (16, 32))
+    for tile, scan in [((16, 32), False), ((8, 32), False), ((32, 32), False), ((16, 64), False),
+                       ((16, 32), True), ((8, 32), True)]:
+        got, (lean, total) = run(True, tile, reupload=tile == (16, 32), scan=scan)
         assert lean > total // 2, (tile, lean, total)  # the lean kernel does most of the work
         for (p1, u1), (p0, u0) in zip(got, ref):
             assert np.array_equal(p1, p0) and np.array_equal(u1, u0), tile
@@ -228,14 +230,17 @@ def test_narrow_band_is_bit_identical_to_the_full_kernel():
 
 def test_grid_split_and_prepared_graphs_are_bit_identical():
     """The persistent grids' blocks per SM (lean and full kernels, run
-    concurrently), the full kernel's block size and graph capture ahead of time
-    change no bits; prepare() takes no step."""
+    concurrently), the full kernel's block size, the scan or list way of finding
+    the interface tiles and graph capture ahead of time change no bits; prepare()
+    takes no step."""
     m, phi, mu = mb.load_case(BINARY["aniso_corner"])
     res = []
-    for grids, prep, block in [((0, 0), False, 256), ((1, 1), True, 512), ((2, 3), True, 256), ((0, 2), False, 512)]:
+    for grids, prep, block, scan in [((0, 0), False, 256, False), ((1, 1), True, 512, True),
+                                     ((2, 3), True, 256, True), ((0, 2), False, 512, False)]:
         with mb.Batch([m, m]) as b:
             b.set_block(block)
-            assert b.block() == block
+            b.set_scan(scan)
+            assert b.block() == block and b.scan() == scan
             b.set_grids(*grids)
             lp, gp, occ_l, occ_g = b.grids()
             assert lp == (grids[0] if 0 < grids[0] < occ_l else occ_l)
