@@ -23,9 +23,17 @@
 //  * The first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress, with that device current) and caches it; make that
 //    first call before any stream capture.
+//  * The device is this library's current device, the one gp_set_device chose
+//    (device 0 unless it was called): the library carries its own CUDA
+//    runtime, so the host program's own device choice does not reach it.  The
+//    four buffers and the stream must belong to that device; a call with any of
+//    them elsewhere is rejected with GP_E_ARG, as is an output whose bytes
+//    overlap an input or the other output.
 //  * Host code cannot use the array's name as a device address: the symbol
 //    seen by host code is a host-side stand-in.  Only the address returned by
 //    cudaGetSymbolAddress is passed to the kernels.
+
+#include <stdint.h>
 
 #include <mutex>
 
@@ -83,11 +91,61 @@ extern "C" int gp_step_f64_noalloc(const gp_model* m, const double* phi, const d
                  (long long)need, (long long)GP_NOALLOC_SCRATCH_BYTES);
     return GP_E_SIZE;
   }
+  // The step reads neighbours of the old state while it writes the new one, so no byte of an
+  // output may lie inside an input (or the other output): compare the byte ranges the call touches.
+  {
+    const int64_t plane = m->mesh_x * pitch, row_end = (m->mesh_x - 1) * pitch + m->mesh_y;
+    const uintptr_t lo[4] = {(uintptr_t)phi, (uintptr_t)mu, (uintptr_t)phi_out, (uintptr_t)mu_out};
+    const int64_t n[4] = {(m->N - 1) * plane + row_end, (m->K1 - 1) * plane + row_end,
+                          (m->N - 1) * plane + row_end, (m->K1 - 1) * plane + row_end};
+    for (int o = 2; o < 4; o++)
+      for (int i = 0; i < o; i++) {
+        const uintptr_t a0 = lo[i], a1 = lo[i] + (uintptr_t)n[i] * sizeof(double);
+        const uintptr_t b0 = lo[o], b1 = lo[o] + (uintptr_t)n[o] * sizeof(double);
+        if (a0 < b1 && b0 < a1) {
+          gp_set_error("gp_step_f64_noalloc: output %s overlaps %s (the step reads neighbours of the old state "
+                       "while it writes the new one)", o == 2 ? "phi_out" : "mu_out",
+                       i == 0 ? "phi" : i == 1 ? "mu" : "phi_out");
+          return GP_E_ARG;
+        }
+      }
+  }
+  // This library carries its own CUDA runtime: its current device is the one gp_set_device chose
+  // (device 0 by default), not the host program's.  The buffers and the stream must live there,
+  // or the kernels would run on another GPU's scratch array and stream.
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     gp_set_error("gp_step_f64_noalloc: no usable current device (%s)", cudaGetErrorString(e));
     return GP_E_CUDA;
+  }
+  {
+    const void* bufs[4] = {phi, mu, phi_out, mu_out};
+    const char* names[4] = {"phi", "mu", "phi_out", "mu_out"};
+    for (int i = 0; i < 4; i++) {
+      cudaPointerAttributes at;
+      e = cudaPointerGetAttributes(&at, bufs[i]);
+      if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        gp_set_error("gp_step_f64_noalloc: %s is not a pointer CUDA knows (%s)", names[i], cudaGetErrorString(e));
+        return GP_E_ARG;
+      }
+      if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != dev) {
+        gp_set_error("gp_step_f64_noalloc: %s is not device memory of the library's current device %d "
+                     "(select the buffers' GPU with gp_set_device)", names[i], dev);
+        return GP_E_ARG;
+      }
+    }
+    if (stream) {
+      int sdev = -1;
+      e = cudaStreamGetDevice((cudaStream_t)stream, &sdev);
+      if (e != cudaSuccess || sdev != dev) {
+        (void)cudaGetLastError();
+        gp_set_error("gp_step_f64_noalloc: the stream belongs to device %d, not the library's current device %d "
+                     "(select it with gp_set_device)", sdev, dev);
+        return GP_E_ARG;
+      }
+    }
   }
   double* scratch = nullptr;
   {

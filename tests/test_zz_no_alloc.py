@@ -40,6 +40,25 @@ def _model(case):
     return m, phi, mu
 
 
+def _poison_scratch(f, m, dev, stream):
+    """One call on a larger grid (480 x 480, within the fixed scratch for up to 4 phases) whose
+    mu is NaN and whose phi is random, so every phase is active and the Delta-phi ring the call
+    leaves in the shared scratch array is NaN over more than the following grid's extent.  The
+    next call must rewrite every ring cell it reads, or NaN reaches its results."""
+    import torch
+
+    big = m.copy()
+    big.mesh_x, big.mesh_y = 480, 480
+    g = torch.Generator(device="cpu").manual_seed(7)
+    P = torch.rand((m.N, 480, 480), generator=g, dtype=torch.float64).to(dev)
+    U = torch.full((m.K1, 480, 480), float("nan"), dtype=torch.float64, device=dev)
+    P2, U2 = torch.empty_like(P), torch.empty_like(U)
+    rc = f(C.byref(big), P.data_ptr(), U.data_ptr(), P2.data_ptr(), U2.data_ptr(), 480, stream.cuda_stream)
+    assert rc == mb.GP_OK, mb.lib().gp_last_error()
+    torch.cuda.synchronize(dev)
+    assert torch.isnan(P2).any()  # the poison reached the step (and so the ring)
+
+
 @pytest.mark.parametrize("case,pitch_pad", [("aniso_obst_bin_per", 0), ("four_phase_ternary", 40),
                                             ("three_phase_eutectic", 7)])
 def test_noalloc_matches_regular_step_twice(case, pitch_pad):
@@ -68,6 +87,7 @@ def test_noalloc_matches_regular_step_twice(case, pitch_pad):
     pb, ub = dev_state(np.zeros_like(phi), np.zeros_like(mu))
     stream = torch.cuda.current_stream(dev)
     f = _entry()
+    _poison_scratch(f, m, dev, stream)
     torch.cuda.synchronize(dev)
     rc = f(C.byref(m), pa.data_ptr(), ua.data_ptr(), pb.data_ptr(), ub.data_ptr(), pitch, stream.cuda_stream)
     assert rc == mb.GP_OK, mb.lib().gp_last_error()
@@ -96,3 +116,19 @@ def test_noalloc_rejects_grids_beyond_the_scratch_and_bad_buffers():
     assert b"scratch" in mb.lib().gp_last_error()
     rc = f(C.byref(m), a.data_ptr(), a.data_ptr(), a.data_ptr(), b.data_ptr(), m.mesh_y, None)
     assert rc == mb.GP_E_ARG  # in place is refused
+    # a partial overlap of an output with an input is refused too (phi_out starts inside phi)
+    plane = m.mesh_x * m.mesh_y
+    P = torch.zeros(4 * m.N * plane, dtype=torch.float64, device=dev)
+    U = torch.zeros(2 * m.K1 * plane, dtype=torch.float64, device=dev)
+    rc = f(C.byref(m), P.data_ptr(), U.data_ptr(), P.data_ptr() + 8 * plane, U.data_ptr() + 8 * m.K1 * plane,
+           m.mesh_y, None)
+    assert rc == mb.GP_E_ARG and b"overlaps" in mb.lib().gp_last_error()
+    # mu_out overlapping phi (phi and mu packed into one buffer the wrong way) is refused
+    rc = f(C.byref(m), P.data_ptr(), U.data_ptr(), P.data_ptr() + 8 * 2 * m.N * plane,
+           P.data_ptr() + 8 * (m.N * plane - 1), m.mesh_y, None)
+    assert rc == mb.GP_E_ARG and b"overlaps" in mb.lib().gp_last_error()
+    # host memory is not a device buffer of the library's current device
+    h = np.zeros(m.N * plane)
+    rc = f(C.byref(m), h.ctypes.data, U.data_ptr(), P.data_ptr() + 8 * 2 * m.N * plane,
+           U.data_ptr() + 8 * m.K1 * plane, m.mesh_y, None)
+    assert rc == mb.GP_E_ARG and b"device memory" in mb.lib().gp_last_error()
