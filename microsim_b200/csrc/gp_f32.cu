@@ -401,6 +401,9 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
       }
       __syncthreads();
     }
+    // every warp has evaluated the loop condition before thread 0 below advances s_scan_k
+    // (a warp reading it late would otherwise see the list exhausted and scan alone)
+    __syncthreads();
   }
   if (threadIdx.x == 0) {
     int2 e = make_int2(-1, 0);
