@@ -10,7 +10,8 @@
   difference;
 * checkpoint spacing does not change the gradient; ceil(N/s) + s states are
   stored;
-* the FP32 adjoint agrees with the FP64 reference adjoint;
+* the FP32 adjoint agrees with the FP64 reference adjoint and with central
+  differences to 1e-3 relative;
 * the torch.autograd.Function gives the same gradient.
 """
 import numpy as np
@@ -108,15 +109,27 @@ def test_checkpoint_spacing_does_not_change_the_gradient():
         np.testing.assert_allclose(g, grads[1], rtol=1e-9, atol=1e-14)
 
 
-def test_fp32_adjoint_agrees_with_fp64_reference():
-    m, phi, mu = mb.load_case(CASES["obstacle_neumann"])
-    _, target = _loss_and_target(m, phi, mu)
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp32_adjoint_agrees_with_fp64_reference_and_central_differences(name):
+    """The FP32 adjoint (FP32 forward and reverse, FP64 parameter reductions) against the FP64
+    reference adjoint and against central differences of the FP64 forward (h = 1e-4 relative):
+    both within the 1e-3 relative bar."""
+    m, phi, mu = mb.load_case(CASES[name])
+    loss, target = _loss_and_target(m, phi, mu)
     g = {}
     for prec in (mb.GP_FP64, mb.GP_FP32):
         with adjoint.Adjoint(m, prec) as a:
             ph, _ = a.forward(phi, mu, STEPS)
             g[prec] = a.backward(2.0 * (ph - target))
-    np.testing.assert_allclose(g[mb.GP_FP32], g[mb.GP_FP64], rtol=1e-2)
+    np.testing.assert_allclose(g[mb.GP_FP32], g[mb.GP_FP64], rtol=1e-3)
+    p = adjoint.params_of(m)
+    for i in range(adjoint.NPARAM):
+        h = 1e-4 * abs(p[i])
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        fd = (loss(pp) - loss(pm)) / (2 * h)
+        assert abs(g[mb.GP_FP32][i] - fd) <= 1e-3 * abs(fd), (name, adjoint.NAMES[i], g[mb.GP_FP32][i], fd)
 
 
 def test_torch_function_gives_the_adjoint_gradient():

@@ -3,7 +3,7 @@ kernel gives up after one second, sets the batch's error word and returns.
 
 The test makes one wait run out by having the next launch leave one staged
 tile box unissued (gp_batch_test_lose_box); nothing faults or hangs.  The
-statistics read-back then reports GP_E_CUDA, and the GPU context stays usable:
+statistics read-back then reports GP_E_TIMEOUT, and the GPU context stays usable:
 a fresh batch on the same device steps and matches a run made before."""
 import time
 
@@ -41,7 +41,7 @@ def test_lost_box_expires_its_wait_and_is_reported():
         with pytest.raises(mb.GpError) as err:
             b.stats(0)
         waited = time.perf_counter() - t0
-        assert err.value.rc == mb.GP_E_CUDA
+        assert err.value.rc == mb.GP_E_TIMEOUT
         assert "did not arrive" in str(err.value)
         assert 0.9 < waited < 30.0  # the one-second limit, not a hang
         with pytest.raises(mb.GpError):  # the results stay flagged invalid

@@ -107,8 +107,9 @@ def test_parser_errors_are_reported():
 def test_shipped_reference_fill_vtk():
     """The one golden vector the reference ships for this path: DATA/output.out_0.vtk
     equals the filling of FILLCYLINDER={0,50,50,0,0,20} on the shipped 100x100 input.
-    Reads the reference tree, so it runs only where that tree is mounted."""
-    ref = "/root/reference/Grand_potential_Finite_difference_2D_serial"
+    Reads the reference tree (MICROSIM_REF, default /root/reference), so it runs only where
+    that tree is mounted."""
+    ref = os.path.join(os.environ.get("MICROSIM_REF", "/root/reference"), "Grand_potential_Finite_difference_2D_serial")
     if not os.path.isdir(ref):
         pytest.skip("reference tree not mounted")
     with tempfile.TemporaryDirectory() as d:
