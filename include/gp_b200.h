@@ -117,6 +117,19 @@ typedef struct gp_stats {
   double solute[GP_MAX_K1]; /* sum over cells of sum_a c_a(mu) h_a(phi) (file_writer.h:203-235 integrand) */
   double phase_fraction[GP_MAX_PHASES]; /* sum over cells of phi_a                                      */
   int64_t nonfinite;  /* number of non-finite phi/mu values found                                         */
+  /* Energies of the current state, FP64 sums over the interior cells times dx*dy.  The reference
+   * has no global energy output; these are the functional whose variational derivatives its phase-field
+   * step uses (solverloop/calculate_divergence_phasefield.h:24-26), with cell-centred gradients
+   * (the gradphi_c of solverloop/calculate_gradients.h:92-131) and ghost cells by the boundary map:
+   *   gradient   eps * sum_{a<b} Gamma_ab a_c(R_ab q_ab)^2 |q_ab|^2,  q_ab = phi_a grad phi_b - phi_b grad phi_a
+   *              (functions/function_A_00.h:4-23, function_A_01.h, anisotropy_01.h:30-48; a_c = 1 isotropic)
+   *   potential  (1/eps) * [16/pi^2 sum_{a<b} Gamma_ab |phi_a phi_b|       (obstacle, functionW_01.h:6-39)
+   *                         or 9 sum_{a<b} Gamma_ab phi_a^2 phi_b^2       (well, functionW_02.h:4-33)
+   *                         + sum_{a<b<c} Gamma_abc |phi_a phi_b phi_c|]
+   *   chemical   sum_a h_a(phi) f_a(c_a(mu))        (functionF_01.h:5-18, functionH.h:24-37, c_mu :30-40)
+   *   grand_potential = gradient + potential + sum_a h_a(phi) (f_a(c_a) - mu . c_a)   (the psi of functionF_01.h:41-57)
+   * The free energy is gradient + potential + chemical. */
+  double energy_gradient, energy_potential, energy_chemical, grand_potential;
 } gp_stats;
 
 /* ---------------- host side: files (reference L3/L4) ---------------- */
@@ -244,9 +257,19 @@ int gp_batch_get_block(gp_batch *b);
  * fewer per step, best with few).  The autotuner chooses it too. */
 int gp_batch_set_scan(gp_batch *b, int on);
 int gp_batch_get_scan(gp_batch *b);
+/* Temporal blocking: depth 1 = one launch set per step; depth 2 = blocked
+ * pairs.  In a pair the lean tiles (pure on the tile and its two-cell ring)
+ * take two diffusion steps from one staged mu box -- half the state traffic per
+ * step -- while the full kernel updates the other tiles twice through an
+ * intermediate buffer, which the lean tiles bordering them fill with their
+ * first step.  The results are bit-identical to single steps.  Needs the narrow
+ * band and the list mode (scan off); the autotuner chooses it.  After a pair,
+ * rel_change_* of gp_batch_get_stats covers the pair's two steps. */
+int gp_batch_set_depth(gp_batch *b, int depth);
+int gp_batch_get_depth(gp_batch *b);
 /* Failure-detection test (no counterpart in the reference): the next step's
  * lean kernel leaves one staged tile box unissued; its wait gives up after one
- * second, the kernel returns, and the next gp_batch_get_stats reports GP_E_CUDA.
+ * second, the kernel returns, and the next gp_batch_get_stats reports GP_E_TIMEOUT.
  * The batch's results are invalid from then on. */
 int gp_batch_test_lose_box(gp_batch *b);
 int gp_batch_get_grids(gp_batch *b, int *lean_per_sm, int *general_per_sm, int *occ_lean, int *occ_general);
@@ -259,8 +282,8 @@ int gp_batch_set_timing(gp_batch *b, int on);
 int gp_batch_kernel_ms(gp_batch *b, double *ms3, int64_t *steps);
 /* Measured sweep over the tile shapes, each with full-kernel blocks of 256
  * and (binary alloys) 512 threads, the list or scan way of finding the
- * interface tiles, and the lean grid at its occupancy and one block per SM
- * below it, on the batch's own state (restored
+ * interface tiles, depth 1 or 2 (list mode), and the lean grid at its occupancy
+ * and one block per SM below it, on the batch's own state (restored
  * afterwards); the winner is applied and cached in cache_path (may be NULL)
  * per batch signature, read back on the next call. */
 int gp_batch_autotune(gp_batch *b, const char *cache_path, int *tx, int *ty);
@@ -273,7 +296,10 @@ int64_t gp_batch_cells(const gp_batch *b);
  * allocate device memory (a framework pool that owns the whole GPU, a fixed
  * start-up memory budget).  phi/mu (inputs) and phi_out/mu_out (outputs) are
  * device buffers in this header's layout with the given row pitch (elements,
- * >= mesh_y; plane stride mesh_x*pitch); inputs and outputs must differ.  The
+ * >= mesh_y; plane stride mesh_x*pitch); no output byte may overlap an input
+ * or the other output (GP_E_ARG).  The buffers and the stream must belong to
+ * this library's current device -- the one gp_set_device chose, device 0 by
+ * default, not the host program's own choice -- or the call returns GP_E_ARG.  The
  * Delta-phi ring between the step's two kernels lives in a fixed device array of
  * GP_NOALLOC_SCRATCH_BYTES per GPU, held until the process exits and shared by
  * every call (contents of the last call kept; calls that overlap on the GPU

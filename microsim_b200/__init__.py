@@ -75,7 +75,10 @@ class GpStats(C.Structure):
         ("phi_max", C.c_double * _P), ("phi_min", C.c_double * _P), ("rel_change_phi", C.c_double * _P),
         ("mu_max", C.c_double * _K), ("mu_min", C.c_double * _K), ("rel_change_mu", C.c_double * _K),
         ("solute", C.c_double * _K), ("phase_fraction", C.c_double * _P), ("nonfinite", C.c_int64),
+        ("energy_gradient", C.c_double), ("energy_potential", C.c_double), ("energy_chemical", C.c_double),
+        ("grand_potential", C.c_double),
     ]
+    ENERGIES = ("energy_gradient", "energy_potential", "energy_chemical", "grand_potential")
 
 
 _lib = None
@@ -116,6 +119,8 @@ _SIGS = {
     "gp_batch_get_block": (C.c_int, [C.c_void_p]),
     "gp_batch_set_scan": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_batch_get_scan": (C.c_int, [C.c_void_p]),
+    "gp_batch_set_depth": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_batch_get_depth": (C.c_int, [C.c_void_p]),
     "gp_batch_test_lose_box": (C.c_int, [C.c_void_p]),
     "gp_batch_get_grids": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
@@ -334,11 +339,7 @@ class Context:
         rc = lib().gp_get_stats(self._h, C.byref(st))
         if rc != GP_OK and not (allow_nonfinite and rc == GP_E_NONFINITE):
             raise GpError("gp_get_stats", rc)
-        N, K1 = self.model.N, self.model.K1
-        out = {n: np.array(getattr(st, n)[: (N if ("phi" in n or "phase" in n) else K1)])
-               for n, _ in GpStats._fields_ if n != "nonfinite"}
-        out["nonfinite"] = st.nonfinite
-        return out
+        return _stats_dict(st, self.model.N, self.model.K1)
 
     @property
     def stream(self) -> int:
@@ -351,8 +352,11 @@ class Context:
 
 def _stats_dict(st: GpStats, N: int, K1: int) -> dict:
     out = {n: np.array(getattr(st, n)[: (N if ("phi" in n or "phase" in n) else K1)])
-           for n, _ in GpStats._fields_ if n != "nonfinite"}
+           for n, _ in GpStats._fields_ if n != "nonfinite" and n not in GpStats.ENERGIES}
     out["nonfinite"] = st.nonfinite
+    for n in GpStats.ENERGIES:
+        out[n] = float(getattr(st, n))
+    out["free_energy"] = out["energy_gradient"] + out["energy_potential"] + out["energy_chemical"]
     return out
 
 
@@ -428,6 +432,13 @@ class Batch:
 
     def scan(self) -> bool:
         return bool(lib().gp_batch_get_scan(self._h))
+
+    def set_depth(self, depth: int):
+        """Temporal blocking: 1 (single steps) or 2 (blocked pairs; narrow band in list mode)."""
+        _check("gp_batch_set_depth", lib().gp_batch_set_depth(self._h, depth))
+
+    def depth(self) -> int:
+        return lib().gp_batch_get_depth(self._h)
 
     def prepare(self):
         """Capture the step graphs now (no step is taken)."""

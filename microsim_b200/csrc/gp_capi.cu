@@ -47,6 +47,11 @@ cudaError_t gp_f32_batch_kernel_ms(gp_f32_batch* b, double* ms, int64_t* steps);
 int gp_f32_batch_timing(const gp_f32_batch* b);
 void gp_f32_batch_set_narrowband(gp_f32_batch* b, int on);
 int gp_f32_batch_launches_per_step(const gp_f32_batch* b);
+void gp_f32_batch_bind_x(gp_f32_batch* b, int i, float* phiX, float* muX);
+bool gp_f32_batch_set_depth(gp_f32_batch* b, int depth);
+int gp_f32_batch_depth(const gp_f32_batch* b);
+cudaError_t gp_f32_batch_launch_pair(gp_f32_batch* b, int parity, cudaStream_t s);
+int gp_f32_batch_launches_per_pair(const gp_f32_batch* b);
 int gp_f32_tile_shape_count();
 void gp_f32_tile_shape(int i, int* tx, int* ty);
 
@@ -79,7 +84,7 @@ static cudaError_t ensure_stage(double** buf, size_t* have, size_t need, cudaStr
 // The FP32 form's lean kernel gave up on a staged box (bounded wait expired).
 static int lean_error() {
   gp_set_error("FP32 lean kernel: a staged mu box did not arrive within one second; results are invalid");
-  return GP_E_CUDA;
+  return GP_E_TIMEOUT;
 }
 
 struct gp_ctx {
@@ -519,7 +524,8 @@ struct StatLayout {
   __host__ __device__ int rel_mu(int k) const { return 4 * N + 2 * K1 + k; }
   __host__ __device__ int solute(int k) const { return 4 * N + 3 * K1 + k; }
   __host__ __device__ int nonfinite() const { return 4 * N + 4 * K1; }
-  __host__ __device__ int count() const { return 4 * N + 4 * K1 + 1; }
+  __host__ __device__ int energy(int e) const { return 4 * N + 4 * K1 + 1 + e; }  // gradient, potential, chemical, grand
+  __host__ __device__ int count() const { return 4 * N + 4 * K1 + 5; }
   __host__ __device__ bool is_max(int s) const { return s < N || (s >= 4 * N && s < 4 * N + K1); }
   __host__ __device__ bool is_min(int s) const {
     return (s >= N && s < 2 * N) || (s >= 4 * N + K1 && s < 4 * N + 2 * K1);
@@ -538,6 +544,71 @@ __device__ __forceinline__ double ident(const StatLayout& L, int s) {
   return 0.0;
 }
 
+constexpr int kStatSlots = 4 * GP_MAX_PHASES + 4 * GP_MAX_K1 + 5;
+static_assert(kStatSlots < 63, "slot 63 of the reduction vector carries the FP32 form's error word");
+
+// 4-fold cubic anisotropy a_c of a rotated q (functions/anisotropy_01.h:30-48, same guard)
+__device__ __forceinline__ double stat_ac(double dab, double q0, double q1) {
+  const double q2 = q0 * q0 + q1 * q1;
+  if (q2 <= 1.0e-15) return 1.0;
+  const double s4 = (q0 * q0 * q0 * q0 + q1 * q1 * q1 * q1) / (q2 * q2);
+  return 1.0 - dab * (3.0 - 4.0 * s4);
+}
+
+// Energy densities of interior cell (x, y) (the integrands of gp_stats' energies), FP64 from the
+// stored state; neighbours of edge cells by the boundary map of phi.  e[0] gradient (with eps),
+// e[1] potential (with 1/eps), e[2] sum_a h_a f_a(c_a), e[3] sum_a h_a psi_a (psi_a = f_a - mu.c_a).
+template <typename T>
+__device__ void cell_energy(const gp_model& m, const T* __restrict__ phi, int pitch, int64_t plane, int x, int y,
+                            const double* ph, const double* mm, double* e) {
+  const int N = m.N, K1 = m.K1;
+  double gx[GP_MAX_PHASES], gy[GP_MAX_PHASES];
+  const int xm = gp_map(x - 1, (int)m.mesh_x, m.bc_phi[0]), xp = gp_map(x + 1, (int)m.mesh_x, m.bc_phi[0]);
+  const int ym = gp_map(y - 1, (int)m.mesh_y, m.bc_phi[3]), yp = gp_map(y + 1, (int)m.mesh_y, m.bc_phi[3]);
+  const double hx = 0.5 / m.dx, hy = 0.5 / m.dy;
+  for (int a = 0; a < N; a++) {
+    const T* p = phi + a * plane;
+    gx[a] = ((double)p[(int64_t)xp * pitch + y] - (double)p[(int64_t)xm * pitch + y]) * hx;
+    gy[a] = ((double)p[(int64_t)x * pitch + yp] - (double)p[(int64_t)x * pitch + ym]) * hy;
+  }
+  double eg = 0.0, ew2 = 0.0, ew3 = 0.0;
+  for (int a = 0; a < N; a++)
+    for (int b = a + 1; b < N; b++) {
+      const double Qx = ph[a] * gx[b] - ph[b] * gx[a], Qy = ph[a] * gy[b] - ph[b] * gy[a];
+      double ac = 1.0;
+      if (m.anisotropy)
+        ac = stat_ac(m.dab[a][b], m.R[a][b][0][0] * Qx + m.R[a][b][0][1] * Qy,
+                     m.R[a][b][1][0] * Qx + m.R[a][b][1][1] * Qy);
+      eg += m.Gamma[a][b] * ac * ac * (Qx * Qx + Qy * Qy);
+      ew2 += m.obstacle ? m.Gamma[a][b] * fabs(ph[a] * ph[b]) : m.Gamma[a][b] * ph[a] * ph[a] * ph[b] * ph[b];
+      for (int c = b + 1; c < N; c++) ew3 += m.Gamma_abc[a][b][c] * fabs(ph[a] * ph[b] * ph[c]);
+    }
+  e[0] = m.epsilon * eg;
+  e[1] = (ew2 * (m.obstacle ? m.w_obstacle : 9.0) + ew3) * m.inv_eps;
+  double fch = 0.0, psi = 0.0;
+  for (int a = 0; a < N; a++) {
+    double h = 3.0 * ph[a] * ph[a] - 2.0 * ph[a] * ph[a] * ph[a], s1 = 0.0;
+    for (int b = 0; b < N; b++)
+      for (int c = b + 1; c < N; c++)
+        if (b != a && c != a) s1 += ph[b] * ph[c];
+    h += 2.0 * ph[a] * s1;
+    double c[GP_MAX_K1], f = m.C[a], mc = 0.0;
+    for (int k = 0; k < K1; k++) {
+      c[k] = 0.0;
+      for (int l = 0; l < K1; l++) c[k] += m.cmu[a][k][l] * (mm[l] - m.Beff[a][l]);
+    }
+    for (int k = 0; k < K1; k++) {
+      for (int l = k; l < K1; l++) f += m.A[a][k][l] * c[k] * c[l];
+      f += m.B[a][k] * c[k];
+      mc += mm[k] * c[k];
+    }
+    fch += h * f;
+    psi += h * (f - mc);
+  }
+  e[2] = fch;
+  e[3] = psi;
+}
+
 // One pass over the interior: each block writes its partial vector.
 // The solute integrand is sum_a c_a(mu) h_a(phi) (file_writer.h:203-235).
 template <typename T>
@@ -546,7 +617,7 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
                                                int have_prev, int pitch, int64_t plane, double* __restrict__ partials) {
   const StatLayout L{m.N, m.K1};
   const int S = L.count();
-  double acc[4 * GP_MAX_PHASES + 4 * GP_MAX_K1 + 1];
+  double acc[kStatSlots];
   for (int s = 0; s < S; s++) acc[s] = ident(L, s);
   const int64_t ncell = (int64_t)m.mesh_x * m.mesh_y;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncell; i += (int64_t)gridDim.x * blockDim.x) {
@@ -589,9 +660,15 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
       }
       acc[L.solute(k)] += comp;
     }
+    double e[4];
+    cell_energy<T>(m, phi, pitch, plane, x, y, ph, mm, e);
+    acc[L.energy(0)] += e[0];
+    acc[L.energy(1)] += e[1];
+    acc[L.energy(2)] += e[2];
+    acc[L.energy(3)] += e[0] + e[1] + e[3];
     if (bad) acc[L.nonfinite()] += 1.0;
   }
-  __shared__ double red[8][4 * GP_MAX_PHASES + 4 * GP_MAX_K1 + 1];
+  __shared__ double red[8][kStatSlots];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int s = 0; s < S; s++) {
     double v = acc[s];
@@ -617,6 +694,15 @@ __global__ void k_stats_final(int N, int K1, const double* __restrict__ partials
   double v = partials[s];
   for (int b = 1; b < nblocks; b++) v = combine(L, s, v, partials[(int64_t)b * 64 + s]);
   out[s] = v;
+}
+
+// The energy sums of the reduction vector, integrated (times dx * dy).
+static void stats_energies(const gp_model& m, const StatLayout& L, const double* v, gp_stats* out) {
+  const double da = m.dx * m.dy;
+  out->energy_gradient = v[L.energy(0)] * da;
+  out->energy_potential = v[L.energy(1)] * da;
+  out->energy_chemical = v[L.energy(2)] * da;
+  out->grand_potential = v[L.energy(3)] * da;
 }
 
 extern "C" int gp_get_stats(gp_ctx* c, gp_stats* out) {
@@ -659,6 +745,7 @@ extern "C" int gp_get_stats(gp_ctx* c, gp_stats* out) {
     out->solute[k] = v[L.solute(k)];
   }
   out->nonfinite = (int64_t)v[L.nonfinite()];
+  stats_energies(m, L, v, out);
   return out->nonfinite ? GP_E_NONFINITE : GP_OK;
 }
 
@@ -674,6 +761,7 @@ struct gp_batch {
   std::vector<int> pitch;
   std::vector<int64_t> plane;
   std::vector<size_t> off_phi[2], off_mu[2];  // float offsets into the pool, per buffer
+  std::vector<size_t> off_phi_x, off_mu_x;     // the intermediate state X of a blocked pair
   float* pool = nullptr;
   size_t pool_floats = 0;
   gp_f32_batch* f32 = nullptr;
@@ -690,6 +778,7 @@ struct gp_batch {
   int64_t launches = 0;
   int tx = 16, ty = 32;
   int lose_pending = 0;  // failure-detection test armed for the next step
+  int narrowband_on = 1;
 };
 
 static void batch_drop_graphs(gp_batch* b) {
@@ -746,6 +835,10 @@ extern "C" int gp_batch_create(const gp_model* models, int n, gp_batch** out) {
       b->off_mu[p].push_back(off);
       off += (size_t)gp_round_up(K1 * plane, 64);
     }
+    b->off_phi_x.push_back(off);
+    off += (size_t)gp_round_up(N * plane, 64);
+    b->off_mu_x.push_back(off);
+    off += (size_t)gp_round_up(K1 * plane, 64);
   }
   b->pool_floats = off;
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
@@ -755,9 +848,11 @@ extern "C" int gp_batch_create(const gp_model* models, int n, gp_batch** out) {
             cudaMalloc(&b->reduced, 64 * sizeof(double)) == cudaSuccess &&
             gp_f32_batch_create(models, n, &b->f32) == cudaSuccess;
   if (ok) {
-    for (int i = 0; i < n; i++)
+    for (int i = 0; i < n; i++) {
       gp_f32_batch_bind(b->f32, i, b->pool + b->off_phi[0][i], b->pool + b->off_mu[0][i], b->pool + b->off_phi[1][i],
                         b->pool + b->off_mu[1][i], b->pitch[i], b->plane[i]);
+      gp_f32_batch_bind_x(b->f32, i, b->pool + b->off_phi_x[i], b->pool + b->off_mu_x[i]);
+    }
     ok = gp_f32_batch_set_tiles(b->f32, b->tx, b->ty) == cudaSuccess;
   }
   if (!ok) {
@@ -806,13 +901,25 @@ extern "C" int gp_batch_download(gp_batch* b, int i, double* phi, double* mu) {
   return rc;
 }
 
-// Capture graph_steps launches starting at `parity` (an even count: the graph
-// ends on the parity it starts from).
+// One launch call of the configured depth: a single step, or a blocked pair
+// (two steps; like a single step it moves the state to the other buffer).
+static cudaError_t batch_launch(gp_batch* b, int parity) {
+  return gp_f32_batch_depth(b->f32) == 2 ? gp_f32_batch_launch_pair(b->f32, parity, b->stream)
+                                         : gp_f32_batch_launch(b->f32, parity, b->stream);
+}
+static int batch_launches(gp_batch* b) {
+  return gp_f32_batch_depth(b->f32) == 2 ? gp_f32_batch_launches_per_pair(b->f32)
+                                         : gp_f32_batch_launches_per_step(b->f32);
+}
+
+// Capture graph_steps steps starting at `parity`: graph_steps / depth launch
+// calls, an even number, so the graph ends on the parity it starts from.
 static int batch_capture(gp_batch* b, int parity) {
   cudaGraph_t g = nullptr;
   GP_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
-  for (int s = 0; s < b->graph_steps && e == cudaSuccess; s++) e = gp_f32_batch_launch(b->f32, parity ^ (s & 1), b->stream);
+  const int calls = b->graph_steps / gp_f32_batch_depth(b->f32);
+  for (int s = 0; s < calls && e == cudaSuccess; s++) e = batch_launch(b, parity ^ (s & 1));
   cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
   if (e != cudaSuccess || e2 != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
@@ -839,14 +946,21 @@ extern "C" int gp_batch_step(gp_batch* b, int64_t nsteps) {
     b->have_prev = 1;
     nsteps--;
   }
+  const int depth = gp_f32_batch_depth(b->f32);
   while (nsteps >= b->graph_steps && !gp_f32_batch_timing(b->f32)) {  // timed steps launch directly
     if (!b->graph[b->parity]) {
       int rc = batch_capture(b, b->parity);
       if (rc != GP_OK) return rc;
     }
     GP_CUDA(cudaGraphLaunch(b->graph[b->parity], b->stream));
-    b->launches += (int64_t)b->graph_steps * gp_f32_batch_launches_per_step(b->f32);
+    b->launches += (int64_t)(b->graph_steps / depth) * batch_launches(b);
     nsteps -= b->graph_steps;
+    b->have_prev = 1;
+  }
+  for (; nsteps >= depth && depth > 1; nsteps -= depth) {  // blocked pairs, then single steps
+    GP_CUDA(batch_launch(b, b->parity));
+    b->launches += batch_launches(b);
+    b->parity ^= 1;
     b->have_prev = 1;
   }
   for (; nsteps > 0; nsteps--) {
@@ -908,6 +1022,7 @@ extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
     out->solute[k] = v[L.solute(k)];
   }
   out->nonfinite = (int64_t)v[L.nonfinite()];
+  stats_energies(m, L, v, out);
   return out->nonfinite ? GP_E_NONFINITE : GP_OK;
 }
 
@@ -938,11 +1053,11 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
     if (f) {
       char line[256];
       while (fgets(line, sizeof line, f)) {
-        int N, K1, an, n, tx, ty, lp, th, sc;
+        int N, K1, an, n, tx, ty, lp, th, sc, dp;
         long long c;
         double ms;
-        if (sscanf(line, "%d %d %d %lld %d %d %d %d %d %d %lf", &N, &K1, &an, &c, &n, &tx, &ty, &lp, &th, &sc, &ms) ==
-                11 &&
+        if (sscanf(line, "%d %d %d %lld %d %d %d %d %d %d %d %lf", &N, &K1, &an, &c, &n, &tx, &ty, &lp, &th, &sc, &dp,
+                   &ms) == 12 &&
             N == m0.N && K1 == m0.K1 && an == m0.anisotropy && c == cells && n == b->n) {
           fclose(f);
           if (tx_out) *tx_out = tx;
@@ -950,6 +1065,7 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
           int rc = gp_batch_set_tile(b, tx, ty);
           if (rc == GP_OK) rc = gp_batch_set_block(b, th);
           if (rc == GP_OK) rc = gp_batch_set_scan(b, sc);
+          if (rc == GP_OK) rc = gp_batch_set_depth(b, dp);
           return rc == GP_OK ? gp_batch_set_grids(b, lp, 0) : rc;
         }
       }
@@ -964,33 +1080,38 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   cudaEvent_t e0, e1;
   GP_CUDA(cudaEventCreate(&e0));
   GP_CUDA(cudaEventCreate(&e1));
-  int best_tx = b->tx, best_ty = b->ty, best_lp = 0, best_th = 256, best_sc = 0;
+  int best_tx = b->tx, best_ty = b->ty, best_lp = 0, best_th = 256, best_sc = 0, best_dp = 1;
   float best = 1e30f;
+  const bool nb = b->narrowband_on != 0;
   for (int s = 0; s < gp_f32_tile_shape_count(); s++) {
     int tx, ty;
     gp_f32_tile_shape(s, &tx, &ty);
     if (gp_batch_set_tile(b, tx, ty) != GP_OK) continue;
-    int lp0, gp0, occ_l, occ_g;
-    gp_f32_batch_get_grids(b->f32, &lp0, &gp0, &occ_l, &occ_g);
     // full-kernel blocks of 256 and (binary alloys) 512 threads; lean grid at occupancy, or
     // one block per SM short of it (room for full-kernel blocks); the interface tiles listed by
-    // the list kernel, or found by the full kernel's blocks themselves
-    for (int v = 0; v < 8; v++) {
-      const int th = v & 1 ? 512 : 256, c = (v >> 1) & 1, sc = v >> 2;
+    // the list kernel, or found by the full kernel's blocks themselves; single steps, or blocked
+    // pairs (two steps per lean box; list mode only)
+    for (int v = 0; v < 16; v++) {
+      const int th = v & 1 ? 512 : 256, c = (v >> 1) & 1, sc = (v >> 2) & 1, dp = v & 8 ? 2 : 1;
       if (th == 512 && !gp_f32_batch_has_wide_step(b->f32)) continue;
+      if (dp == 2 && (sc || !nb)) continue;
+      if (!gp_f32_batch_set_depth(b->f32, dp)) continue;
+      int lp0, gp0, occ_l, occ_g;
+      gp_f32_batch_get_grids(b->f32, &lp0, &gp0, &occ_l, &occ_g);
       if (c && occ_l < 2) continue;
       const int lp = c ? occ_l - 1 : 0;
       gp_f32_batch_set_step_threads(b->f32, th);
       gp_f32_batch_set_grids(b->f32, lp, 0);
       gp_f32_batch_set_scan(b->f32, sc);
-      for (int w = 0; w < 3; w++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (w & 1), b->stream));
+      const int warm = dp == 2 ? 2 : 3, calls = 10 / dp;
+      for (int w = 0; w < warm; w++) GP_CUDA(batch_launch(b, b->parity ^ (w & 1)));
       GP_CUDA(cudaEventRecord(e0, b->stream));
-      for (int r = 0; r < 10; r++) GP_CUDA(gp_f32_batch_launch(b->f32, b->parity ^ (r & 1), b->stream));
+      for (int r = 0; r < calls; r++) GP_CUDA(batch_launch(b, b->parity ^ (r & 1)));
       GP_CUDA(cudaEventRecord(e1, b->stream));
       GP_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
       GP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      b->launches += 13 * gp_f32_batch_launches_per_step(b->f32);
+      b->launches += (int64_t)(warm + calls) * batch_launches(b);
       // a reduced lean grid must win by 3%: at equal speed the kernels keep their occupancy
       if (c ? ms < 0.97f * best : ms < best) {
         best = ms;
@@ -999,8 +1120,10 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
         best_lp = lp;
         best_th = th;
         best_sc = sc;
+        best_dp = dp;
       }
     }
+    gp_f32_batch_set_depth(b->f32, 1);
     gp_f32_batch_set_grids(b->f32, 0, 0);
     gp_f32_batch_set_step_threads(b->f32, 256);
     gp_f32_batch_set_scan(b->f32, 0);
@@ -1014,12 +1137,14 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   int rc = gp_batch_set_tile(b, best_tx, best_ty);
   if (rc == GP_OK) rc = gp_batch_set_block(b, best_th);
   if (rc == GP_OK) rc = gp_batch_set_scan(b, best_sc);
+  if (rc == GP_OK) rc = gp_batch_set_depth(b, best_dp);
   if (rc == GP_OK) rc = gp_batch_set_grids(b, best_lp, 0);
   if (rc != GP_OK) return rc;
   if (cache_path) {
     FILE* f = fopen(cache_path, "a");
     if (f) {
-      fprintf(f, "%s %d %d %d %d %d %.6f\n", key, best_tx, best_ty, best_lp, best_th, best_sc, best / 10.0f);
+      fprintf(f, "%s %d %d %d %d %d %d %.6f\n", key, best_tx, best_ty, best_lp, best_th, best_sc, best_dp,
+              best / 10.0f);
       fclose(f);
     }
   }
@@ -1032,6 +1157,8 @@ extern "C" int gp_batch_set_narrowband(gp_batch* b, int on) {
   if (!b) return GP_E_ARG;
   GP_CUDA(cudaStreamSynchronize(b->stream));
   gp_f32_batch_set_narrowband(b->f32, on);
+  b->narrowband_on = on ? 1 : 0;
+  if (!on) gp_f32_batch_set_depth(b->f32, 1);  // blocked pairs need the narrow band
   batch_drop_graphs(b);
   return GP_OK;
 }
@@ -1054,11 +1181,29 @@ extern "C" int gp_batch_set_scan(gp_batch* b, int on) {
   if (!b) return GP_E_ARG;
   GP_CUDA(cudaStreamSynchronize(b->stream));
   gp_f32_batch_set_scan(b->f32, on);
+  if (on) gp_f32_batch_set_depth(b->f32, 1);  // blocked pairs use the list
   batch_drop_graphs(b);
   return GP_OK;
 }
 
 extern "C" int gp_batch_get_scan(gp_batch* b) { return b ? gp_f32_batch_scan(b->f32) : 0; }
+
+extern "C" int gp_batch_set_depth(gp_batch* b, int depth) {
+  if (!b) return GP_E_ARG;
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  if (depth == 2 && (gp_f32_batch_scan(b->f32) || !b->narrowband_on)) {
+    gp_set_error("gp_batch_set_depth: two-step blocking needs the narrow band in list mode (scan off)");
+    return GP_E_ARG;
+  }
+  if (!gp_f32_batch_set_depth(b->f32, depth)) {
+    gp_set_error("gp_batch_set_depth: depth %d not available (1 or 2)", depth);
+    return GP_E_ARG;
+  }
+  batch_drop_graphs(b);
+  return GP_OK;
+}
+
+extern "C" int gp_batch_get_depth(gp_batch* b) { return b ? gp_f32_batch_depth(b->f32) : 0; }
 
 extern "C" int gp_batch_test_lose_box(gp_batch* b) {
   if (!b) return GP_E_ARG;

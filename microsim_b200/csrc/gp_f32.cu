@@ -296,8 +296,11 @@ __host__ __device__ __forceinline__ uint32_t pf_all(int c) { return (uint32_t)c 
 // index stride of the x-neighbours), which of the four neighbours exist, and
 // whether the tile is never lean (its two-cell ring leaves the grid where it
 // is not a trusted mirror: a periodic wrap, or fewer than 3 cells on that axis).
+// TG_REJECT2: the tile never takes the two-step lean update, because its two-cell
+// ring leaves the grid across a periodic boundary of phi or mu (the ring's purity
+// and the partner cells of the intermediate step are not known there).
 enum : uint32_t { TG_NY = 0xFFFFFFu, TG_XM = 1u << 24, TG_XP = 1u << 25, TG_YM = 1u << 26, TG_YP = 1u << 27,
-                  TG_REJECT = 1u << 28 };
+                  TG_REJECT = 1u << 28, TG_REJECT2 = 1u << 29 };
 
 inline uint32_t tile_geo(const Inst& I, int t, int TX, int TY) {
   const int ny = I.tiles_y, lt = t - I.tile_begin, tx = lt / ny, ty = lt % ny;
@@ -305,8 +308,12 @@ inline uint32_t tile_geo(const Inst& I, int t, int TX, int TY) {
   const bool xm = tx > 0, xp = tx + 1 < I.tiles_x, ym = ty > 0, yp = ty + 1 < ny;
   const bool reject = ((!xm || !xp) && !(I.bc.phi_x == GP_BC_NEUMANN && ex >= 3)) ||
                       ((!ym || !yp) && !(I.bc.phi_y == GP_BC_NEUMANN && ey >= 3));
+  const int x0 = tx * TX, y0 = ty * TY;
+  const bool cross_x = x0 - 2 < 0 || x0 + TX + 2 > I.mx, cross_y = y0 - 2 < 0 || y0 + TY + 2 > I.my;
+  const bool reject2 = (cross_x && (I.bc.phi_x != GP_BC_NEUMANN || I.bc.mu_x != GP_BC_NEUMANN)) ||
+                       (cross_y && (I.bc.phi_y != GP_BC_NEUMANN || I.bc.mu_y != GP_BC_NEUMANN));
   return (uint32_t)ny | (xm ? TG_XM : 0u) | (xp ? TG_XP : 0u) | (ym ? TG_YM : 0u) | (yp ? TG_YP : 0u) |
-         (reject ? TG_REJECT : 0u);
+         (reject ? TG_REJECT : 0u) | (reject2 ? TG_REJECT2 : 0u);
 }
 
 // Phase b >= 0 when tile t may take the lean update: in the input, the tile
@@ -355,7 +362,7 @@ template <int N, int K1, bool ANISO, int TX, int TY, int THREADS = 256>
 __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS : (K1 >= 3 || THREADS > 256 ? 1 : 2))
     k_step32(const Inst* __restrict__ insts, const Model* __restrict__ models, const int* __restrict__ tile_inst,
              const int2* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out, int total,
-             const int4* __restrict__ tile_desc, const uint32_t* __restrict__ flags_in) {
+             const int4* __restrict__ tile_desc, const uint32_t* __restrict__ flags_in, int keep_list) {
   using T = Tile<N, K1, ANISO, TX, TY>;
   constexpr int X2 = T::X2, Y2 = T::Y2, X1 = T::X1, Y1 = T::Y1, W = T::W, Q = T::Q;
   constexpr int L = N - 1;
@@ -1060,10 +1067,12 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
   if (glist && threadIdx.x == 0) {
     __threadfence();
     if (atomicAdd(&cnt[2], 1) == (int)gridDim.x - 1) {
-      cnt[0] = 0;
+      if (!keep_list) {  // keep_list: a second pass over the same list follows (two-step blocking)
+        cnt[0] = 0;
+        cnt[3] = 0;
+      }
       cnt[1] = 0;
       cnt[2] = 0;
-      cnt[3] = 0;
     }
   }
 }
@@ -1443,18 +1452,383 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
   }
 }
 
+// ---------------------------------------------------------------- two steps per staged box (depth 2)
+//
+// A cell's update is the pure-phase one (diffusion of mu in phase b, phi kept)
+// when phi is the one-hot field of b on the cell's 3x3 neighbourhood: its face
+// mobilities are those of b, its antitrapping currents vanish (zero gradients),
+// it takes the bulk branch and its divphi is zero.  So the pure region shrinks by
+// at most one cell per step, and a tile lean_phase accepts (phi one-hot b on the
+// tile and its two-cell ring) has its cells and its ring's first row/column pure
+// for two steps.  One box of mu -- rows x0-2 .. x0+TX+1, columns y0-4 .. y0+TY+3,
+// at step t -- then gives the tile at t+2: sub-step 1 computes rows x0-1 .. x0+TX
+// of step t+1 into a second shared array (over the box's columns; of those only
+// the tile's columns and the ring column beside them are used), sub-step 2 the
+// tile.  Each cell and face is evaluated by the same helper calls on the same
+// operands as in two single steps, so the results are the same bits.
+//
+// One tile per warp; a ring of two stages (one box loading while the other is
+// computed).  Lanes own a float4 column group and stream a segment of rows
+// along x, carrying the x-face flux from row to row.
+template <int N, int K1, int TX, int TY>
+struct Lean2 {
+  static constexpr int R2 = TX + 4;                        // box rows x0-2 .. x0+TX+1
+  static constexpr int R1 = TX + 2;                        // intermediate rows x0-1 .. x0+TX
+  static constexpr int W = TY + 8;                         // columns y0-4 .. y0+TY+3
+  static constexpr int Q1 = W / 4;                         // column groups of sub-step 1
+  static constexpr int Q2 = TY / 4;                        // column groups of sub-step 2 (the tile)
+  static constexpr int S1 = 32 / Q1 > 0 ? 32 / Q1 : 1;     // row segments of sub-step 1
+  static constexpr int RS1 = (R1 + S1 - 1) / S1;           // rows per segment
+  static constexpr int S2 = 32 / Q2;
+  static constexpr int RS2 = (TX + S2 - 1) / S2;
+  static constexpr int BYTES = K1 * R2 * W * 4;            // one box
+  static constexpr int SLOT = (BYTES + 127) / 128 * 128;
+  static constexpr int MID = (K1 * R1 * W * 4 + 127) / 128 * 128;
+  static constexpr int STAGES = 2;
+  static constexpr int WARPS = 4;
+  static constexpr int CTRL = 128;                         // barriers, ring entries
+  static constexpr int WARP_BYTES = CTRL + STAGES * SLOT + MID;
+  static constexpr size_t smem = (size_t)WARPS * WARP_BYTES + 128;
+  static_assert(Q1 <= 32 && Q2 * S2 <= 32 && S2 >= 1, "tile shape");
+  static_assert(W <= 256 && R2 <= 256 && W * 4 % 16 == 0, "TMA box");
+};
+
+// One lane's diffusion sweep over output rows [r0, r1) of a staged array with
+// R rows of W columns per plane: output row r comes from source rows r, r+1,
+// r+2 (the source starts one row earlier) at columns c0 .. c0+3, with the
+// y-neighbours c0-1 and c0+4 (clamped into the array: a cell whose neighbour
+// lies outside it is never used).  put(r, mnew) stores a row's four new cells.
+// The arithmetic is that of lean_compute, helper call for helper call.
+template <int K1, int R, int W, int RS, typename Put>
+__device__ __forceinline__ void lean_sweep(const float* __restrict__ src, int c0, int r0, int r1,
+                                           const float (&Db)[MK][MK], const float (&cm)[MK][MK],
+                                           const float (&be)[MK], const float (&aa)[MK][MK], float hx, float hy,
+                                           Put put) {
+  const int cl = c0 > 0 ? c0 - 1 : 0, cr = c0 + 4 < W ? c0 + 4 : W - 1;
+  auto row = [&](int r, float (&v)[4][K1]) {
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      const float4 q = *reinterpret_cast<const float4*>(src + (k * R + r) * W + c0);
+      v[0][k] = q.x;
+      v[1][k] = q.y;
+      v[2][k] = q.z;
+      v[3][k] = q.w;
+    }
+  };
+  float cur[4][K1], fxm[4][K1];
+  {
+    float prev[4][K1];
+    row(r0, prev);
+    row(r0 + 1, cur);
+#pragma unroll
+    for (int j = 0; j < 4; j++) diff_flux<K1>(Db, Db, prev[j], cur[j], hx, fxm[j]);
+  }
+#pragma unroll
+  for (int i = 0; i < RS; i++) {
+    const int r = r0 + i;
+    if (r >= r1) break;
+    float nx[4][K1], left[K1], right[K1], fy[5][K1], mnew[4][K1];
+    row(r + 2, nx);
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      left[k] = src[(k * R + r + 1) * W + cl];
+      right[k] = src[(k * R + r + 1) * W + cr];
+    }
+    diff_flux<K1>(Db, Db, left, cur[0], hy, fy[0]);
+#pragma unroll
+    for (int j = 0; j < 3; j++) diff_flux<K1>(Db, Db, cur[j], cur[j + 1], hy, fy[j + 1]);
+    diff_flux<K1>(Db, Db, cur[3], right, hy, fy[4]);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      float fxp[K1], dc[K1];
+      diff_flux<K1>(Db, Db, cur[j], nx[j], hx, fxp);
+#pragma unroll
+      for (int k = 0; k < K1; k++) {
+        dc[k] = flux_div(fxp[k], fxm[j][k], fy[j + 1][k], fy[j][k]);
+        fxm[j][k] = fxp[k];
+      }
+      bulk_update_v<K1>(cm, be, aa, cur[j], dc, mnew[j]);
+    }
+    put(r, mnew);
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int k = 0; k < K1; k++) cur[j][k] = nx[j][k];
+  }
+}
+
+// Cells of a staged mu array (rows gx0 .. gx0+R-1, columns gy0 .. gy0+W-1 of
+// instance I, K1 planes) on the grid's first ghost row or column (-1, M) get
+// their boundary-map source: from the array when the source lies in it, else
+// from `gmu` (the state the array holds; the periodic partner of a row or
+// column the array crosses).  Ghost rows over the grid's columns first, then
+// ghost columns over the grid's rows.  Called by the whole warp.
+template <int K1, int R, int W>
+__device__ __forceinline__ void lean2_ghosts(const Inst& I, int gx0, int gy0, float* buf, const float* gmu,
+                                             int lane) {
+  const int mx = I.mx, my = I.my;
+  const int ylo = max(0, gy0), yhi = min(my, gy0 + W), xlo = max(0, gx0), xhi = min(mx, gx0 + R);
+  for (int side = 0; side < 2; side++) {
+    const int gx = side ? mx : -1, dr = gx - gx0;
+    if (dr < 0 || dr >= R) continue;
+    const int src = gp_map(gx, mx, I.bc.mu_x), sr = src - gx0;
+    const bool in_buf = sr >= 0 && sr < R;
+    if (!in_buf && !gmu) continue;
+    for (int gy = ylo + lane; gy < yhi; gy += 32)
+#pragma unroll
+      for (int k = 0; k < K1; k++)
+        buf[(k * R + dr) * W + (gy - gy0)] =
+            in_buf ? buf[(k * R + sr) * W + (gy - gy0)] : gmu[k * I.plane + (int64_t)src * I.pitch + gy];
+  }
+  __syncwarp();
+  for (int side = 0; side < 2; side++) {
+    const int gy = side ? my : -1, dc = gy - gy0;
+    if (dc < 0 || dc >= W) continue;
+    const int src = gp_map(gy, my, I.bc.mu_y), sc = src - gy0;
+    const bool in_buf = sc >= 0 && sc < W;
+    if (!in_buf && !gmu) continue;
+    for (int gx = xlo + lane; gx < xhi; gx += 32)
+#pragma unroll
+      for (int k = 0; k < K1; k++)
+        buf[(k * R + (gx - gx0)) * W + dc] =
+            in_buf ? buf[(k * R + (gx - gx0)) * W + sc] : gmu[k * I.plane + (int64_t)gx * I.pitch + src];
+  }
+  __syncwarp();
+}
+
+// Some existing neighbour of tile t is listed for the full kernel (gen[] from k_general_list).
+__device__ __forceinline__ bool next_to_full(const uint8_t* __restrict__ gen, uint32_t geo, int t) {
+  const int ny = (int)(geo & TG_NY);
+  const bool xm = geo & TG_XM, xp = geo & TG_XP, ym = geo & TG_YM, yp = geo & TG_YP;
+  bool f = false;
+  f |= xm && gen[t - ny];
+  f |= xp && gen[t + ny];
+  f |= ym && gen[t - 1];
+  f |= yp && gen[t + 1];
+  f |= xm && ym && gen[t - ny - 1];
+  f |= xm && yp && gen[t - ny + 1];
+  f |= xp && ym && gen[t + ny - 1];
+  f |= xp && yp && gen[t + ny + 1];
+  return f;
+}
+
+// Two steps of the lean tiles of a blocked pair.  adj_mode 1: only the lean tiles
+// next to a tile of the full kernel's list, which also store their step-t+1
+// state (mu, and phi unless the buffer holds it) into the intermediate buffer X
+// (insts_x[i].phi_out / mu_out, purity words flags_x) for the full kernel's
+// second pass; adj_mode 0: the other lean tiles.  Bounded waits as k_lean32.
+template <int N, int K1, int TX, int TY>
+__global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
+    k_lean2(const Inst* __restrict__ insts, const Inst* __restrict__ insts_x, const LeanConst* __restrict__ lconst,
+            const CUtensorMap* __restrict__ tmaps, const int4* __restrict__ tile_desc,
+            const uint32_t* __restrict__ flags_in, uint32_t* __restrict__ flags_out, uint32_t* __restrict__ flags_x,
+            const uint8_t* __restrict__ gen, int total, int reverse, int adj_mode, int* __restrict__ err) {
+  using S = Lean2<N, K1, TX, TY>;
+  constexpr int R1 = S::R1, R2 = S::R2, W = S::W, STAGES = S::STAGES;
+  extern __shared__ __align__(16) unsigned char lsm_raw[];
+  unsigned char* lsm = lsm_raw + ((128 - (smem_u32(lsm_raw) & 127)) & 127);
+  const int lane = threadIdx.x & 31;
+  unsigned char* wsm = lsm + (threadIdx.x >> 5) * S::WARP_BYTES;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(wsm);                    // [STAGES]
+  int4* ent = reinterpret_cast<int4*>(wsm + 64);                       // [STAGES] {tile, inst * 8 + phase, x0, y0}
+  float* slots = reinterpret_cast<float*>(wsm + S::CTRL);              // [STAGES][SLOT / 4]
+  float* mid = reinterpret_cast<float*>(wsm + S::CTRL + STAGES * S::SLOT);  // [K1][R1][W]
+  const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) - 32 * nwarp;
+  unsigned todo = 0;
+  int mine = -1, mx0 = 0, my0 = 0;
+  if (lane == 0) {
+    for (int s = 0; s < STAGES; s++) mbar_init(&bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncwarp();
+  auto next = [&]() -> int4 {
+    while (!todo) {
+      base += 32 * nwarp;
+      if (base >= total) return make_int4(-1, 0, 0, 0);
+      int64_t tc = base + lane * nwarp;
+      if (reverse) tc = total - 1 - tc;
+      mine = -1;
+      if (tc >= 0 && tc < total) {
+        const int4 d = tile_desc[tc];
+        const uint32_t geo = (uint32_t)d.w;
+        const int bc = (geo & TG_REJECT2) ? -1 : lean_phase(flags_in, geo, (int)tc);
+        if (bc >= 0 && next_to_full(gen, geo, (int)tc) == (adj_mode != 0)) {
+          mine = d.x * 8 + bc;
+          mx0 = d.y;
+          my0 = d.z;
+        }
+      }
+      todo = __ballot_sync(0xffffffffu, mine >= 0);
+    }
+    const int src = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const int t = (int)(base + src * nwarp);
+    return make_int4(reverse ? total - 1 - t : t, __shfl_sync(0xffffffffu, mine, src),
+                     __shfl_sync(0xffffffffu, mx0, src), __shfl_sync(0xffffffffu, my0, src));
+  };
+  auto fill = [&](int s) {
+    const int4 e = next();
+    if (lane == 0) {
+      ent[s] = e;
+      if (e.x >= 0) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(&bar[s], S::BYTES);
+        tma_load_3d(slots + s * (S::SLOT / 4), &tmaps[e.y >> 3], &bar[s], e.w - 4, e.z - 2, 0);
+      }
+    }
+  };
+  for (int s = 0; s < STAGES - 1; s++) fill(s);
+  __syncwarp();
+  uint32_t phase = 0;
+  for (int s = 0;; s = s + 1 == STAGES ? 0 : s + 1) {
+    const int4 e = ent[s];
+    if (e.x < 0) break;
+    fill(s == 0 ? STAGES - 1 : s - 1);
+    const int inst = e.y >> 3, b = e.y & 7, x0 = e.z, y0 = e.w;
+    const Inst I = insts[inst];
+    const LeanConst C = lconst[inst * N + b];
+    const bool write_phi = pf(flags_out[e.x], PF_CORE) != 1 + b;
+    const bool write_phi_x = adj_mode && pf(flags_x[e.x], PF_CORE) != 1 + b;
+    if (!mbar_wait(&bar[s], (phase >> s) & 1)) {
+      if (lane == 0) atomicExch(err, 1);
+      __syncwarp();
+      for (int j = 0; j < STAGES; j++)
+        if (ent[j].x >= 0) mbar_wait(&bar[j], (phase >> j) & 1);
+      return;
+    }
+    phase ^= 1u << s;
+    float* box = slots + s * (S::SLOT / 4);
+    const int mx = I.mx, my = I.my;
+    const int ex = min(TX, mx - x0), ey = min(TY, my - y0);
+    // the box's cells on the grid's first ghost row/column: boundary map of step t
+    if (x0 - 2 < 0 || x0 + TX + 2 > mx || y0 - 4 < 0 || y0 + TY + 4 > my)
+      lean2_ghosts<K1, R2, W>(I, x0 - 2, y0 - 4, box, I.mu, lane);
+    float Db[MK][MK], cm[MK][MK], be[MK], aa[MK][MK];
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      be[k] = C.be[k];
+#pragma unroll
+      for (int l = 0; l < K1; l++) {
+        Db[k][l] = C.Db[k][l];
+        cm[k][l] = C.cm[k][l];
+        aa[k][l] = C.aa[k][l];
+      }
+    }
+    // sub-step 1: rows x0-1 .. x0+TX of step t+1 into mid
+    {
+      const int g = lane % S::Q1, seg = lane / S::Q1;
+      if (seg < S::S1) {
+        const int r0 = seg * S::RS1, r1 = min(R1, r0 + S::RS1);
+        lean_sweep<K1, R2, W, S::RS1>(box, 4 * g, r0, r1, Db, cm, be, aa, C.hx, C.hy,
+                                      [&](int r, const float (&v)[4][K1]) {
+#pragma unroll
+                                        for (int k = 0; k < K1; k++)
+                                          *reinterpret_cast<float4*>(mid + (k * R1 + r) * W + 4 * g) =
+                                              make_float4(v[0][k], v[1][k], v[2][k], v[3][k]);
+                                      });
+      }
+    }
+    __syncwarp();
+    // step t+1 ghosts of a tile at the grid edge (Neumann: sources inside mid)
+    if (x0 == 0 || x0 + ex == mx || y0 == 0 || y0 + ey == my)
+      lean2_ghosts<K1, R1, W>(I, x0 - 1, y0 - 4, mid, nullptr, lane);
+    if (adj_mode) {  // the tile at step t+1 into X for the full kernel's second pass
+      const Inst& X = insts_x[inst];
+      for (int e2 = lane; e2 < ex * S::Q2; e2 += 32) {
+        const int r = e2 / S::Q2, g = e2 % S::Q2, yb = y0 + 4 * g;
+        if (yb >= my) continue;
+        const int64_t o = (int64_t)(x0 + r) * X.pitch + yb;
+#pragma unroll
+        for (int k = 0; k < K1; k++) {
+          const float* v = mid + (k * R1 + r + 1) * W + 4 + 4 * g;
+          if (yb + 3 < my) {
+            *reinterpret_cast<float4*>(X.mu_out + o + k * X.plane) = *reinterpret_cast<const float4*>(v);
+          } else {
+            for (int j = 0; j < 4 && yb + j < my; j++) X.mu_out[o + k * X.plane + j] = v[j];
+          }
+        }
+        if (write_phi_x)
+#pragma unroll
+          for (int a = 0; a < N; a++) {
+            const float pv = a == b ? 1.f : 0.f;
+            if (yb + 3 < my) *reinterpret_cast<float4*>(X.phi_out + o + a * X.plane) = make_float4(pv, pv, pv, pv);
+            else
+              for (int j = 0; j < 4 && yb + j < my; j++) X.phi_out[o + a * X.plane + j] = pv;
+          }
+      }
+    }
+    __syncwarp();
+    // sub-step 2: the tile at step t+2
+    {
+      const int g = lane % S::Q2, seg = lane / S::Q2;
+      const int yb = y0 + 4 * g;
+      const bool full = x0 + TX <= mx && y0 + TY <= my;
+      float* const out = I.mu_out + (int64_t)x0 * I.pitch + yb;
+      if (seg < S::S2) {
+        const int r0 = seg * S::RS2, r1 = min(TX, r0 + S::RS2);
+        lean_sweep<K1, R1, W, S::RS2>(mid, 4 + 4 * g, r0, r1, Db, cm, be, aa, C.hx, C.hy,
+                                      [&](int r, const float (&v)[4][K1]) {
+                                        if (full) {
+#pragma unroll
+                                          for (int k = 0; k < K1; k++)
+                                            __stwb(reinterpret_cast<float4*>(out + r * I.pitch + k * I.plane),
+                                                   make_float4(v[0][k], v[1][k], v[2][k], v[3][k]));
+                                        } else if (x0 + r < mx && yb < my) {
+                                          if (yb + 3 < my) {
+#pragma unroll
+                                            for (int k = 0; k < K1; k++)
+                                              __stwb(reinterpret_cast<float4*>(out + r * I.pitch + k * I.plane),
+                                                     make_float4(v[0][k], v[1][k], v[2][k], v[3][k]));
+                                          } else {
+#pragma unroll
+                                            for (int j = 0; j < 4; j++)
+                                              if (yb + j < my)
+#pragma unroll
+                                                for (int k = 0; k < K1; k++)
+                                                  out[r * I.pitch + k * I.plane + j] = v[j][k];
+                                          }
+                                        }
+                                      });
+        if (write_phi) {
+          float* const po = I.phi_out + (int64_t)x0 * I.pitch + yb;
+          for (int r = r0; r < r1 && x0 + r < mx; r++)
+#pragma unroll
+            for (int a = 0; a < N; a++) {
+              const float v = a == b ? 1.f : 0.f;
+              if (yb + 3 < my) {
+                *reinterpret_cast<float4*>(po + r * I.pitch + a * I.plane) = make_float4(v, v, v, v);
+              } else {
+                for (int j = 0; j < 4 && yb + j < my; j++) po[r * I.pitch + a * I.plane + j] = v;
+              }
+            }
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      flags_out[e.x] = pf_all(1 + b);
+      if (adj_mode) flags_x[e.x] = pf_all(1 + b);
+    }
+  }
+}
+
 // The tiles of one step that lean_phase rejects, listed for the full kernel:
 // tiles whose own cells are not all one pure phase from glist[0] up (count in
 // cnt[0]), the others (an interface only in their ring) from glist[total - 1]
-// down (count in cnt[3]).
+// down (count in cnt[3]).  For a two-step blocked pair (depth 2) the tiles
+// marked TG_REJECT2 are listed too, and gen[t] records which tiles are listed.
 template <int TX, int TY>
 __global__ void __launch_bounds__(256) k_general_list(const int4* __restrict__ tile_desc,
                                                       const uint32_t* __restrict__ flags_in, int total,
-                                                      int2* __restrict__ glist, int* __restrict__ cnt) {
+                                                      int2* __restrict__ glist, int* __restrict__ cnt,
+                                                      uint8_t* __restrict__ genb, int depth) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   int4 d = make_int4(0, 0, 0, 0);
   if (t < total) d = tile_desc[t];
-  const bool gen = t < total && lean_phase(flags_in, (uint32_t)d.w, t) < 0;
+  const bool gen = t < total && (lean_phase(flags_in, (uint32_t)d.w, t) < 0 ||
+                                 (depth > 1 && ((uint32_t)d.w & TG_REJECT2)));
+  if (genb && t < total) genb[t] = gen ? 1 : 0;
   const bool ring = gen && pf(flags_in[t], PF_CORE) != 0;  // pure inside
   const unsigned bal = __ballot_sync(0xffffffffu, gen && !ring), balr = __ballot_sync(0xffffffffu, ring);
   const int lane = threadIdx.x & 31;
@@ -1529,13 +1903,15 @@ using namespace gp32;
 // Kernels of one (N, K1, anisotropy, tile shape).
 struct KernelSet {
   void (*general)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*, int, const int4*,
-                  const uint32_t*);
+                  const uint32_t*, int);
   void (*general_wide)(const Inst*, const Model*, const int*, const int2*, int*, uint32_t*, int, const int4*,
-                       const uint32_t*);  // 512 threads
+                       const uint32_t*, int);  // 512 threads
   void (*lean)(const Inst*, const LeanConst*, const CUtensorMap*, const int4*, const uint32_t*, uint32_t*, int, int,
                int, int*);
-  void (*list)(const int4*, const uint32_t*, int, int2*, int*);
-  size_t smem_general, smem_lean;
+  void (*lean2)(const Inst*, const Inst*, const LeanConst*, const CUtensorMap*, const int4*, const uint32_t*,
+                uint32_t*, uint32_t*, const uint8_t*, int, int, int, int*);
+  void (*list)(const int4*, const uint32_t*, int, int2*, int*, uint8_t*, int);
+  size_t smem_general, smem_lean, smem_lean2;
 };
 
 template <int N, int K1, bool AN, int TX, int TY>
@@ -1545,9 +1921,11 @@ static KernelSet make_set() {
   k.general_wide = nullptr;
   if constexpr (N == 2 && K1 == 1) k.general_wide = k_step32<N, K1, AN, TX, TY, 512>;
   k.lean = k_lean32<N, K1, TX, TY>;
+  k.lean2 = k_lean2<N, K1, TX, TY>;
   k.list = k_general_list<TX, TY>;
   k.smem_general = Tile<N, K1, AN, TX, TY>::bytes;
   k.smem_lean = Lean<N, K1, TX, TY>::smem;
+  k.smem_lean2 = Lean2<N, K1, TX, TY>::smem;
   return k;
 }
 
@@ -1589,6 +1967,15 @@ struct gp_f32_batch {
   int n = 0, N = 0, K1 = 0, aniso = 0;
   int tx = 16, ty = 32;  // tile shape (autotuned)
   int narrowband = 1;    // send the tiles lean_phase accepts to the lean kernel
+  int depth = 1;         // steps per blocked launch: 1, or 2 (lean tiles two steps per box; needs X)
+  int has_x = 0;         // intermediate buffers X bound (gp_f32_batch_bind_x)
+  std::vector<Inst> hinst_x1[2], hinst_x2[2];  // [parity] buffer p -> X, X -> buffer p^1
+  Inst* dinst_x1[2] = {nullptr, nullptr};
+  Inst* dinst_x2[2] = {nullptr, nullptr};
+  CUtensorMap* dtmap2[2] = {nullptr, nullptr};  // [parity][n] mu boxes of the two-step lean kernel
+  uint8_t* dgen = nullptr;                      // [total_tiles] tile listed for the full kernel (blocked pairs)
+  cudaEvent_t ev_list = nullptr, ev_adj = nullptr;
+  int grid_lean2 = 0, occ_lean2 = 0;
   int lose_box = 0;      // failure-detection test: the next lean launch loses one stage's boxes
   std::vector<gp_model> gm;
   std::vector<Inst> hinst[2];  // [buffer parity]
@@ -1599,7 +1986,7 @@ struct gp_f32_batch {
   int* derr = nullptr;                          // lean kernel: a staged box did not arrive
   int total_tiles = 0;
   KernelSet ks;
-  uint32_t* dflags = nullptr;  // [2][total_tiles] purity words of the state in buffer p
+  uint32_t* dflags = nullptr;  // [3][total_tiles] purity words of buffer 0, buffer 1 and X
   int* dtile_inst = nullptr;   // [total_tiles] instance of each tile
   int4* dtile_desc = nullptr;  // [total_tiles] {instance, x0, y0, tile_geo}
   std::vector<int4> htile_desc;
@@ -1617,9 +2004,11 @@ struct gp_f32_batch {
   // per-kernel timing (off by default): a ring of event sets, one per step
   static constexpr int kTimingSlots = 64;
   int timing = 0, tn = 0, tdone = 0;
-  std::vector<cudaEvent_t> tev;  // [kTimingSlots][5]: lean start/end, list start, general start/end
+  std::vector<cudaEvent_t> tev;  // [kTimingSlots][kEv]: lean start/end, list start/end, general start/end
+  static constexpr int kEv = 6;
   double tms[3] = {0, 0, 0};     // accumulated lean, list, general milliseconds
   int64_t tsteps = 0;
+  int tslot_steps[kTimingSlots] = {};  // steps of each slot (negative: narrow band off, no lean/list events)
 };
 
 void gp_f32_batch_destroy(gp_f32_batch* b);
@@ -1629,10 +2018,12 @@ static void free_tiles(gp_f32_batch* b) {
   cudaFree(b->dtile_inst);
   cudaFree(b->dtile_desc);
   cudaFree(b->dglist);
+  cudaFree(b->dgen);
   b->dflags = nullptr;
   b->dtile_inst = nullptr;
   b->dtile_desc = nullptr;
   b->dglist = nullptr;
+  b->dgen = nullptr;
 }
 
 cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** out) {
@@ -1678,10 +2069,17 @@ cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** ou
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_list, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_adj, cudaEventDisableTiming);
   for (int p = 0; e == cudaSuccess && p < 2; p++) {
     b->hinst[p].resize(n);
+    b->hinst_x1[p].resize(n);
+    b->hinst_x2[p].resize(n);
     e = cudaMalloc(&b->dinst[p], sizeof(Inst) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&b->dinst_x1[p], sizeof(Inst) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&b->dinst_x2[p], sizeof(Inst) * n);
     if (e == cudaSuccess) e = cudaMalloc(&b->dtmap[p], sizeof(CUtensorMap) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&b->dtmap2[p], sizeof(CUtensorMap) * n);
   }
   if (e != cudaSuccess) {
     gp_f32_batch_destroy(b);
@@ -1695,10 +2093,13 @@ void gp_f32_batch_destroy(gp_f32_batch* b) {
   if (!b) return;
   if (b->side) cudaStreamSynchronize(b->side);
   cudaFree(b->dmodel);
-  cudaFree(b->dinst[0]);
-  cudaFree(b->dinst[1]);
-  cudaFree(b->dtmap[0]);
-  cudaFree(b->dtmap[1]);
+  for (int p = 0; p < 2; p++) {
+    cudaFree(b->dinst[p]);
+    cudaFree(b->dinst_x1[p]);
+    cudaFree(b->dinst_x2[p]);
+    cudaFree(b->dtmap[p]);
+    cudaFree(b->dtmap2[p]);
+  }
   cudaFree(b->dlconst);
   cudaFree(b->derr);
   free_tiles(b);
@@ -1706,6 +2107,8 @@ void gp_f32_batch_destroy(gp_f32_batch* b) {
   for (cudaEvent_t ev : b->tev) cudaEventDestroy(ev);
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->ev_join) cudaEventDestroy(b->ev_join);
+  if (b->ev_list) cudaEventDestroy(b->ev_list);
+  if (b->ev_adj) cudaEventDestroy(b->ev_adj);
   if (b->side) cudaStreamDestroy(b->side);
   delete b;
 }
@@ -1728,11 +2131,27 @@ void gp_f32_batch_bind(gp_f32_batch* b, int i, float* phiA, float* muA, float* p
   }
 }
 
+// Bind the intermediate buffers X of instance i (step t+1 of a blocked pair:
+// the full kernel's first pass writes it, its second pass reads it).
+void gp_f32_batch_bind_x(gp_f32_batch* b, int i, float* phiX, float* muX) {
+  for (int p = 0; p < 2; p++) {
+    Inst& A = b->hinst_x1[p][i];
+    A = b->hinst[p][i];
+    A.phi_out = phiX;
+    A.mu_out = muX;
+    Inst& B = b->hinst_x2[p][i];
+    B = b->hinst[p][i];
+    B.phi = phiX;
+    B.mu = muX;
+  }
+  b->has_x = 1;
+}
+
 // The purity flags describe the buffers' contents; after the state changes
 // behind the kernels' back (upload, restore) they are reset to "unknown".
 cudaError_t gp_f32_batch_invalidate(gp_f32_batch* b, cudaStream_t s) {
   if (!b->dflags) return cudaSuccess;
-  return cudaMemsetAsync(b->dflags, 0, 2 * sizeof(uint32_t) * (size_t)b->total_tiles, s);
+  return cudaMemsetAsync(b->dflags, 0, 3 * sizeof(uint32_t) * (size_t)b->total_tiles, s);
 }
 
 void gp_f32_batch_set_narrowband(gp_f32_batch* b, int on) { b->narrowband = on ? 1 : 0; }
@@ -1757,7 +2176,9 @@ static EncodeTiledFn encode_tiled() {
 // The lean kernel's mu box of every instance read at parity p: a 3-D tensor
 // (columns, rows, planes) over the instance's input mu, box (TY + 8) x (TX + 2)
 // x K1 starting at (y0 - 4, x0 - 1, 0); cells outside the grid read as zero.
-static cudaError_t encode_boxes(gp_f32_batch* b, int p) {
+// halo = 1: the single-step lean kernel's box (TX + 2 rows); halo = 2: the
+// two-step one's (TX + 4 rows from x0 - 2).
+static cudaError_t encode_boxes(gp_f32_batch* b, int p, int halo = 1) {
   EncodeTiledFn enc = encode_tiled();
   if (!enc) return cudaErrorNotSupported;
   std::vector<CUtensorMap> maps(b->n);
@@ -1765,22 +2186,25 @@ static cudaError_t encode_boxes(gp_f32_batch* b, int p) {
     const Inst& I = b->hinst[p][i];
     const cuuint64_t dim[3] = {(cuuint64_t)I.my, (cuuint64_t)I.mx, (cuuint64_t)b->K1};
     const cuuint64_t stride[2] = {(cuuint64_t)I.pitch * 4, (cuuint64_t)I.plane * 4};
-    const cuuint32_t box[3] = {(cuuint32_t)b->ty + 8, (cuuint32_t)b->tx + 2, (cuuint32_t)b->K1};
+    const cuuint32_t box[3] = {(cuuint32_t)b->ty + 8, (cuuint32_t)b->tx + 2 * halo, (cuuint32_t)b->K1};
     const cuuint32_t estride[3] = {1, 1, 1};
     if (enc(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)I.mu, dim, stride, box, estride,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return cudaErrorInvalidValue;
   }
-  return cudaMemcpy(b->dtmap[p], maps.data(), sizeof(CUtensorMap) * b->n, cudaMemcpyHostToDevice);
+  return cudaMemcpy(halo == 2 ? b->dtmap2[p] : b->dtmap[p], maps.data(), sizeof(CUtensorMap) * b->n,
+                    cudaMemcpyHostToDevice);
 }
 
 // Persistent grid sizes: blocks per SM as set (clamped to the occupancy), else the occupancy.
 // Fewer lean blocks than fit leave room on every SM for full-kernel blocks to run beside them.
 static void set_grids(gp_f32_batch* b) {
   const int l = b->lean_per_sm > 0 && b->lean_per_sm < b->occ_lean ? b->lean_per_sm : b->occ_lean;
+  const int l2 = b->lean_per_sm > 0 && b->lean_per_sm < b->occ_lean2 ? b->lean_per_sm : b->occ_lean2;
   const int g = b->general_per_sm > 0 && b->general_per_sm < b->occ_general ? b->general_per_sm : b->occ_general;
   b->grid_lean = b->sms * l;
+  b->grid_lean2 = b->sms * l2;
   b->grid_general = b->sms * g;
 }
 
@@ -1808,11 +2232,21 @@ bool gp_f32_batch_has_wide_step(const gp_f32_batch* b) { return b->ks.general_wi
 
 void gp_f32_batch_get_grids(const gp_f32_batch* b, int* lean_per_sm, int* general_per_sm, int* occ_lean,
                             int* occ_general) {
-  *lean_per_sm = b->sms ? b->grid_lean / b->sms : 0;
+  const bool two = b->depth == 2;
+  *lean_per_sm = b->sms ? (two ? b->grid_lean2 : b->grid_lean) / b->sms : 0;
   *general_per_sm = b->sms ? b->grid_general / b->sms : 0;
-  *occ_lean = b->occ_lean;
+  *occ_lean = two ? b->occ_lean2 : b->occ_lean;
   *occ_general = b->occ_general;
 }
+
+// Steps per blocked launch: 1, or 2 (needs the intermediate buffers X and the
+// list way of finding the interface tiles).  False if unavailable.
+bool gp_f32_batch_set_depth(gp_f32_batch* b, int depth) {
+  if (depth != 1 && !(depth == 2 && b->has_x)) return false;
+  b->depth = depth;
+  return true;
+}
+int gp_f32_batch_depth(const gp_f32_batch* b) { return b->depth; }
 
 // Recompute the tile decomposition for shape (tx, ty) and upload the instance tables.
 cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
@@ -1838,13 +2272,27 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   }
   b->total_tiles = t;
   for (int p = 0; p < 2; p++) {
+    for (int i = 0; i < b->n; i++) {  // the X tables carry the tile decomposition too
+      for (Inst* x : {&b->hinst_x1[p][i], &b->hinst_x2[p][i]}) {
+        x->tiles_x = b->hinst[p][i].tiles_x;
+        x->tiles_y = b->hinst[p][i].tiles_y;
+        x->tile_begin = b->hinst[p][i].tile_begin;
+      }
+    }
     cudaError_t e = cudaMemcpy(b->dinst[p], b->hinst[p].data(), sizeof(Inst) * b->n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && b->has_x)
+      e = cudaMemcpy(b->dinst_x1[p], b->hinst_x1[p].data(), sizeof(Inst) * b->n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && b->has_x)
+      e = cudaMemcpy(b->dinst_x2[p], b->hinst_x2[p].data(), sizeof(Inst) * b->n, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = encode_boxes(b, p);
+    if (e == cudaSuccess) e = encode_boxes(b, p, 2);
     if (e != cudaSuccess) return e;
   }
   free_tiles(b);
-  cudaError_t e = cudaMalloc(&b->dflags, 2 * sizeof(uint32_t) * (size_t)t);
-  if (e == cudaSuccess) e = cudaMemset(b->dflags, 0, 2 * sizeof(uint32_t) * (size_t)t);
+  cudaError_t e = cudaMalloc(&b->dflags, 3 * sizeof(uint32_t) * (size_t)t);
+  if (e == cudaSuccess) e = cudaMemset(b->dflags, 0, 3 * sizeof(uint32_t) * (size_t)t);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dgen, (size_t)t);
+  if (e == cudaSuccess) e = cudaMemset(b->dgen, 0, (size_t)t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dtile_inst, sizeof(int) * t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dglist, sizeof(int2) * t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dtile_desc, sizeof(int4) * t);
@@ -1859,7 +2307,7 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // one shared-memory carve-out for the three kernels of a step: no L1/shared reconfiguration
   // between them, and lean and full blocks can share an SM
-  for (const void* f : {(const void*)ks.general, (const void*)ks.lean, (const void*)ks.list}) {
+  for (const void* f : {(const void*)ks.general, (const void*)ks.lean, (const void*)ks.lean2, (const void*)ks.list}) {
     e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
   }
@@ -1876,7 +2324,12 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   if (e == cudaSuccess) e = cudaFuncSetAttribute(ks.lean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_lean);
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, ks.lean, 32 * GP_LEAN_WARPS, ks.smem_lean);
+  int occ_l2 = 0;
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ks.lean2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_lean2);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l2, ks.lean2, 32 * 4, ks.smem_lean2);
   if (e != cudaSuccess) return e;
+  b->occ_lean2 = occ_l2 > 0 ? occ_l2 : 1;
   b->sms = sms;
   b->occ_general_by[0] = occ_g > 0 ? occ_g : 1;
   b->occ_general_by[1] = occ_w > 0 ? occ_w : 1;
@@ -1890,21 +2343,25 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
 int gp_f32_batch_tiles(const gp_f32_batch* b) { return b->total_tiles; }
 
 // Fold the event times of timing slot `slot` into the totals.
+// Slot layout: [0] lean start, [1] lean end, [2] list start, [3] list end,
+// [4] full start, [5] full end, [6] steps the slot covers (as an event count is
+// not an event, the step count of each slot is kept in tslot_steps).
 static cudaError_t timing_collect(gp_f32_batch* b, int slot) {
-  cudaEvent_t* E = &b->tev[5 * slot];
-  cudaError_t e = cudaEventSynchronize(E[4]);
+  cudaEvent_t* E = &b->tev[gp_f32_batch::kEv * slot];
+  cudaError_t e = cudaEventSynchronize(E[5]);
   if (e == cudaSuccess) e = cudaEventSynchronize(E[1]);
   if (e != cudaSuccess) return e;
   float lean = 0.f, list = 0.f, gen = 0.f;
-  if (b->narrowband) {
+  const int st = b->tslot_steps[slot];
+  if (st > 0) {  // narrow band on
     cudaEventElapsedTime(&lean, E[0], E[1]);
     cudaEventElapsedTime(&list, E[2], E[3]);
   }
-  cudaEventElapsedTime(&gen, E[3], E[4]);
+  cudaEventElapsedTime(&gen, E[4], E[5]);
   b->tms[0] += lean;
   b->tms[1] += list;
   b->tms[2] += gen;
-  b->tsteps++;
+  b->tsteps += st > 0 ? st : -st;
   return cudaSuccess;
 }
 
@@ -1913,7 +2370,7 @@ cudaError_t gp_f32_batch_set_timing(gp_f32_batch* b, int on) {
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return e;
   if (on && b->tev.empty()) {
-    b->tev.resize(5 * gp_f32_batch::kTimingSlots);
+    b->tev.resize(gp_f32_batch::kEv * gp_f32_batch::kTimingSlots);
     for (cudaEvent_t& ev : b->tev)
       if ((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
   }
@@ -1936,6 +2393,21 @@ cudaError_t gp_f32_batch_kernel_ms(gp_f32_batch* b, double* ms, int64_t* steps) 
   return cudaSuccess;
 }
 
+// The timing slot of the next launch (nullptr when timing is off).
+static cudaError_t timing_slot(gp_f32_batch* b, int steps, cudaEvent_t** E) {
+  *E = nullptr;
+  if (!b->timing) return cudaSuccess;
+  if (b->tn - b->tdone == gp_f32_batch::kTimingSlots) {  // ring full: fold the oldest slot first
+    cudaError_t e = timing_collect(b, b->tdone % gp_f32_batch::kTimingSlots);
+    if (e != cudaSuccess) return e;
+    b->tdone++;
+  }
+  const int slot = b->tn++ % gp_f32_batch::kTimingSlots;
+  b->tslot_steps[slot] = steps;
+  *E = &b->tev[gp_f32_batch::kEv * slot];
+  return cudaSuccess;
+}
+
 // One step of every instance, reading buffer parity `parity`.
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   const KernelSet& k = b->ks;
@@ -1944,21 +2416,15 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   uint32_t* flags_out = b->dflags + (size_t)(p ^ 1) * b->total_tiles;
   cudaEvent_t* E = nullptr;
   cudaError_t e;
-  if (b->timing) {
-    if (b->tn - b->tdone == gp_f32_batch::kTimingSlots) {  // ring full: fold the oldest slot first
-      if ((e = timing_collect(b, b->tdone % gp_f32_batch::kTimingSlots)) != cudaSuccess) return e;
-      b->tdone++;
-    }
-    E = &b->tev[5 * (b->tn++ % gp_f32_batch::kTimingSlots)];
-  }
+  if ((e = timing_slot(b, b->narrowband ? 1 : -1, &E)) != cudaSuccess) return e;
   if (!b->narrowband) {
     b->lose_box = 0;  // no lean kernel, no staged boxes to lose
-    if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
+    if (E && ((e = cudaEventRecord(E[4], s)) != cudaSuccess)) return e;
     (b->step_threads == 512 ? k.general_wide : k.general)<<<b->total_tiles, b->step_threads, k.smem_general, s>>>(
-        b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr, flags_out, b->total_tiles, nullptr, nullptr);
+        b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr, flags_out, b->total_tiles, nullptr, nullptr, 0);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (E) {
-      if ((e = cudaEventRecord(E[4], s)) != cudaSuccess) return e;
+      if ((e = cudaEventRecord(E[5], s)) != cudaSuccess) return e;
       if ((e = cudaEventRecord(E[1], s)) != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -1981,15 +2447,68 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   if (E && ((e = cudaEventRecord(E[2], s)) != cudaSuccess)) return e;
   if (!b->scan) {
     k.list<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dtile_desc, flags_in, b->total_tiles, b->dglist,
-                                                        b->dcnt);
+                                                        b->dcnt, nullptr, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
+  if (E && ((e = cudaEventRecord(E[4], s)) != cudaSuccess)) return e;
   (b->step_threads == 512 ? k.general_wide : k.general)<<<b->grid_general, b->step_threads, k.smem_general, s>>>(
       b->dinst[p], b->dmodel, b->dtile_inst, b->scan ? nullptr : b->dglist, b->scan ? nullptr : b->dcnt, flags_out,
-      b->total_tiles, b->scan ? b->dtile_desc : nullptr, b->scan ? flags_in : nullptr);
+      b->total_tiles, b->scan ? b->dtile_desc : nullptr, b->scan ? flags_in : nullptr, 0);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if (E) return cudaEventRecord(E[4], s);
+  if (E) return cudaEventRecord(E[5], s);
+  if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess) return e;
+  return cudaStreamWaitEvent(s, b->ev_join, 0);
+}
+
+// Two steps of every instance (a blocked pair), reading buffer parity `parity`
+// and writing parity^1; X holds step t+1 of the tiles that need it.
+//   stream s:    list (tiles for the full kernel, gen bytes)  -> full pass 1 (buffer p -> X)
+//                -> [lean tiles next to the list done] -> full pass 2 (X -> buffer p^1)
+//   side stream: [list done] -> two-step lean kernel on the tiles next to the list (also writing
+//                their step t+1 into X) -> two-step lean kernel on the other lean tiles
+// Timed launches run one after the other on s.
+cudaError_t gp_f32_batch_launch_pair(gp_f32_batch* b, int parity, cudaStream_t s) {
+  if (b->depth != 2 || !b->narrowband || !b->has_x) return cudaErrorInvalidValue;
+  const KernelSet& k = b->ks;
+  const int p = parity & 1;
+  const size_t T = (size_t)b->total_tiles;
+  const uint32_t* flags_in = b->dflags + p * T;
+  uint32_t* flags_out = b->dflags + (p ^ 1) * T;
+  uint32_t* flags_x = b->dflags + 2 * T;
+  cudaEvent_t* E = nullptr;
+  cudaError_t e;
+  if ((e = timing_slot(b, 2, &E)) != cudaSuccess) return e;
+  b->lose_box = 0;
+  auto full = b->step_threads == 512 ? k.general_wide : k.general;
+  if (E && (e = cudaEventRecord(E[2], s)) != cudaSuccess) return e;
+  k.list<<<(b->total_tiles + 255) / 256, 256, 0, s>>>(b->dtile_desc, flags_in, b->total_tiles, b->dglist, b->dcnt,
+                                                      b->dgen, 2);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (E && (e = cudaEventRecord(E[3], s)) != cudaSuccess) return e;
+  cudaStream_t ls = E ? s : b->side;
+  if (!E) {
+    if ((e = cudaEventRecord(b->ev_list, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(b->side, b->ev_list, 0)) != cudaSuccess) return e;
+  }
+  if (E && (e = cudaEventRecord(E[0], ls)) != cudaSuccess) return e;
+  for (int adj = 1; adj >= 0; adj--) {
+    k.lean2<<<b->grid_lean2, 128, k.smem_lean2, ls>>>(b->dinst[p], b->dinst_x1[p], b->dlconst, b->dtmap2[p],
+                                                      b->dtile_desc, flags_in, flags_out, flags_x, b->dgen,
+                                                      b->total_tiles, p, adj, b->derr);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (adj && !E && (e = cudaEventRecord(b->ev_adj, ls)) != cudaSuccess) return e;
+  }
+  if (E && (e = cudaEventRecord(E[1], ls)) != cudaSuccess) return e;
+  if (E && (e = cudaEventRecord(E[4], s)) != cudaSuccess) return e;
+  full<<<b->grid_general, b->step_threads, k.smem_general, s>>>(b->dinst_x1[p], b->dmodel, b->dtile_inst, b->dglist,
+                                                                 b->dcnt, flags_x, b->total_tiles, nullptr, nullptr, 1);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (!E && (e = cudaStreamWaitEvent(s, b->ev_adj, 0)) != cudaSuccess) return e;
+  full<<<b->grid_general, b->step_threads, k.smem_general, s>>>(b->dinst_x2[p], b->dmodel, b->dtile_inst, b->dglist,
+                                                                 b->dcnt, flags_out, b->total_tiles, nullptr, nullptr, 0);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (E) return cudaEventRecord(E[5], s);
   if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess) return e;
   return cudaStreamWaitEvent(s, b->ev_join, 0);
 }
@@ -1997,7 +2516,8 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
 int gp_f32_batch_timing(const gp_f32_batch* b) { return b->timing; }
 
 // Tiles the next step (reading buffer parity `parity`) sends to the lean
-// kernel: lean_phase evaluated on the host over a copy of the purity words.
+// kernel: lean_phase evaluated on the host over a copy of the purity words
+// (with depth 2, the tiles the two-step lean kernel takes).
 cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s, int64_t* lean,
                                     int64_t* lean_cells) {
   std::vector<uint32_t> F(b->total_tiles);
@@ -2009,7 +2529,8 @@ cudaError_t gp_f32_batch_lean_tiles(gp_f32_batch* b, int parity, cudaStream_t s,
   for (int i = 0; i < b->n && b->narrowband; i++) {
     const Inst& I = b->hinst[parity & 1][i];
     for (int t = I.tile_begin; t < I.tile_begin + I.tiles_x * I.tiles_y; t++)
-      if (lean_phase(F.data(), (uint32_t)b->htile_desc[t].w, t) >= 0) {
+      if (lean_phase(F.data(), (uint32_t)b->htile_desc[t].w, t) >= 0 &&
+          !(b->depth == 2 && ((uint32_t)b->htile_desc[t].w & TG_REJECT2))) {
         const int lt = t - I.tile_begin, x0 = (lt / I.tiles_y) * b->tx, y0 = (lt % I.tiles_y) * b->ty;
         n++;
         c += (int64_t)(I.mx - x0 < b->tx ? I.mx - x0 : b->tx) * (I.my - y0 < b->ty ? I.my - y0 : b->ty);
@@ -2029,3 +2550,5 @@ const int* gp_f32_batch_error_word(const gp_f32_batch* b) { return b->derr; }
 
 // kernel launches one gp_f32_batch_launch issues
 int gp_f32_batch_launches_per_step(const gp_f32_batch* b) { return b->narrowband ? (b->scan ? 2 : 3) : 1; }
+// kernel launches one gp_f32_batch_launch_pair issues (two steps)
+int gp_f32_batch_launches_per_pair(const gp_f32_batch*) { return 5; }

@@ -241,3 +241,93 @@ def run_reference_harness(workdir: str, input_in: str, filling_in: str, nsteps: 
     if r.returncode != 0:
         raise RuntimeError("reference harness failed: %s" % r.stderr[-2000:])
     return r.stdout
+
+
+# ---------------------------------------------------------------------------
+# Energies of a state (numpy, FP64): the checker of gp_stats' energy sums
+# ---------------------------------------------------------------------------
+
+def _bc_index(M: int, kind: int) -> np.ndarray:
+    """Source interior index of every coordinate -1 .. M (the boundary copy of
+    solverloop/boundary_serial.h:176-203 as an index map: Neumann mirrors about the
+    first/last interior cell, the periodic copy has period M-1,
+    functions/utility_functions.h:471-653)."""
+    v = np.arange(-1, M + 1)
+    out = v.copy()
+    if kind == 1:
+        out[v < 0] = -v[v < 0]
+        out[v >= M] = 2 * M - 2 - v[v >= M]
+    else:
+        out[v < 0] = M - 1 + v[v < 0]
+        out[v >= M] = 1 + v[v >= M] - M
+    return out
+
+
+def energies(c: dict, phi: np.ndarray, mu: np.ndarray) -> dict:
+    """Integrated energies of interior fields phi[N, mx, my], mu[K1, mx, my].
+
+    c holds the model: N, K1, dx, dy, epsilon, obstacle, anisotropy, bc_phi (x, y
+    types), Gamma[N,N], Gamma_abc[N,N,N], dab[N,N], R[N,N,2,2], cmu[N,K1,K1],
+    A[N,K1,K1], Beff[N,K1] (Beq + dBbdT (T - Teq)), B[N,K1], C[N].  Per cell, with
+    cell-centred gradients (gradphi_c of solverloop/calculate_gradients.h:92-131):
+      gradient   eps sum_{a<b} Gamma_ab a_c(R_ab q_ab)^2 |q_ab|^2,
+                 q_ab = phi_a grad phi_b - phi_b grad phi_a
+                 (function_A_00.h:4-23 is its phi-derivative; a_c of anisotropy_01.h:30-48)
+      potential  (1/eps) [16/pi^2 sum_{a<b} Gamma_ab |phi_a phi_b|      (functionW_01.h:6-39)
+                          or 9 sum_{a<b} Gamma_ab phi_a^2 phi_b^2      (functionW_02.h:4-33)
+                          + sum_{a<b<c} Gamma_abc |phi_a phi_b phi_c|]
+      chemical   sum_a h_a f_a(c_a(mu))      (functionF_01.h:5-18 free_energy, :30-40 c_mu, functionH.h)
+      grand      gradient + potential + sum_a h_a (f_a - mu . c_a)   (the psi of functionF_01.h:41-57)
+    Each sum is multiplied by dx * dy."""
+    N, K1 = c["N"], c["K1"]
+    mx, my = phi.shape[1], phi.shape[2]
+    ix, iy = _bc_index(mx, c["bc_phi"][0]), _bc_index(my, c["bc_phi"][1])
+    P = phi[:, ix][:, :, iy]  # ghost ring of one cell
+    gx = (P[:, 2:, 1:-1] - P[:, :-2, 1:-1]) * (0.5 / c["dx"])
+    gy = (P[:, 1:-1, 2:] - P[:, 1:-1, :-2]) * (0.5 / c["dy"])
+    eg = np.zeros((mx, my))
+    w2 = np.zeros((mx, my))
+    w3 = np.zeros((mx, my))
+    for a in range(N):
+        for b in range(a + 1, N):
+            Qx = phi[a] * gx[b] - phi[b] * gx[a]
+            Qy = phi[a] * gy[b] - phi[b] * gy[a]
+            ac = np.ones((mx, my))
+            if c["anisotropy"]:
+                R = c["R"][a][b]
+                q0, q1 = R[0][0] * Qx + R[0][1] * Qy, R[1][0] * Qx + R[1][1] * Qy
+                q2 = q0 * q0 + q1 * q1
+                big = q2 > 1.0e-15
+                s4 = np.where(big, (q0 ** 4 + q1 ** 4) / np.where(big, q2 * q2, 1.0), 0.0)
+                ac = np.where(big, 1.0 - c["dab"][a][b] * (3.0 - 4.0 * s4), 1.0)
+            eg += c["Gamma"][a][b] * ac * ac * (Qx * Qx + Qy * Qy)
+            if c["obstacle"]:
+                w2 += c["Gamma"][a][b] * np.abs(phi[a] * phi[b])
+            else:
+                w2 += c["Gamma"][a][b] * phi[a] ** 2 * phi[b] ** 2
+            for d in range(b + 1, N):
+                w3 += c["Gamma_abc"][a][b][d] * np.abs(phi[a] * phi[b] * phi[d])
+    pot = (w2 * (16.0 / (np.pi * np.pi) if c["obstacle"] else 9.0) + w3) / c["epsilon"]
+    fch = np.zeros((mx, my))
+    psi = np.zeros((mx, my))
+    for a in range(N):
+        s1 = np.zeros((mx, my))
+        for b in range(N):
+            for d in range(b + 1, N):
+                if a not in (b, d):
+                    s1 += phi[b] * phi[d]
+        h = phi[a] ** 2 * (3.0 - 2.0 * phi[a]) + 2.0 * phi[a] * s1
+        conc = [sum(c["cmu"][a][k][l] * (mu[l] - c["Beff"][a][l]) for l in range(K1)) for k in range(K1)]
+        f = np.full((mx, my), float(c["C"][a]))
+        mc = np.zeros((mx, my))
+        for k in range(K1):
+            for l in range(k, K1):
+                f += c["A"][a][k][l] * conc[k] * conc[l]
+            f += c["B"][a][k] * conc[k]
+            mc += mu[k] * conc[k]
+        fch += h * f
+        psi += h * (f - mc)
+    da = c["dx"] * c["dy"]
+    grad = c["epsilon"] * eg
+    return {"energy_gradient": grad.sum() * da, "energy_potential": pot.sum() * da,
+            "energy_chemical": fch.sum() * da, "grand_potential": (grad + pot + psi).sum() * da}

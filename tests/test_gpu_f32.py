@@ -152,7 +152,7 @@ def test_autotune_restores_state_and_caches(tmp_path):
         after = b.download(0)
         assert (tx, ty) in [(16, 32), (8, 32), (32, 32), (16, 64)]
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
-        assert os.path.exists(cache) and len(open(cache).read().split()) == 11
+        assert os.path.exists(cache) and len(open(cache).read().split()) == 12
         assert b.autotune(cache) == (tx, ty)  # read back from the cache
 
 
@@ -226,6 +226,82 @@ def test_narrow_band_is_bit_identical_to_the_full_kernel():
     (a, la), (c, lc) = res
     assert la[0] > 0 and lc[0] == 0
     assert np.array_equal(a[0], c[0]) and np.array_equal(a[1], c[1])
+
+
+def test_two_step_blocking_is_bit_identical_to_single_steps():
+    """Blocked pairs (the lean tiles two diffusion steps per staged box, the other
+    tiles through the full kernel twice via the intermediate buffer) give the bits of
+    single steps, for every tile shape: Neumann borders (two-deep mirrored boxes and
+    the intermediate step's ghosts), a periodic member (its border tiles take the full
+    kernel), a periodic mu under Neumann phi, partial edge tiles (1- and 2-cell
+    remainders), odd step counts (a single step after the pairs), graph replays of
+    both parities, re-uploads, and a four-phase ternary case."""
+    cases = [configs.binary_case(200, 150, gap=1.0, supersat=0.55, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
+                                 seed=(0, 0, 8.0)),
+             configs.binary_case(160, 224, gap=1.0, supersat=0.4, eps=3.0, delta=0.03, theta=15.0, dt=0.05,
+                                 tau=1.3332, seed=(80, 100, 9.0), bc=(3, 3, 3, 3)),
+             configs.binary_case(98, 130, gap=1.0, supersat=0.5, eps=4.0, delta=0.01, dt=0.05, tau=1.7776,
+                                 seed=(49, 65, 7.0)),
+             configs.binary_case(129, 161, gap=1.0, supersat=0.5, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
+                                 seed=(128, 160, 10.0)),
+             configs.binary_case(145, 98, gap=1.0, supersat=0.45, eps=3.0, delta=0.015, dt=0.05, tau=1.3332,
+                                 seed=(70, 0, 9.0))]
+    loaded = [mb.load_case(c) for c in cases]
+    m4, p4, u4 = mb.load_case(cases[0])
+    m4 = m4.copy()
+    for i in range(4):
+        m4.bc_mu[i] = 3
+    loaded.append((m4, p4, u4))
+    models = [m for m, _, _ in loaded]
+
+    def run(depth, tile, reupload=False):
+        with mb.Batch(models) as b:
+            b.set_tile(*tile)
+            b.set_depth(depth)
+            assert b.depth() == depth
+            for i, (_, p, u) in enumerate(loaded):
+                b.upload(i, p, u)
+            b.step(150)  # 16-step graphs of both parities (9 replays), then pairs
+            if reupload:
+                for i, st in enumerate([b.download(i) for i in range(len(models))]):
+                    b.upload(i, *st)
+            b.step(151)  # odd: pairs and one single step
+            lean = b.lean_tiles()
+            return [b.download(i) for i in range(len(models))], lean
+
+    for tile in [(16, 32), (8, 32), (32, 32), (16, 64)]:
+        ref, _ = run(1, tile)
+        got, (lean, total) = run(2, tile, reupload=tile == (16, 32))
+        assert lean > total // 2, (tile, lean, total)
+        for i, ((p1, u1), (p0, u0)) in enumerate(zip(got, ref)):
+            assert np.array_equal(p1, p0) and np.array_equal(u1, u0), (tile, i, np.abs(u1 - u0).max())
+    m, phi, mu = mb.load_case(configs.c3(steps=200, mesh=160, nseeds=6, rng_seed=7))
+    res = []
+    for depth in (2, 1):
+        with mb.Batch([m]) as b:
+            b.set_depth(depth)
+            b.upload(0, phi, mu)
+            b.step(120)
+            res.append(b.download(0))
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+def test_two_step_blocking_timing_and_stats():
+    """Per-kernel timing of blocked pairs covers two steps per launch set, and the
+    statistics read after pairs see the blocked state."""
+    m, phi, mu = mb.load_case(configs.binary_case(256, 256, gap=1.0, supersat=0.5, eps=4.0, delta=0.02, dt=0.05,
+                                                  tau=1.7776, seed=(0, 0, 12.0)))
+    with mb.Batch([m, m]) as b:
+        b.set_depth(2)
+        for i in range(2):
+            b.upload(i, phi, mu)
+        b.set_timing(True)
+        b.step(10)
+        kt = b.kernel_ms()
+        b.set_timing(False)
+        assert kt["steps"] == 10 and kt["lean"] > 0 and kt["general"] > 0
+        st = b.stats(0)
+        assert st["nonfinite"] == 0 and st["rel_change_mu"][0] > 0
 
 
 def test_grid_split_and_prepared_graphs_are_bit_identical():
