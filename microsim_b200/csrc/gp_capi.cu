@@ -769,7 +769,7 @@ struct gp_batch {
   int parity = 0;     // which buffer holds the current state
   int have_prev = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  int graph_steps = 16;
+  int graph_steps = 4;  // steps per captured graph (two blocked pairs at depth 2)
   double* partials = nullptr;
   double* reduced = nullptr;
   double* stage = nullptr;  // device staging of FP64 host fields (kept between copies)
@@ -1103,15 +1103,20 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
       gp_f32_batch_set_step_threads(b->f32, th);
       gp_f32_batch_set_grids(b->f32, lp, 0);
       gp_f32_batch_set_scan(b->f32, sc);
-      const int warm = dp == 2 ? 2 : 3, calls = 10 / dp;
-      for (int w = 0; w < warm; w++) GP_CUDA(batch_launch(b, b->parity ^ (w & 1)));
+      // timed as the steps run: one replay of the step graph (graph_steps steps) to warm up, four timed
+      batch_drop_graphs(b);
+      int rc = batch_capture(b, b->parity);
+      if (rc != GP_OK) return rc;
+      GP_CUDA(cudaGraphLaunch(b->graph[b->parity], b->stream));
       GP_CUDA(cudaEventRecord(e0, b->stream));
-      for (int r = 0; r < calls; r++) GP_CUDA(batch_launch(b, b->parity ^ (r & 1)));
+      for (int r = 0; r < 4; r++) GP_CUDA(cudaGraphLaunch(b->graph[b->parity], b->stream));
       GP_CUDA(cudaEventRecord(e1, b->stream));
       GP_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
       GP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      b->launches += (int64_t)(warm + calls) * batch_launches(b);
+      ms *= 10.0f / (float)(4 * b->graph_steps);  // per 10 steps, as the cache records
+      b->launches += (int64_t)5 * (b->graph_steps / dp) * batch_launches(b);
+      batch_drop_graphs(b);
       // a reduced lean grid must win by 3%: at equal speed the kernels keep their occupancy
       if (c ? ms < 0.97f * best : ms < best) {
         best = ms;

@@ -54,6 +54,10 @@ struct alignas(16) Model {
   float C[MP];
   float DC[MP][MK][MK];  // sum_k Diff[b][i][k] * cmu[b][k][j]: D(phi) = sum_b DC_b phi_b
   float atf[MP][MK];     // 1 - Diff[a][k][k] / Diff[N-1][k][k]
+  float H[MP][MK][MK];   // d mu / d c of phase b (2 A_kk on the diagonal, A_kl off it): bulk mu += H dc
+  float Gx[MP][MK][MK];  // pure-phase update: mu += Gx Lx + Gy Ly, Gx = H (2 DC) dt / (2 dx^2)
+  float Gy[MP][MK][MK];
+  float pad2[2];
   double cmu_d[MP][MK][MK];
 };
 static_assert(sizeof(Model) % 16 == 0, "Model is copied to shared memory as float4");
@@ -190,54 +194,64 @@ __device__ __forceinline__ float flux_div(float fxp, float fxm, float fyp, float
   return __fadd_rn(__fsub_rn(fxp, fxm), __fsub_rn(fyp, fym));
 }
 
-// bulk cell of one phase: c -> c + dc, mu = dF/dc (calculate_divergence_concentration.h:216-224),
-// with that phase's cmu, Beff and A
+// Bulk cell of phase b whose face fluxes dc were evaluated (a neighbour is not
+// pure b): c -> c + dc, mu = dF/dc (calculate_divergence_concentration.h:216-224)
+// is, for quadratic free energies, mu + H dc with H = d mu / d c of the phase;
+// the FP32 form evaluates it that way (one rounding at mu's scale).
 template <int K1>
-__device__ __forceinline__ void bulk_update_v(const float (&cm)[MK][MK], const float (&be)[MK],
-                                              const float (&aa)[MK][MK], const float* mu, const float* dc,
+__device__ __forceinline__ void bulk_update_h(const float (&H)[MK][MK], const float* mu, const float* dc,
                                               float* mnew) {
-  float c[K1];
 #pragma unroll
   for (int k = 0; k < K1; k++) {
-    float s = 0.f;
+    float s = __fmul_rn(H[k][0], dc[0]);
 #pragma unroll
-    for (int l = 0; l < K1; l++) s = __fmaf_rn(cm[k][l], __fsub_rn(mu[l], be[l]), s);
-    c[k] = __fadd_rn(s, dc[k]);
-  }
-#pragma unroll
-  for (int k = 0; k < K1; k++) {
-    float s = __fmaf_rn(__fmul_rn(2.f, aa[k][k]), c[k], be[k]);
-#pragma unroll
-    for (int l = 0; l < K1; l++)
-      if (l != k) s = __fmaf_rn(aa[k][l], c[l], s);
-    mnew[k] = s;
+    for (int l = 1; l < K1; l++) s = __fmaf_rn(H[k][l], dc[l], s);
+    mnew[k] = __fadd_rn(mu[k], s);
   }
 }
 
-// the constants bulk_update_v needs, of phase b
+// Pure-phase update of a cell whose 3x3 neighbourhood is the one-hot field of
+// phase b: diffusion of mu inside b, mu + Gx Lx + Gy Ly (the face fluxes with
+// both mobilities D_b and the bulk update folded into Gx = H (2 D_b) dt/(2 dx^2),
+// Gy likewise).  Lx = dxp - dxm from the face differences dxp = mu(x+1) - mu,
+// dxm = mu - mu(x-1), which are exact in floating point for neighbouring values
+// (Sterbenz), so the increment is formed at its own scale and added once.  Every
+// kernel uses this for every such cell, so a cell gets the same bits whichever
+// kernel or tile shape updates it.
+template <int K1>
+__device__ __forceinline__ void pure_update(const float (&gx)[MK][MK], const float (&gy)[MK][MK], const float* mu,
+                                            const float* dxp, const float* dxm, const float* dyp, const float* dym,
+                                            float* mnew) {
+  float Lx[K1], Ly[K1];
+#pragma unroll
+  for (int k = 0; k < K1; k++) {
+    Lx[k] = __fsub_rn(dxp[k], dxm[k]);
+    Ly[k] = __fsub_rn(dyp[k], dym[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < K1; k++) {
+    float s = __fmul_rn(gy[k][0], Ly[0]);
+    s = __fmaf_rn(gx[k][0], Lx[0], s);
+#pragma unroll
+    for (int l = 1; l < K1; l++) {
+      s = __fmaf_rn(gy[k][l], Ly[l], s);
+      s = __fmaf_rn(gx[k][l], Lx[l], s);
+    }
+    mnew[k] = __fadd_rn(mu[k], s);
+  }
+}
+
+// the (K1 x K1) block of phase b of a per-phase constant array
 template <int N, int K1>
-__device__ __forceinline__ void phase_consts(const Model& m, int b, float (&cm)[MK][MK], float (&be)[MK],
-                                             float (&aa)[MK][MK]) {
+__device__ __forceinline__ void phase_mat(const float (&src)[MP][MK][MK], int b, float (&out)[MK][MK]) {
 #pragma unroll
   for (int a = 0; a < N; a++)
     if (a == b) {
 #pragma unroll
-      for (int k = 0; k < K1; k++) {
-        be[k] = m.Beff[a][k];
+      for (int k = 0; k < K1; k++)
 #pragma unroll
-        for (int l = 0; l < K1; l++) {
-          cm[k][l] = m.cmu[a][k][l];
-          aa[k][l] = m.A[a][k][l];
-        }
-      }
+        for (int l = 0; l < K1; l++) out[k][l] = src[a][k][l];
     }
-}
-
-template <int N, int K1>
-__device__ __forceinline__ void bulk_update(const Model& m, int bulk, const float* mu, const float* dc, float* mnew) {
-  float cm[MK][MK], be[MK], aa[MK][MK];
-  phase_consts<N, K1>(m, bulk, cm, be, aa);
-  bulk_update_v<K1>(cm, be, aa, mu, dc, mnew);
 }
 
 // ---------------------------------------------------------------- the fused step
@@ -498,15 +512,9 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
   const bool pure = __syncthreads_and(ok) != 0;
 
   if (pure) {
-    float Db[MK][MK];
-#pragma unroll
-    for (int a = 0; a < N; a++)
-      if (a == b0) {
-#pragma unroll
-        for (int k = 0; k < K1; k++)
-#pragma unroll
-          for (int l = 0; l < K1; l++) Db[k][l] = m.DC[a][k][l];
-      }
+    float gx[MK][MK], gy[MK][MK];
+    phase_mat<N, K1>(m.Gx, b0, gx);
+    phase_mat<N, K1>(m.Gy, b0, gy);
     for (int r = warp; r < TX; r += nw) {
       const int x = x0 + r;
       if (x >= mx) break;
@@ -524,14 +532,15 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
           ml[k] = MU(k, i1, j1 - 1);
           mr[k] = MU(k, i1, j1 + 1);
         }
-        float fxp[K1], fxm[K1], fyp[K1], fym[K1], dc[K1], mnew[K1];
-        diff_flux<K1>(Db, Db, mc, mf, m.hx, fxp);
-        diff_flux<K1>(Db, Db, mb, mc, m.hx, fxm);
-        diff_flux<K1>(Db, Db, mc, mr, m.hy, fyp);
-        diff_flux<K1>(Db, Db, ml, mc, m.hy, fym);
+        float dxp[K1], dxm[K1], dyp[K1], dym[K1], mnew[K1];
 #pragma unroll
-        for (int k = 0; k < K1; k++) dc[k] = flux_div(fxp[k], fxm[k], fyp[k], fym[k]);
-        bulk_update<N, K1>(m, b0, mc, dc, mnew);
+        for (int k = 0; k < K1; k++) {
+          dxp[k] = __fsub_rn(mf[k], mc[k]);
+          dxm[k] = __fsub_rn(mc[k], mb[k]);
+          dyp[k] = __fsub_rn(mr[k], mc[k]);
+          dym[k] = __fsub_rn(mc[k], ml[k]);
+        }
+        pure_update<K1>(gx, gy, mc, dxp, dxm, dyp, dym, mnew);
         const int64_t o = (int64_t)x * I.pitch + y;
 #pragma unroll
         for (int k = 0; k < K1; k++) I.mu_out[o + k * I.plane] = mnew[k];
@@ -937,7 +946,31 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
         if (bulk < 0 && ph[a] == 1.f) bulk = a;
       float mnew[K1];
       if (bulk >= 0) {
-        bulk_update<N, K1>(m, bulk, mu, dc, mnew);
+        // phi one-hot `bulk` on the 3x3 neighbourhood: the pure-phase update (the lean kernels' arithmetic)
+        bool p3 = true;
+#pragma unroll
+        for (int di = -1; di <= 1; di++)
+#pragma unroll
+          for (int dj = -1; dj <= 1; dj++)
+#pragma unroll
+            for (int a = 0; a < N; a++) p3 &= PH(a, i1 + 1 + di, j1 + 1 + dj) == (a == bulk ? 1.f : 0.f);
+        if (p3) {
+          float gx[MK][MK], gy[MK][MK], dxp[K1], dxm[K1], dyp[K1], dym[K1];
+          phase_mat<N, K1>(m.Gx, bulk, gx);
+          phase_mat<N, K1>(m.Gy, bulk, gy);
+#pragma unroll
+          for (int k = 0; k < K1; k++) {
+            dxp[k] = __fsub_rn(MU(k, i1 + 1, j1), mu[k]);
+            dxm[k] = __fsub_rn(mu[k], MU(k, i1 - 1, j1));
+            dyp[k] = __fsub_rn(MU(k, i1, j1 + 1), mu[k]);
+            dym[k] = __fsub_rn(mu[k], MU(k, i1, j1 - 1));
+          }
+          pure_update<K1>(gx, gy, mu, dxp, dxm, dyp, dym, mnew);
+        } else {
+          float hb[MK][MK];
+          phase_mat<N, K1>(m.H, bulk, hb);
+          bulk_update_h<K1>(hb, mu, dc, mnew);
+        }
       } else {
         float hh[N];
 #pragma unroll
@@ -1128,7 +1161,7 @@ struct Lean {
 
 // Constants of the lean update of one phase of one instance.
 struct alignas(16) LeanConst {
-  float Db[MK][MK], cm[MK][MK], aa[MK][MK], be[MK], hx, hy;
+  float gx[MK][MK], gy[MK][MK];  // Model::Gx, Gy of the phase
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -1233,18 +1266,14 @@ __device__ __forceinline__ void lean_compute(const Inst& I, const LeanConst& C, 
   const int64_t pitch = I.pitch, plane = I.plane;
   float* const out = I.mu_out + (int64_t)xs * pitch + yb;
   const float* const sb = buf + grp * RG * W + 4 + 4 * lg;  // the group's first staged row, the lane's first cell
-  const float hx = C.hx, hy = C.hy;
-  float Db[MK][MK], cm[MK][MK], be[MK], aa[MK][MK];
+  float gx[MK][MK], gy[MK][MK];
 #pragma unroll
-  for (int k = 0; k < K1; k++) {
-    be[k] = C.be[k];
+  for (int k = 0; k < K1; k++)
 #pragma unroll
     for (int l = 0; l < K1; l++) {
-      Db[k][l] = C.Db[k][l];
-      cm[k][l] = C.cm[k][l];
-      aa[k][l] = C.aa[k][l];
+      gx[k][l] = C.gx[k][l];
+      gy[k][l] = C.gy[k][l];
     }
-  }
   auto row = [&](int r, float (&v)[4][K1]) {
 #pragma unroll
     for (int k = 0; k < K1; k++) {
@@ -1255,37 +1284,35 @@ __device__ __forceinline__ void lean_compute(const Inst& I, const LeanConst& C, 
       v[3][k] = q.w;
     }
   };
-  float cur[4][K1], fxm[4][K1];
+  float cur[4][K1], dxm[4][K1];  // dxm: the difference across each cell's lower x-face
   {
     float prev[4][K1];
     row(0, prev);
     row(1, cur);
 #pragma unroll
-    for (int j = 0; j < 4; j++) diff_flux<K1>(Db, Db, prev[j], cur[j], hx, fxm[j]);
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int k = 0; k < K1; k++) dxm[j][k] = __fsub_rn(cur[j][k], prev[j][k]);
   }
-  // the new mu of the lane's four cells in group row r (box row r + 1); advances cur and fxm
+  // the new mu of the lane's four cells in group row r (box row r + 1); advances cur and dxm
   auto step = [&](int r, float (&mnew)[4][K1]) {
-    float nx[4][K1], left[K1], right[K1], fy[5][K1];
+    float nx[4][K1], dy[5][K1];
     row(r + 2, nx);
 #pragma unroll
     for (int k = 0; k < K1; k++) {
-      left[k] = sb[(k * R + r + 1) * W - 1];
-      right[k] = sb[(k * R + r + 1) * W + 4];
-    }
-    diff_flux<K1>(Db, Db, left, cur[0], hy, fy[0]);
+      dy[0][k] = __fsub_rn(cur[0][k], sb[(k * R + r + 1) * W - 1]);
 #pragma unroll
-    for (int j = 0; j < 3; j++) diff_flux<K1>(Db, Db, cur[j], cur[j + 1], hy, fy[j + 1]);
-    diff_flux<K1>(Db, Db, cur[3], right, hy, fy[4]);
+      for (int j = 1; j < 4; j++) dy[j][k] = __fsub_rn(cur[j][k], cur[j - 1][k]);
+      dy[4][k] = __fsub_rn(sb[(k * R + r + 1) * W + 4], cur[3][k]);
+    }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      float fxp[K1], dc[K1];
-      diff_flux<K1>(Db, Db, cur[j], nx[j], hx, fxp);
+      float dxp[K1];
 #pragma unroll
-      for (int k = 0; k < K1; k++) {
-        dc[k] = flux_div(fxp[k], fxm[j][k], fy[j + 1][k], fy[j][k]);
-        fxm[j][k] = fxp[k];
-      }
-      bulk_update_v<K1>(cm, be, aa, cur[j], dc, mnew[j]);
+      for (int k = 0; k < K1; k++) dxp[k] = __fsub_rn(nx[j][k], cur[j][k]);
+      pure_update<K1>(gx, gy, cur[j], dxp, dxm[j], dy[j + 1], dy[j], mnew[j]);
+#pragma unroll
+      for (int k = 0; k < K1; k++) dxm[j][k] = dxp[k];
     }
 #pragma unroll
     for (int j = 0; j < 4; j++)
@@ -1454,22 +1481,23 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
 
 // ---------------------------------------------------------------- two steps per staged box (depth 2)
 //
-// A cell's update is the pure-phase one (diffusion of mu in phase b, phi kept)
-// when phi is the one-hot field of b on the cell's 3x3 neighbourhood: its face
-// mobilities are those of b, its antitrapping currents vanish (zero gradients),
-// it takes the bulk branch and its divphi is zero.  So the pure region shrinks by
-// at most one cell per step, and a tile lean_phase accepts (phi one-hot b on the
+// A cell's update is the pure-phase one (pure_update: diffusion of mu in phase
+// b, phi kept) when phi is the one-hot field of b on the cell's 3x3
+// neighbourhood, and then its phi stays one-hot: the pure region shrinks by at
+// most one cell per step.  So a tile lean_phase accepts (phi one-hot b on the
 // tile and its two-cell ring) has its cells and its ring's first row/column pure
-// for two steps.  One box of mu -- rows x0-2 .. x0+TX+1, columns y0-4 .. y0+TY+3,
-// at step t -- then gives the tile at t+2: sub-step 1 computes rows x0-1 .. x0+TX
-// of step t+1 into a second shared array (over the box's columns; of those only
-// the tile's columns and the ring column beside them are used), sub-step 2 the
-// tile.  Each cell and face is evaluated by the same helper calls on the same
-// operands as in two single steps, so the results are the same bits.
+// for two steps, and one box of mu -- rows x0-2 .. x0+TX+1, columns y0-4 ..
+// y0+TY+3, at step t -- gives the tile at t+2: sub-step 1 computes rows x0-1 ..
+// x0+TX of step t+1 into a second shared array (over the box's columns; of
+// those only the tile's columns and the ring column beside them are used),
+// sub-step 2 the tile.  Each cell and face goes through the same helper calls
+// on the same operands as two single steps, so the results are the same bits.
 //
 // One tile per warp; a ring of two stages (one box loading while the other is
 // computed).  Lanes own a float4 column group and stream a segment of rows
-// along x, carrying the x-face flux from row to row.
+// along x, carrying the x-face difference from row to row; y-neighbours come
+// from the neighbouring lanes by shuffles (only the tile's outermost groups
+// read the ring column from shared memory in sub-step 2).
 template <int N, int K1, int TX, int TY>
 struct Lean2 {
   static constexpr int R2 = TX + 4;                        // box rows x0-2 .. x0+TX+1
@@ -1495,17 +1523,20 @@ struct Lean2 {
 
 // One lane's diffusion sweep over output rows [r0, r1) of a staged array with
 // R rows of W columns per plane: output row r comes from source rows r, r+1,
-// r+2 (the source starts one row earlier) at columns c0 .. c0+3, with the
-// y-neighbours c0-1 and c0+4 (clamped into the array: a cell whose neighbour
-// lies outside it is never used).  put(r, mnew) stores a row's four new cells.
-// The arithmetic is that of lean_compute, helper call for helper call.
+// r+2 (the source starts one row earlier) at columns c0 .. c0+3.  The
+// y-neighbours c0-1 and c0+4 come from the lanes holding them (shuffles: the
+// warp's lanes hold consecutive groups of a segment; a segment's outermost
+// lanes get an unused value) or, where ld_left / ld_right, from the array.
+// Every lane runs RS rows (the shuffles need the whole warp); rows at or past
+// r1 are computed from clamped rows and not stored.  put(r, mnew) stores a
+// row's four new cells.
 template <int K1, int R, int W, int RS, typename Put>
-__device__ __forceinline__ void lean_sweep(const float* __restrict__ src, int c0, int r0, int r1,
-                                           const float (&Db)[MK][MK], const float (&cm)[MK][MK],
-                                           const float (&be)[MK], const float (&aa)[MK][MK], float hx, float hy,
+__device__ __forceinline__ void lean_sweep(const float* __restrict__ src, int c0, int r0, int r1, bool ld_left,
+                                           bool ld_right, const float (&gx)[MK][MK], const float (&gy)[MK][MK],
                                            Put put) {
   const int cl = c0 > 0 ? c0 - 1 : 0, cr = c0 + 4 < W ? c0 + 4 : W - 1;
   auto row = [&](int r, float (&v)[4][K1]) {
+    r = r < R - 1 ? r : R - 1;
 #pragma unroll
     for (int k = 0; k < K1; k++) {
       const float4 q = *reinterpret_cast<const float4*>(src + (k * R + r) * W + c0);
@@ -1515,41 +1546,42 @@ __device__ __forceinline__ void lean_sweep(const float* __restrict__ src, int c0
       v[3][k] = q.w;
     }
   };
-  float cur[4][K1], fxm[4][K1];
+  float cur[4][K1], dxm[4][K1];
   {
     float prev[4][K1];
     row(r0, prev);
     row(r0 + 1, cur);
 #pragma unroll
-    for (int j = 0; j < 4; j++) diff_flux<K1>(Db, Db, prev[j], cur[j], hx, fxm[j]);
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int k = 0; k < K1; k++) dxm[j][k] = __fsub_rn(cur[j][k], prev[j][k]);
   }
 #pragma unroll
   for (int i = 0; i < RS; i++) {
     const int r = r0 + i;
-    if (r >= r1) break;
-    float nx[4][K1], left[K1], right[K1], fy[5][K1], mnew[4][K1];
+    const int rr = r + 1 < R - 1 ? r + 1 : R - 1;
+    float nx[4][K1], dy[5][K1], mnew[4][K1];
     row(r + 2, nx);
 #pragma unroll
     for (int k = 0; k < K1; k++) {
-      left[k] = src[(k * R + r + 1) * W + cl];
-      right[k] = src[(k * R + r + 1) * W + cr];
-    }
-    diff_flux<K1>(Db, Db, left, cur[0], hy, fy[0]);
+      float left = __shfl_up_sync(0xffffffffu, cur[3][k], 1), right = __shfl_down_sync(0xffffffffu, cur[0][k], 1);
+      if (ld_left) left = src[(k * R + rr) * W + cl];
+      if (ld_right) right = src[(k * R + rr) * W + cr];
+      dy[0][k] = __fsub_rn(cur[0][k], left);
 #pragma unroll
-    for (int j = 0; j < 3; j++) diff_flux<K1>(Db, Db, cur[j], cur[j + 1], hy, fy[j + 1]);
-    diff_flux<K1>(Db, Db, cur[3], right, hy, fy[4]);
+      for (int j = 1; j < 4; j++) dy[j][k] = __fsub_rn(cur[j][k], cur[j - 1][k]);
+      dy[4][k] = __fsub_rn(right, cur[3][k]);
+    }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      float fxp[K1], dc[K1];
-      diff_flux<K1>(Db, Db, cur[j], nx[j], hx, fxp);
+      float dxp[K1];
 #pragma unroll
-      for (int k = 0; k < K1; k++) {
-        dc[k] = flux_div(fxp[k], fxm[j][k], fy[j + 1][k], fy[j][k]);
-        fxm[j][k] = fxp[k];
-      }
-      bulk_update_v<K1>(cm, be, aa, cur[j], dc, mnew[j]);
+      for (int k = 0; k < K1; k++) dxp[k] = __fsub_rn(nx[j][k], cur[j][k]);
+      pure_update<K1>(gx, gy, cur[j], dxp, dxm[j], dy[j + 1], dy[j], mnew[j]);
+#pragma unroll
+      for (int k = 0; k < K1; k++) dxm[j][k] = dxp[k];
     }
-    put(r, mnew);
+    if (r < r1) put(r, mnew);
 #pragma unroll
     for (int j = 0; j < 4; j++)
 #pragma unroll
@@ -1612,19 +1644,45 @@ __device__ __forceinline__ bool next_to_full(const uint8_t* __restrict__ gen, ui
   return f;
 }
 
-// Two steps of the lean tiles of a blocked pair.  adj_mode 1: only the lean tiles
-// next to a tile of the full kernel's list, which also store their step-t+1
-// state (mu, and phi unless the buffer holds it) into the intermediate buffer X
-// (insts_x[i].phi_out / mu_out, purity words flags_x) for the full kernel's
-// second pass; adj_mode 0: the other lean tiles.  Bounded waits as k_lean32.
+// The lean tiles of a blocked pair that border a tile of the full kernel's list,
+// as entries {tile, inst * 8 + phase, x0, y0} (count in cnt[4]).
+__global__ void __launch_bounds__(256) k_adj_list(const int4* __restrict__ tile_desc,
+                                                  const uint32_t* __restrict__ flags_in,
+                                                  const uint8_t* __restrict__ gen, int total,
+                                                  int4* __restrict__ alist, int* __restrict__ cnt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int4 d = make_int4(0, 0, 0, 0);
+  bool adj = false;
+  int b = -1;
+  if (t < total && !gen[t]) {
+    d = tile_desc[t];
+    b = lean_phase(flags_in, (uint32_t)d.w, t);
+    adj = b >= 0 && next_to_full(gen, (uint32_t)d.w, t);
+  }
+  const unsigned bal = __ballot_sync(0xffffffffu, adj);
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0 && bal) base = atomicAdd(&cnt[4], __popc(bal));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (adj) alist[base + __popc(bal & ((1u << lane) - 1u))] = make_int4(t, d.x * 8 + b, d.y, d.z);
+}
+
+// Two steps of the lean tiles of a blocked pair.  alist given (adjacent mode):
+// the listed tiles (lean tiles next to the full kernel's tiles), warp w taking
+// entries w, w + warps, ...; they also store their step t+1 (mu, and phi unless
+// the buffer holds it) into the intermediate buffer X (insts_x[i].phi_out /
+// mu_out, purity words flags_x) for the full kernel's second pass.  Otherwise
+// the lean tiles not next to the list, found by scanning.  Bounded waits as
+// k_lean32.
 template <int N, int K1, int TX, int TY>
 __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
     k_lean2(const Inst* __restrict__ insts, const Inst* __restrict__ insts_x, const LeanConst* __restrict__ lconst,
             const CUtensorMap* __restrict__ tmaps, const int4* __restrict__ tile_desc,
             const uint32_t* __restrict__ flags_in, uint32_t* __restrict__ flags_out, uint32_t* __restrict__ flags_x,
-            const uint8_t* __restrict__ gen, int total, int reverse, int adj_mode, int* __restrict__ err) {
+            const uint8_t* __restrict__ gen, int total, int reverse, const int4* __restrict__ alist,
+            const int* __restrict__ acnt, int* __restrict__ err) {
   using S = Lean2<N, K1, TX, TY>;
-  constexpr int R1 = S::R1, R2 = S::R2, W = S::W, STAGES = S::STAGES;
+  constexpr int R1 = S::R1, R2 = S::R2, W = S::W, STAGES = S::STAGES, Q1 = S::Q1, Q2 = S::Q2;
   extern __shared__ __align__(16) unsigned char lsm_raw[];
   unsigned char* lsm = lsm_raw + ((128 - (smem_u32(lsm_raw) & 127)) & 127);
   const int lane = threadIdx.x & 31;
@@ -1634,7 +1692,10 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
   float* slots = reinterpret_cast<float*>(wsm + S::CTRL);              // [STAGES][SLOT / 4]
   float* mid = reinterpret_cast<float*>(wsm + S::CTRL + STAGES * S::SLOT);  // [K1][R1][W]
   const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) - 32 * nwarp;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int64_t base = wid - 32 * nwarp;
+  int64_t ai = wid - nwarp;  // adjacent mode: the last list entry taken
+  const int na = alist ? *acnt : 0;
   unsigned todo = 0;
   int mine = -1, mx0 = 0, my0 = 0;
   if (lane == 0) {
@@ -1643,17 +1704,21 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
   }
   __syncwarp();
   auto next = [&]() -> int4 {
+    if (alist) {
+      ai += nwarp;
+      return ai < na ? alist[ai] : make_int4(-1, 0, 0, 0);
+    }
     while (!todo) {
       base += 32 * nwarp;
       if (base >= total) return make_int4(-1, 0, 0, 0);
       int64_t tc = base + lane * nwarp;
       if (reverse) tc = total - 1 - tc;
       mine = -1;
-      if (tc >= 0 && tc < total) {
+      if (tc >= 0 && tc < total && !gen[tc]) {
         const int4 d = tile_desc[tc];
         const uint32_t geo = (uint32_t)d.w;
-        const int bc = (geo & TG_REJECT2) ? -1 : lean_phase(flags_in, geo, (int)tc);
-        if (bc >= 0 && next_to_full(gen, geo, (int)tc) == (adj_mode != 0)) {
+        const int bc = lean_phase(flags_in, geo, (int)tc);
+        if (bc >= 0 && !next_to_full(gen, geo, (int)tc)) {
           mine = d.x * 8 + bc;
           mx0 = d.y;
           my0 = d.z;
@@ -1678,6 +1743,12 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
       }
     }
   };
+  // lane layouts of the two sub-steps (lanes outside every segment run a dummy sweep: no stores)
+  const int g1 = lane % Q1, seg1 = lane / Q1, g2 = lane % Q2, seg2 = lane / Q2;
+  const bool live1 = seg1 < S::S1, live2 = seg2 < S::S2;
+  const int a1 = live1 ? seg1 * S::RS1 : 0, e1 = live1 ? min(R1, a1 + S::RS1) : 0;
+  const int a2 = live2 ? seg2 * S::RS2 : 0, e2 = live2 ? min(TX, a2 + S::RS2) : 0;
+  const int c1 = live1 ? 4 * g1 : 0;
   for (int s = 0; s < STAGES - 1; s++) fill(s);
   __syncwarp();
   uint32_t phase = 0;
@@ -1688,8 +1759,9 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
     const int inst = e.y >> 3, b = e.y & 7, x0 = e.z, y0 = e.w;
     const Inst I = insts[inst];
     const LeanConst C = lconst[inst * N + b];
+    const bool adjm = alist != nullptr;
     const bool write_phi = pf(flags_out[e.x], PF_CORE) != 1 + b;
-    const bool write_phi_x = adj_mode && pf(flags_x[e.x], PF_CORE) != 1 + b;
+    const bool write_phi_x = adjm && pf(flags_x[e.x], PF_CORE) != 1 + b;
     if (!mbar_wait(&bar[s], (phase >> s) & 1)) {
       if (lane == 0) atomicExch(err, 1);
       __syncwarp();
@@ -1704,39 +1776,28 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
     // the box's cells on the grid's first ghost row/column: boundary map of step t
     if (x0 - 2 < 0 || x0 + TX + 2 > mx || y0 - 4 < 0 || y0 + TY + 4 > my)
       lean2_ghosts<K1, R2, W>(I, x0 - 2, y0 - 4, box, I.mu, lane);
-    float Db[MK][MK], cm[MK][MK], be[MK], aa[MK][MK];
+    float gx[MK][MK], gy[MK][MK];
 #pragma unroll
-    for (int k = 0; k < K1; k++) {
-      be[k] = C.be[k];
+    for (int k = 0; k < K1; k++)
 #pragma unroll
       for (int l = 0; l < K1; l++) {
-        Db[k][l] = C.Db[k][l];
-        cm[k][l] = C.cm[k][l];
-        aa[k][l] = C.aa[k][l];
+        gx[k][l] = C.gx[k][l];
+        gy[k][l] = C.gy[k][l];
       }
-    }
     // sub-step 1: rows x0-1 .. x0+TX of step t+1 into mid
-    {
-      const int g = lane % S::Q1, seg = lane / S::Q1;
-      if (seg < S::S1) {
-        const int r0 = seg * S::RS1, r1 = min(R1, r0 + S::RS1);
-        lean_sweep<K1, R2, W, S::RS1>(box, 4 * g, r0, r1, Db, cm, be, aa, C.hx, C.hy,
-                                      [&](int r, const float (&v)[4][K1]) {
+    lean_sweep<K1, R2, W, S::RS1>(box, c1, a1, e1, false, false, gx, gy, [&](int r, const float (&v)[4][K1]) {
 #pragma unroll
-                                        for (int k = 0; k < K1; k++)
-                                          *reinterpret_cast<float4*>(mid + (k * R1 + r) * W + 4 * g) =
-                                              make_float4(v[0][k], v[1][k], v[2][k], v[3][k]);
-                                      });
-      }
-    }
+      for (int k = 0; k < K1; k++)
+        *reinterpret_cast<float4*>(mid + (k * R1 + r) * W + c1) = make_float4(v[0][k], v[1][k], v[2][k], v[3][k]);
+    });
     __syncwarp();
     // step t+1 ghosts of a tile at the grid edge (Neumann: sources inside mid)
     if (x0 == 0 || x0 + ex == mx || y0 == 0 || y0 + ey == my)
       lean2_ghosts<K1, R1, W>(I, x0 - 1, y0 - 4, mid, nullptr, lane);
-    if (adj_mode) {  // the tile at step t+1 into X for the full kernel's second pass
+    if (adjm) {  // the tile at step t+1 into X for the full kernel's second pass
       const Inst& X = insts_x[inst];
-      for (int e2 = lane; e2 < ex * S::Q2; e2 += 32) {
-        const int r = e2 / S::Q2, g = e2 % S::Q2, yb = y0 + 4 * g;
+      for (int e3 = lane; e3 < ex * Q2; e3 += 32) {
+        const int r = e3 / Q2, g = e3 % Q2, yb = y0 + 4 * g;
         if (yb >= my) continue;
         const int64_t o = (int64_t)(x0 + r) * X.pitch + yb;
 #pragma unroll
@@ -1750,65 +1811,60 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
         }
         if (write_phi_x)
 #pragma unroll
-          for (int a = 0; a < N; a++) {
-            const float pv = a == b ? 1.f : 0.f;
-            if (yb + 3 < my) *reinterpret_cast<float4*>(X.phi_out + o + a * X.plane) = make_float4(pv, pv, pv, pv);
+          for (int aa = 0; aa < N; aa++) {
+            const float pv = aa == b ? 1.f : 0.f;
+            if (yb + 3 < my) *reinterpret_cast<float4*>(X.phi_out + o + aa * X.plane) = make_float4(pv, pv, pv, pv);
             else
-              for (int j = 0; j < 4 && yb + j < my; j++) X.phi_out[o + a * X.plane + j] = pv;
+              for (int j = 0; j < 4 && yb + j < my; j++) X.phi_out[o + aa * X.plane + j] = pv;
           }
       }
     }
     __syncwarp();
     // sub-step 2: the tile at step t+2
     {
-      const int g = lane % S::Q2, seg = lane / S::Q2;
-      const int yb = y0 + 4 * g;
+      const int yb = y0 + 4 * g2;
       const bool full = x0 + TX <= mx && y0 + TY <= my;
       float* const out = I.mu_out + (int64_t)x0 * I.pitch + yb;
-      if (seg < S::S2) {
-        const int r0 = seg * S::RS2, r1 = min(TX, r0 + S::RS2);
-        lean_sweep<K1, R1, W, S::RS2>(mid, 4 + 4 * g, r0, r1, Db, cm, be, aa, C.hx, C.hy,
-                                      [&](int r, const float (&v)[4][K1]) {
-                                        if (full) {
+      lean_sweep<K1, R1, W, S::RS2>(
+          mid, 4 + 4 * g2, a2, e2, g2 == 0, g2 == Q2 - 1, gx, gy, [&](int r, const float (&v)[4][K1]) {
+            if (full) {
 #pragma unroll
-                                          for (int k = 0; k < K1; k++)
-                                            __stwb(reinterpret_cast<float4*>(out + r * I.pitch + k * I.plane),
-                                                   make_float4(v[0][k], v[1][k], v[2][k], v[3][k]));
-                                        } else if (x0 + r < mx && yb < my) {
-                                          if (yb + 3 < my) {
-#pragma unroll
-                                            for (int k = 0; k < K1; k++)
-                                              __stwb(reinterpret_cast<float4*>(out + r * I.pitch + k * I.plane),
-                                                     make_float4(v[0][k], v[1][k], v[2][k], v[3][k]));
-                                          } else {
-#pragma unroll
-                                            for (int j = 0; j < 4; j++)
-                                              if (yb + j < my)
-#pragma unroll
-                                                for (int k = 0; k < K1; k++)
-                                                  out[r * I.pitch + k * I.plane + j] = v[j][k];
-                                          }
-                                        }
-                                      });
-        if (write_phi) {
-          float* const po = I.phi_out + (int64_t)x0 * I.pitch + yb;
-          for (int r = r0; r < r1 && x0 + r < mx; r++)
-#pragma unroll
-            for (int a = 0; a < N; a++) {
-              const float v = a == b ? 1.f : 0.f;
+              for (int k = 0; k < K1; k++)
+                __stwb(reinterpret_cast<float4*>(out + r * I.pitch + k * I.plane),
+                       make_float4(v[0][k], v[1][k], v[2][k], v[3][k]));
+            } else if (x0 + r < mx && yb < my) {
               if (yb + 3 < my) {
-                *reinterpret_cast<float4*>(po + r * I.pitch + a * I.plane) = make_float4(v, v, v, v);
+#pragma unroll
+                for (int k = 0; k < K1; k++)
+                  __stwb(reinterpret_cast<float4*>(out + r * I.pitch + k * I.plane),
+                         make_float4(v[0][k], v[1][k], v[2][k], v[3][k]));
               } else {
-                for (int j = 0; j < 4 && yb + j < my; j++) po[r * I.pitch + a * I.plane + j] = v;
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                  if (yb + j < my)
+#pragma unroll
+                    for (int k = 0; k < K1; k++) out[r * I.pitch + k * I.plane + j] = v[j][k];
               }
             }
-        }
+          });
+      if (write_phi) {
+        float* const po = I.phi_out + (int64_t)x0 * I.pitch + yb;
+        for (int r = a2; r < e2 && x0 + r < mx; r++)
+#pragma unroll
+          for (int aa = 0; aa < N; aa++) {
+            const float v = aa == b ? 1.f : 0.f;
+            if (yb + 3 < my) {
+              *reinterpret_cast<float4*>(po + r * I.pitch + aa * I.plane) = make_float4(v, v, v, v);
+            } else {
+              for (int j = 0; j < 4 && yb + j < my; j++) po[r * I.pitch + aa * I.plane + j] = v;
+            }
+          }
       }
     }
     __syncwarp();
     if (lane == 0) {
       flags_out[e.x] = pf_all(1 + b);
-      if (adj_mode) flags_x[e.x] = pf_all(1 + b);
+      if (adjm) flags_x[e.x] = pf_all(1 + b);
     }
   }
 }
@@ -1829,6 +1885,7 @@ __global__ void __launch_bounds__(256) k_general_list(const int4* __restrict__ t
   const bool gen = t < total && (lean_phase(flags_in, (uint32_t)d.w, t) < 0 ||
                                  (depth > 1 && ((uint32_t)d.w & TG_REJECT2)));
   if (genb && t < total) genb[t] = gen ? 1 : 0;
+  if (depth > 1 && t == 0) cnt[4] = 0;  // the adjacency list (k_adj_list) of this pair starts empty
   const bool ring = gen && pf(flags_in[t], PF_CORE) != 0;  // pure inside
   const unsigned bal = __ballot_sync(0xffffffffu, gen && !ring), balr = __ballot_sync(0xffffffffu, ring);
   const int lane = threadIdx.x & 31;
@@ -1890,8 +1947,21 @@ Model make_model(const gp_model& g) {
         double s = 0.0;
         for (int k = 0; k < K1; k++) s += g.Diff[a][i][k] * g.cmu[a][k][j];
         m.DC[a][i][j] = (float)s;
+        m.H[a][i][j] = (float)(i == j ? 2.0 * g.A[a][i][i] : g.A[a][i][j]);
       }
     }
+    // Gx = H (2 DC) dt / (2 dx^2), Gy likewise, folded in double
+    for (int i = 0; i < K1; i++)
+      for (int j = 0; j < K1; j++) {
+        double s = 0.0;
+        for (int k = 0; k < K1; k++) {
+          double dc = 0.0;
+          for (int l = 0; l < K1; l++) dc += g.Diff[a][k][l] * g.cmu[a][l][j];
+          s += (k == i ? 2.0 * g.A[a][i][i] : g.A[a][i][k]) * 2.0 * dc;
+        }
+        m.Gx[a][i][j] = (float)(s * 0.5 * g.dt / (g.dx * g.dx));
+        m.Gy[a][i][j] = (float)(s * 0.5 * g.dt / (g.dy * g.dy));
+      }
   }
   return m;
 }
@@ -1909,7 +1979,7 @@ struct KernelSet {
   void (*lean)(const Inst*, const LeanConst*, const CUtensorMap*, const int4*, const uint32_t*, uint32_t*, int, int,
                int, int*);
   void (*lean2)(const Inst*, const Inst*, const LeanConst*, const CUtensorMap*, const int4*, const uint32_t*,
-                uint32_t*, uint32_t*, const uint8_t*, int, int, int, int*);
+                uint32_t*, uint32_t*, const uint8_t*, int, int, const int4*, const int*, int*);
   void (*list)(const int4*, const uint32_t*, int, int2*, int*, uint8_t*, int);
   size_t smem_general, smem_lean, smem_lean2;
 };
@@ -1974,7 +2044,9 @@ struct gp_f32_batch {
   Inst* dinst_x2[2] = {nullptr, nullptr};
   CUtensorMap* dtmap2[2] = {nullptr, nullptr};  // [parity][n] mu boxes of the two-step lean kernel
   uint8_t* dgen = nullptr;                      // [total_tiles] tile listed for the full kernel (blocked pairs)
+  int4* dalist = nullptr;                       // [total_tiles] lean tiles next to the list (blocked pairs)
   cudaEvent_t ev_list = nullptr, ev_adj = nullptr;
+  cudaStream_t side2 = nullptr;  // blocked pairs: the lean tiles next to the full kernel's list
   int grid_lean2 = 0, occ_lean2 = 0;
   int lose_box = 0;      // failure-detection test: the next lean launch loses one stage's boxes
   std::vector<gp_model> gm;
@@ -1991,7 +2063,7 @@ struct gp_f32_batch {
   int4* dtile_desc = nullptr;  // [total_tiles] {instance, x0, y0, tile_geo}
   std::vector<int4> htile_desc;
   int2* dglist = nullptr;      // [total_tiles] {tile, instance} of the full kernel's tiles
-  int* dcnt = nullptr;         // [4] list count, queue head, finished blocks
+  int* dcnt = nullptr;         // [8] list count, queue head, finished blocks, ring-only count, adjacency count
   int grid_general = 0, grid_lean = 0;
   int occ_general = 0, occ_lean = 0;         // resident blocks per SM at full occupancy
   int step_threads = 256;                    // full-kernel block size: 256 or 512
@@ -2019,6 +2091,8 @@ static void free_tiles(gp_f32_batch* b) {
   cudaFree(b->dtile_desc);
   cudaFree(b->dglist);
   cudaFree(b->dgen);
+  cudaFree(b->dalist);
+  b->dalist = nullptr;
   b->dflags = nullptr;
   b->dtile_inst = nullptr;
   b->dtile_desc = nullptr;
@@ -2046,16 +2120,11 @@ cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** ou
     for (int a = 0; a < b->N; a++) {
       LeanConst& L = hl[(size_t)i * b->N + a];
       memset(&L, 0, sizeof L);
-      for (int k = 0; k < MK; k++) {
-        L.be[k] = hm[i].Beff[a][k];
+      for (int k = 0; k < MK; k++)
         for (int l = 0; l < MK; l++) {
-          L.Db[k][l] = hm[i].DC[a][k][l];
-          L.cm[k][l] = hm[i].cmu[a][k][l];
-          L.aa[k][l] = hm[i].A[a][k][l];
+          L.gx[k][l] = hm[i].Gx[a][k][l];
+          L.gy[k][l] = hm[i].Gy[a][k][l];
         }
-      }
-      L.hx = hm[i].hx;
-      L.hy = hm[i].hy;
     }
   cudaError_t e = cudaMalloc(&b->dmodel, sizeof(Model) * n);
   if (e == cudaSuccess) e = cudaMemcpy(b->dmodel, hm.data(), sizeof(Model) * n, cudaMemcpyHostToDevice);
@@ -2064,13 +2133,14 @@ cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** ou
     e = cudaMemcpy(b->dlconst, hl.data(), sizeof(LeanConst) * hl.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc(&b->derr, 2 * sizeof(int));  // error word, test token
   if (e == cudaSuccess) e = cudaMemset(b->derr, 0, 2 * sizeof(int));
-  if (e == cudaSuccess) e = cudaMalloc(&b->dcnt, 4 * sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(b->dcnt, 0, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->dcnt, 8 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->dcnt, 0, 8 * sizeof(int));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_list, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_adj, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side2, cudaStreamNonBlocking);
   for (int p = 0; e == cudaSuccess && p < 2; p++) {
     b->hinst[p].resize(n);
     b->hinst_x1[p].resize(n);
@@ -2110,6 +2180,10 @@ void gp_f32_batch_destroy(gp_f32_batch* b) {
   if (b->ev_list) cudaEventDestroy(b->ev_list);
   if (b->ev_adj) cudaEventDestroy(b->ev_adj);
   if (b->side) cudaStreamDestroy(b->side);
+  if (b->side2) {
+    cudaStreamSynchronize(b->side2);
+    cudaStreamDestroy(b->side2);
+  }
   delete b;
 }
 
@@ -2293,6 +2367,7 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   if (e == cudaSuccess) e = cudaMemset(b->dflags, 0, 3 * sizeof(uint32_t) * (size_t)t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dgen, (size_t)t);
   if (e == cudaSuccess) e = cudaMemset(b->dgen, 0, (size_t)t);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dalist, sizeof(int4) * (size_t)t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dtile_inst, sizeof(int) * t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dglist, sizeof(int2) * t);
   if (e == cudaSuccess) e = cudaMalloc(&b->dtile_desc, sizeof(int4) * t);
@@ -2465,8 +2540,9 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
 // and writing parity^1; X holds step t+1 of the tiles that need it.
 //   stream s:    list (tiles for the full kernel, gen bytes)  -> full pass 1 (buffer p -> X)
 //                -> [lean tiles next to the list done] -> full pass 2 (X -> buffer p^1)
-//   side stream: [list done] -> two-step lean kernel on the tiles next to the list (also writing
-//                their step t+1 into X) -> two-step lean kernel on the other lean tiles
+//   second side stream: [list done] -> list of the lean tiles next to the list -> two-step lean
+//                kernel on them (also writing their step t+1 into X)
+//   side stream: [list done] -> two-step lean kernel on the other lean tiles
 // Timed launches run one after the other on s.
 cudaError_t gp_f32_batch_launch_pair(gp_f32_batch* b, int parity, cudaStream_t s) {
   if (b->depth != 2 || !b->narrowband || !b->has_x) return cudaErrorInvalidValue;
@@ -2486,18 +2562,22 @@ cudaError_t gp_f32_batch_launch_pair(gp_f32_batch* b, int parity, cudaStream_t s
                                                       b->dgen, 2);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (E && (e = cudaEventRecord(E[3], s)) != cudaSuccess) return e;
-  cudaStream_t ls = E ? s : b->side;
+  cudaStream_t ls = E ? s : b->side, as = E ? s : b->side2;
   if (!E) {
     if ((e = cudaEventRecord(b->ev_list, s)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(b->side, b->ev_list, 0)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(b->side2, b->ev_list, 0)) != cudaSuccess) return e;
   }
   if (E && (e = cudaEventRecord(E[0], ls)) != cudaSuccess) return e;
+  k_adj_list<<<(b->total_tiles + 255) / 256, 256, 0, as>>>(b->dtile_desc, flags_in, b->dgen, b->total_tiles,
+                                                           b->dalist, b->dcnt);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   for (int adj = 1; adj >= 0; adj--) {
-    k.lean2<<<b->grid_lean2, 128, k.smem_lean2, ls>>>(b->dinst[p], b->dinst_x1[p], b->dlconst, b->dtmap2[p],
-                                                      b->dtile_desc, flags_in, flags_out, flags_x, b->dgen,
-                                                      b->total_tiles, p, adj, b->derr);
+    k.lean2<<<b->grid_lean2, 128, k.smem_lean2, adj ? as : ls>>>(
+        b->dinst[p], b->dinst_x1[p], b->dlconst, b->dtmap2[p], b->dtile_desc, flags_in, flags_out, flags_x, b->dgen,
+        b->total_tiles, p, adj ? b->dalist : nullptr, adj ? b->dcnt + 4 : nullptr, b->derr);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (adj && !E && (e = cudaEventRecord(b->ev_adj, ls)) != cudaSuccess) return e;
+    if (adj && !E && (e = cudaEventRecord(b->ev_adj, as)) != cudaSuccess) return e;
   }
   if (E && (e = cudaEventRecord(E[1], ls)) != cudaSuccess) return e;
   if (E && (e = cudaEventRecord(E[4], s)) != cudaSuccess) return e;
@@ -2551,4 +2631,4 @@ const int* gp_f32_batch_error_word(const gp_f32_batch* b) { return b->derr; }
 // kernel launches one gp_f32_batch_launch issues
 int gp_f32_batch_launches_per_step(const gp_f32_batch* b) { return b->narrowband ? (b->scan ? 2 : 3) : 1; }
 // kernel launches one gp_f32_batch_launch_pair issues (two steps)
-int gp_f32_batch_launches_per_pair(const gp_f32_batch*) { return 5; }
+int gp_f32_batch_launches_per_pair(const gp_f32_batch*) { return 6; }

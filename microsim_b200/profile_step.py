@@ -3,13 +3,15 @@
 
     python -m microsim_b200.profile_step [--workload c4|c2|c1] [--state FILE]
                                          [--tile TX TY] [--steps S] [--full]
+                                         [--depth 1|2] [--lean-per-sm L]
 
 The workload's state is first advanced as the benchmark does (the batched
 sweep 2,500 steps, the 1024^2 dendrite 25,000, the 200^2 seed 5,000); with
 --state the advanced state is saved to FILE on the first run and read back on
 later ones, so a profiled run launches only a handful of kernels before the
 range.  --full switches the narrow band off (every tile through the full
-kernel).
+kernel); --depth 2 steps in blocked pairs (two steps per lean box);
+--lean-per-sm sets the lean grid's blocks per SM (0: occupancy).
 """
 from __future__ import annotations
 
@@ -30,6 +32,8 @@ def main(argv=None):
     ap.add_argument("--tile", type=int, nargs=2, default=[16, 32])
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--full", action="store_true")
+    ap.add_argument("--depth", type=int, default=1, choices=[1, 2])
+    ap.add_argument("--lean-per-sm", type=int, default=0)
     a = ap.parse_args(argv)
     cases = {"c4": configs.c4, "c2": lambda: [configs.c2(literal=False, steps=50000)],
              "c1": lambda: [configs.c1(literal=False, steps=10000)]}[a.workload]()
@@ -51,6 +55,9 @@ def main(argv=None):
     with mb.Batch(models) as b:
         b.set_tile(*a.tile)
         b.set_narrowband(not a.full)
+        if not a.full:
+            b.set_depth(a.depth)
+        b.set_grids(a.lean_per_sm, 0)
         for i, f in enumerate(fields):
             b.upload(i, *f)
         b.step(3)
@@ -60,7 +67,8 @@ def main(argv=None):
         b.sync()
         torch.cuda.nvtx.range_pop()
         lean, total, _ = b.lean_stats()
-    print(f"profiled {a.steps} steps of {a.workload}, tile {a.tile[0]}x{a.tile[1]}, lean tiles {lean} of {total}")
+    print(f"profiled {a.steps} steps of {a.workload}, tile {a.tile[0]}x{a.tile[1]}, depth {a.depth}, "
+          f"lean tiles {lean} of {total}")
 
 
 if __name__ == "__main__":
