@@ -253,28 +253,44 @@ def traffic_table():
 
 def fp64_plain_rate(models, fields, steps, warmup, dev, world):
     """FP64 plain step (bit-exact to the reference) over every instance of the
-    workload: one context per instance, K steps each bracketed by CUDA events
-    on its stream; time = sum over instances."""
+    workload: one context per instance, each on its own stream, all stepped
+    concurrently; K steps between a CUDA event on a master stream (which every
+    context's stream waits on) and the master's wait on every context's end
+    event."""
     import torch
     import microsim_b200 as mb
-    total_ms, cells = 0.0, 0
-    for m, (p, u) in zip(models, fields):
-        with mb.Context(m, mb.GP_FP64) as c:
+    ctxs = []
+    try:
+        for m, (p, u) in zip(models, fields):
+            c = mb.Context(m, mb.GP_FP64)
+            ctxs.append(c)
             c.upload(p, u)
             c.step(warmup)
+        for c in ctxs:
             c.sync()
-            s = torch.cuda.ExternalStream(c.stream, device=dev)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            with torch.cuda.stream(s):
-                e0.record(s)
+        torch.cuda.synchronize()
+        master = torch.cuda.Stream(device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(master)
+        streams = [torch.cuda.ExternalStream(c.stream, device=dev) for c in ctxs]
+        for s in streams:
+            s.wait_event(e0)
+        for c in ctxs:
             c.step(steps)
-            with torch.cuda.stream(s):
-                e1.record(s)
-            e1.synchronize()
-            total_ms += e0.elapsed_time(e1)
-            cells += m.mesh_x * m.mesh_y
+        for s in streams:
+            ev = torch.cuda.Event()
+            ev.record(s)
+            master.wait_event(ev)
+        e1.record(master)
+        e1.synchronize()
+        total_ms = e0.elapsed_time(e1)
+        cells = sum(m.mesh_x * m.mesh_y for m in models)
+    finally:
+        for c in ctxs:
+            c.close()
     total_ms = allmax(total_ms, world)
-    return {"value": allsum(cells, world) * steps / (total_ms / 1e3), "unit": UNIT, "ms_per_step": total_ms / steps}
+    return {"value": allsum(cells, world) * steps / (total_ms / 1e3), "unit": UNIT, "ms_per_step": total_ms / steps,
+            "how": f"{len(models)} contexts, one stream each, stepped concurrently"}
 
 
 def run_ours(args, world, rank, local):
@@ -365,6 +381,32 @@ def run_ours(args, world, rank, local):
     esize = 4
     alg_bytes = 2 * (N + K1) * esize
 
+    # ---- dense FP32 (narrow band off: every tile through the full kernel, phi and mu moved every
+    # step): the chosen form's precision and kernels without the narrow band or temporal blocking
+    dense = None
+    if not args.no_fp64:
+        nb_depth = ctx.depth()
+        ctx.set_narrowband(False)
+        ctx.prepare()
+        ctx.step(args.warmup)
+        ctx.sync()
+        ed0, ed1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            ed0.record(stream)
+        ctx.step(args.steps)
+        with torch.cuda.stream(stream):
+            ed1.record(stream)
+        ctx.sync()
+        dms = allmax(ed0.elapsed_time(ed1), world)
+        dval = cells_all * args.steps / (dms / 1e3)
+        dach = dval / world * alg_bytes / 1e9
+        dense = {"value": dval, "unit": UNIT, "ms_per_step": dms / args.steps,
+                 "roofline": {"bound": "hbm", "achieved": dach, "peak": peak, "unit": "GB/s", "frac": dach / peak,
+                              "alg_bytes_per_cell": alg_bytes,
+                              "note": "phi and mu read + write once per cell-update, every tile"}}
+        ctx.set_narrowband(True)
+        ctx.set_depth(nb_depth)
+
     # ---- FP64 plain on the same workload
     fp64 = None
     if not args.no_fp64:
@@ -433,9 +475,18 @@ def run_ours(args, world, rank, local):
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
+        if dense:
+            line["fp32_dense"] = dense
         if fp64:
+            alg64 = 2 * (N + K1) * 8
+            fp64["roofline"] = {"bound": "hbm", "achieved": fp64["value"] / world * alg64 / 1e9, "peak": peak,
+                                "unit": "GB/s", "frac": fp64["value"] / world * alg64 / 1e9 / peak,
+                                "alg_bytes_per_cell": alg64}
             line["fp64_plain"] = fp64
             line["fp32_over_fp64"] = value / fp64["value"]
+            if dense:  # the speed-up in parts: precision and kernels, then narrow band and blocking
+                line["speedup_parts"] = {"fp32_dense_over_fp64": dense["value"] / fp64["value"],
+                                         "narrowband_and_blocking_over_dense": value / dense["value"]}
         print(json.dumps(line))
 
 

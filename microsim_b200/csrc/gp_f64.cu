@@ -139,6 +139,18 @@ __device__ __forceinline__ double free_energy(const gp_model& m, const double* c
 }
 
 // d psi / d phi_a, functions/functionF_01.h:41-57
+// x / d with IEEE rounding.  When d is an exact power of two the quotient equals
+// the product with the exact reciprocal (one rounding of the same real number),
+// so that case multiplies: the bits are those of the division, without the
+// division routine (dx = dy = 1 and 2 dy = 2 in most inputs).
+__device__ __forceinline__ double gp_ddiv(double x, double d) {
+  const long long bits = __double_as_longlong(d);
+  const long long ex = (bits >> 52) & 0x7FF;
+  if ((bits & 0x000FFFFFFFFFFFFFLL) == 0 && ex > 1 && ex < 2046 && bits > 0)
+    return x * __longlong_as_double((2046LL << 52) - bits);
+  return x / d;
+}
+
 template <int N, int K1>
 __device__ __forceinline__ double dpsi(const gp_model& m, const double* mu, const double* phi, int a) {
   double sum = 0.0;
@@ -213,20 +225,20 @@ template <int N>
 __device__ __forceinline__ void make_grads(const gp_model& m, const double (&P)[3][3][N], double two_dy, Grads<N>& G) {
 #pragma unroll
   for (int a = 0; a < N; a++) {
-    G.gx[a] = (P[2][1][a] - P[1][1][a]) / m.dx;
+    G.gx[a] = gp_ddiv((P[2][1][a] - P[1][1][a]), m.dx);
     G.sx[a] = 0.5 * (P[2][1][a] + P[1][1][a]);
-    G.gy[a] = (P[1][2][a] - P[1][1][a]) / m.dy;
+    G.gy[a] = gp_ddiv((P[1][2][a] - P[1][1][a]), m.dy);
     G.sy[a] = 0.5 * (P[1][2][a] + P[1][1][a]);
-    G.cy[a] = (P[1][2][a] - P[1][0][a]) / two_dy;
-    G.b_gx[a] = (P[1][1][a] - P[0][1][a]) / m.dx;
+    G.cy[a] = gp_ddiv((P[1][2][a] - P[1][0][a]), two_dy);
+    G.b_gx[a] = gp_ddiv((P[1][1][a] - P[0][1][a]), m.dx);
     G.cx[a] = 0.5 * (G.gx[a] + G.b_gx[a]);
     G.b_sx[a] = 0.5 * (P[1][1][a] + P[0][1][a]);
-    G.b_cy[a] = (P[0][2][a] - P[0][0][a]) / two_dy;
-    G.f_cy[a] = (P[2][2][a] - P[2][0][a]) / two_dy;
-    G.l_gy[a] = (P[1][1][a] - P[1][0][a]) / m.dy;
+    G.b_cy[a] = gp_ddiv((P[0][2][a] - P[0][0][a]), two_dy);
+    G.f_cy[a] = gp_ddiv((P[2][2][a] - P[2][0][a]), two_dy);
+    G.l_gy[a] = gp_ddiv((P[1][1][a] - P[1][0][a]), m.dy);
     G.l_sy[a] = 0.5 * (P[1][1][a] + P[1][0][a]);
-    G.l_cx[a] = 0.5 * ((P[2][0][a] - P[1][0][a]) / m.dx + (P[1][0][a] - P[0][0][a]) / m.dx);
-    G.r_cx[a] = 0.5 * ((P[2][2][a] - P[1][2][a]) / m.dx + (P[1][2][a] - P[0][2][a]) / m.dx);
+    G.l_cx[a] = 0.5 * (gp_ddiv((P[2][0][a] - P[1][0][a]), m.dx) + gp_ddiv((P[1][0][a] - P[0][0][a]), m.dx));
+    G.r_cx[a] = 0.5 * (gp_ddiv((P[2][2][a] - P[1][2][a]), m.dx) + gp_ddiv((P[1][2][a] - P[0][2][a]), m.dx));
   }
 }
 
@@ -253,10 +265,10 @@ __device__ __forceinline__ double grad_energy_term(const gp_model& m, const doub
     for (int b = 0; b < N; b++) {
       if (b == a) continue;
       double dv;
-      dv = ((G.sx[a] * G.gx[b] - G.sx[b] * G.gx[a]) * (-G.sx[b]) -
-            ((G.b_sx[a] * G.b_gx[b] - G.b_sx[b] * G.b_gx[a]) * (-G.b_sx[b]))) / m.dx;
-      dv += ((G.sy[a] * G.gy[b] - G.sy[b] * G.gy[a]) * (-G.sy[b]) -
-             ((G.l_sy[a] * G.l_gy[b] - G.l_sy[b] * G.l_gy[a]) * (-G.l_sy[b]))) / m.dy;
+      dv = gp_ddiv(((G.sx[a] * G.gx[b] - G.sx[b] * G.gx[a]) * (-G.sx[b]) -
+            ((G.b_sx[a] * G.b_gx[b] - G.b_sx[b] * G.b_gx[a]) * (-G.b_sx[b]))), m.dx);
+      dv += gp_ddiv(((G.sy[a] * G.gy[b] - G.sy[b] * G.gy[a]) * (-G.sy[b]) -
+             ((G.l_sy[a] * G.l_gy[b] - G.l_sy[b] * G.l_gy[a]) * (-G.l_sy[b]))), m.dy);
       dv *= m.Gamma[a][b];
       sum += dv;
     }
@@ -307,10 +319,10 @@ __device__ __forceinline__ double grad_energy_term(const gp_model& m, const doub
     const double acr = aniso_ac(dab, qr0, qr1), acr2 = acr * acr;
     const double acl = aniso_ac(dab, ql0, ql1), acl2 = acl * acl;
     double d1;
-    d1 = ((acf2 * (G.sx[a] * G.gx[b] - G.sx[b] * G.gx[a]) * (-G.sx[b])) -
-          (acb2 * (G.b_sx[a] * G.b_gx[b] - G.b_sx[b] * G.b_gx[a]) * (-G.b_sx[b]))) / m.dx;
-    d1 += ((acr2 * (G.sy[a] * G.gy[b] - G.sy[b] * G.gy[a]) * (-G.sy[b])) -
-           (acl2 * (G.l_sy[a] * G.l_gy[b] - G.l_sy[b] * G.l_gy[a]) * (-G.l_sy[b]))) / m.dy;
+    d1 = gp_ddiv(((acf2 * (G.sx[a] * G.gx[b] - G.sx[b] * G.gx[a]) * (-G.sx[b])) -
+          (acb2 * (G.b_sx[a] * G.b_gx[b] - G.b_sx[b] * G.b_gx[a]) * (-G.b_sx[b]))), m.dx);
+    d1 += gp_ddiv(((acr2 * (G.sy[a] * G.gy[b] - G.sy[b] * G.gy[a]) * (-G.sy[b])) -
+           (acl2 * (G.l_sy[a] * G.l_gy[b] - G.l_sy[b] * G.l_gy[a]) * (-G.l_sy[b]))), m.dy);
     d1 *= gam;
     s1 += d1;
     double e0, e1, rf0, rf1, rb0, rb1, rr0, rr1, rl0, rl1;
@@ -328,8 +340,8 @@ __device__ __forceinline__ double grad_energy_term(const gp_model& m, const doub
     const double ql2 = ql0 * ql0 + ql1 * ql1;
     (void)rf1; (void)rb1; (void)rr0; (void)rl0;
     double d2;
-    d2 = (acf * qf2 * rf0 * (-G.sx[b]) - acb * qb2 * rb0 * (-G.b_sx[b])) / m.dx;
-    d2 += (acr * qr2 * rr1 * (-G.sy[b]) - acl * ql2 * rl1 * (-G.l_sy[b])) / m.dy;
+    d2 = gp_ddiv((acf * qf2 * rf0 * (-G.sx[b]) - acb * qb2 * rb0 * (-G.b_sx[b])), m.dx);
+    d2 += gp_ddiv((acr * qr2 * rr1 * (-G.sy[b]) - acl * ql2 * rl1 * (-G.l_sy[b])), m.dy);
     d2 *= gam;
     s2 += d2;
   }
@@ -439,7 +451,7 @@ __device__ __forceinline__ void project_simplex(const double* phi, const double*
     for (int b = 0; b < N; b++)
       if ((fabs(divphi[b]) > 0.0) && ((phi[b] + dp[b]) > 0.0) && ((phi[b] + dp[b]) < 1.0)) {
         if (fabs(sum_phib) > 0.0) dp[b] -= Deltaphi * (phi[b]) / (sum_phib);
-        else dp[b] -= Deltaphi / (double)(count);
+        else dp[b] -= gp_ddiv(Deltaphi, (double)(count));
       }
   }
   int hit = -1;
@@ -478,7 +490,7 @@ __device__ __forceinline__ void project_simplex_unweighted(const double* phi, co
 #pragma unroll
       for (int b = 0; b < N; b++)
         if (((fabs(divphi[b]) > 0.0) && b != a) && (phi[b] + dp[b]) > 0.0 && (phi[b] + dp[b]) < 1.0)
-          dp[b] -= D / (double)(count);
+          dp[b] -= gp_ddiv(D, (double)(count));
     }
   }
 }
@@ -490,7 +502,7 @@ __device__ __forceinline__ void project_simplex_unweighted(const double* phi, co
 // isotropic gradient energy, no dpsi, the unsigned potential when anisotropic,
 // unweighted projection.
 template <int N, int K1, bool SMOOTH>
-__global__ void __launch_bounds__(256) k_dphi(const __grid_constant__ gp_model m, Geo g,
+__global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_dphi(const __grid_constant__ gp_model m, Geo g,
                                               const double* __restrict__ phi, const double* __restrict__ mu,
                                               double* __restrict__ dphi) {
   const int y = blockIdx.x * blockDim.x + threadIdx.x - 1;
@@ -510,8 +522,8 @@ __global__ void __launch_bounds__(256) k_dphi(const __grid_constant__ gp_model m
   double divphi[N], lambda[N], dp[N];
 #pragma unroll
   for (int a = 0; a < N; a++) {
-    divphi[a] = (G.gx[a] - G.b_gx[a]) / m.dx;
-    divphi[a] += (G.gy[a] - G.l_gy[a]) / m.dy;
+    divphi[a] = gp_ddiv((G.gx[a] - G.b_gx[a]), m.dx);
+    divphi[a] += gp_ddiv((G.gy[a] - G.l_gy[a]), m.dy);
   }
   double sum_lambda = 0.0;
   long active = 0;
@@ -529,7 +541,7 @@ __global__ void __launch_bounds__(256) k_dphi(const __grid_constant__ gp_model m
       active++;
     }
   }
-  if (active) sum_lambda /= (double)active;
+  if (active) sum_lambda = gp_ddiv(sum_lambda, (double)active);
   const double tphi = tau_phi<N>(m, ph);
 #pragma unroll
   for (int a = 0; a < N; a++) {
@@ -683,7 +695,7 @@ __device__ __forceinline__ void lu_inverse(double (&mm)[K][K], double (&inv)[K][
 // (calculate_divergence_concentration.h:154-253): no antitrapping current, no
 // dh/dt source, the LU inverse (matinvnew) for every mu solve.
 template <int N, int K1, bool SMOOTH>
-__global__ void __launch_bounds__(256) k_update(const __grid_constant__ gp_model m, Geo g,
+__global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_update(const __grid_constant__ gp_model m, Geo g,
                                                 const double* __restrict__ phi, const double* __restrict__ mu,
                                                 const double* __restrict__ dphi, double* __restrict__ phi_out,
                                                 double* __restrict__ mu_out) {
@@ -719,16 +731,16 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ gp_model
   double cy_c[N], cy_b[N], cy_f[N], cx_c[N], cx_l[N], cx_r[N];
 #pragma unroll
   for (int a = 0; a < N; a++) {
-    gx_c[a] = (P[2][1][a] - P[1][1][a]) / m.dx;
-    gx_b[a] = (P[1][1][a] - P[0][1][a]) / m.dx;
-    gy_c[a] = (P[1][2][a] - P[1][1][a]) / m.dy;
-    gy_l[a] = (P[1][1][a] - P[1][0][a]) / m.dy;
-    cy_c[a] = (P[1][2][a] - P[1][0][a]) / two_dy;
-    cy_b[a] = (P[0][2][a] - P[0][0][a]) / two_dy;
-    cy_f[a] = (P[2][2][a] - P[2][0][a]) / two_dy;
+    gx_c[a] = gp_ddiv((P[2][1][a] - P[1][1][a]), m.dx);
+    gx_b[a] = gp_ddiv((P[1][1][a] - P[0][1][a]), m.dx);
+    gy_c[a] = gp_ddiv((P[1][2][a] - P[1][1][a]), m.dy);
+    gy_l[a] = gp_ddiv((P[1][1][a] - P[1][0][a]), m.dy);
+    cy_c[a] = gp_ddiv((P[1][2][a] - P[1][0][a]), two_dy);
+    cy_b[a] = gp_ddiv((P[0][2][a] - P[0][0][a]), two_dy);
+    cy_f[a] = gp_ddiv((P[2][2][a] - P[2][0][a]), two_dy);
     cx_c[a] = 0.5 * (gx_c[a] + gx_b[a]);
-    cx_l[a] = 0.5 * ((P[2][0][a] - P[1][0][a]) / m.dx + (P[1][0][a] - P[0][0][a]) / m.dx);
-    cx_r[a] = 0.5 * ((P[2][2][a] - P[1][2][a]) / m.dx + (P[1][2][a] - P[0][2][a]) / m.dx);
+    cx_l[a] = 0.5 * (gp_ddiv((P[2][0][a] - P[1][0][a]), m.dx) + gp_ddiv((P[1][0][a] - P[0][0][a]), m.dx));
+    cx_r[a] = 0.5 * (gp_ddiv((P[2][2][a] - P[1][2][a]), m.dx) + gp_ddiv((P[1][2][a] - P[0][2][a]), m.dx));
   }
   // j_at on the four faces; the y-face at ghosted row MESH_Y-2 carries none
   // (calculate_fluxes_concentration.h:65), i.e. interior row my-5
@@ -768,16 +780,16 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ gp_model
       const double Dxb = (Dcc + Dcell<N, K1>(m, P[0][1], k, l)) * 0.5;
       const double Dy = (Dcell<N, K1>(m, P[1][2], k, l) + Dcc) * 0.5;
       const double Dyl = (Dcc + Dcell<N, K1>(m, P[1][0], k, l)) * 0.5;
-      const double gmx = (Mf[l] - Mc[l]) / m.dx;
-      const double gmxb = (Mc[l] - Mb[l]) / m.dx;
-      const double gmy = (Mr[l] - Mc[l]) / m.dy;
-      const double gmyl = (Mc[l] - Ml[l]) / m.dy;
-      divflux[k] += (Dx * gmx - Dxb * gmxb) / m.dx;
-      divflux[k] += (Dy * gmy - Dyl * gmyl) / m.dy;
+      const double gmx = gp_ddiv((Mf[l] - Mc[l]), m.dx);
+      const double gmxb = gp_ddiv((Mc[l] - Mb[l]), m.dx);
+      const double gmy = gp_ddiv((Mr[l] - Mc[l]), m.dy);
+      const double gmyl = gp_ddiv((Mc[l] - Ml[l]), m.dy);
+      divflux[k] += gp_ddiv((Dx * gmx - Dxb * gmxb), m.dx);
+      divflux[k] += gp_ddiv((Dy * gmy - Dyl * gmyl), m.dy);
     }
     if (!SMOOTH) {
-      divjat[k] = (jx_c[k] - jx_b[k]) * (jscale) / m.dx;
-      divjat[k] += (jy_c[k] - jy_l[k]) * (jscale) / m.dy;
+      divjat[k] = gp_ddiv((jx_c[k] - jx_b[k]) * (jscale), m.dx);
+      divjat[k] += gp_ddiv((jy_c[k] - jy_l[k]) * (jscale), m.dy);
     }
   }
   int bulk = -1;

@@ -3,7 +3,7 @@
 
     python -m microsim_b200.profile_step [--workload c4|c2|c1] [--state FILE]
                                          [--tile TX TY] [--steps S] [--full]
-                                         [--depth 1|2] [--lean-per-sm L]
+                                         [--depth 1|2] [--lean-per-sm L] [--fp64]
 
 The workload's state is first advanced as the benchmark does (the batched
 sweep 2,500 steps, the 1024^2 dendrite 25,000, the 200^2 seed 5,000); with
@@ -11,7 +11,8 @@ sweep 2,500 steps, the 1024^2 dendrite 25,000, the 200^2 seed 5,000); with
 later ones, so a profiled run launches only a handful of kernels before the
 range.  --full switches the narrow band off (every tile through the full
 kernel); --depth 2 steps in blocked pairs (two steps per lean box);
---lean-per-sm sets the lean grid's blocks per SM (0: occupancy).
+--lean-per-sm sets the lean grid's blocks per SM (0: occupancy); --fp64
+profiles the plain FP64 step of the workload's first instance instead.
 """
 from __future__ import annotations
 
@@ -34,6 +35,7 @@ def main(argv=None):
     ap.add_argument("--full", action="store_true")
     ap.add_argument("--depth", type=int, default=1, choices=[1, 2])
     ap.add_argument("--lean-per-sm", type=int, default=0)
+    ap.add_argument("--fp64", action="store_true")
     a = ap.parse_args(argv)
     cases = {"c4": configs.c4, "c2": lambda: [configs.c2(literal=False, steps=50000)],
              "c1": lambda: [configs.c1(literal=False, steps=10000)]}[a.workload]()
@@ -52,6 +54,18 @@ def main(argv=None):
         if a.state:
             np.savez(a.state, **{f"p{i}": f[0] for i, f in enumerate(fields)},
                      **{f"u{i}": f[1] for i, f in enumerate(fields)})
+    if a.fp64:
+        with mb.Context(models[0], mb.GP_FP64) as c:
+            c.upload(*fields[0])
+            c.step(3)
+            c.sync()
+            torch.cuda.nvtx.range_push("profile")
+            c.step(a.steps)
+            c.sync()
+            torch.cuda.nvtx.range_pop()
+        print(f"profiled {a.steps} FP64 steps of {a.workload} instance 0 "
+              f"({models[0].mesh_x}x{models[0].mesh_y})")
+        return
     with mb.Batch(models) as b:
         b.set_tile(*a.tile)
         b.set_narrowband(not a.full)

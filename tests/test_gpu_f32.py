@@ -169,6 +169,19 @@ def test_tip_velocity_within_half_percent_of_fp64():
     assert r["solute_rel_diff"] <= 1e-4
 
 
+def test_batched_sweep_subset_within_half_percent_of_fp64():
+    """A 32-instance sub-sweep of the batched-sweep workload (sides 128..512, uneven
+    parameters), 1,000 steps: every instance's FP32 tip velocity within 0.5% of the FP64
+    plain form's, solute mass within 1e-4 (the full 256 x 5,000-step run:
+    python -m microsim_b200.validate --workload c4)."""
+    from microsim_b200 import validate
+    r = validate.compare("c4", steps=1000, every=100, instances=32)
+    assert r["instances"] == 32
+    assert r["nonfinite_max"] == 0
+    assert r["tip_velocity_rel_err_max"] <= 5e-3, r
+    assert r["solute_rel_diff_max"] <= 1e-4, r
+
+
 def test_narrow_band_is_bit_identical_to_the_full_kernel():
     """Tiles sent to the lean pure-phase kernel get the same bits as from the
     full kernel, for every tile shape: Neumann borders (mirrored rings), a
