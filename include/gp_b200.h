@@ -288,6 +288,11 @@ int gp_batch_kernel_ms(gp_batch *b, double *ms3, int64_t *steps);
  * per batch signature, read back on the next call. */
 int gp_batch_autotune(gp_batch *b, const char *cache_path, int *tx, int *ty);
 void *gp_batch_stream(gp_batch *b);
+/* The current state buffers of instance i on the device (FP32: esize 4), as
+ * gp_state_device; after writing into them (halo rows of a grid split across
+ * GPUs), call gp_batch_state_changed, which is ordered on the batch's stream. */
+int gp_batch_state_device(gp_batch *b, int i, void **phi, void **mu, int64_t *pitch, int64_t *plane, int *esize);
+int gp_batch_state_changed(gp_batch *b);
 int64_t gp_batch_launch_count(const gp_batch *b);
 int64_t gp_batch_cells(const gp_batch *b);
 

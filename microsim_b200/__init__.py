@@ -120,6 +120,9 @@ _SIGS = {
     "gp_batch_set_scan": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_batch_get_scan": (C.c_int, [C.c_void_p]),
     "gp_batch_set_depth": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_batch_state_device": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
+    "gp_batch_state_changed": (C.c_int, [C.c_void_p]),
     "gp_batch_get_depth": (C.c_int, [C.c_void_p]),
     "gp_batch_test_lose_box": (C.c_int, [C.c_void_p]),
     "gp_batch_get_grids": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -302,21 +305,10 @@ class Context:
     def device_state(self):
         """(phi, mu) torch views [planes, mesh_x, pitch] of the current device
         buffers (valid until the next step); call state_changed() after writing."""
-        import torch
         ph, mu_, pitch, plane, es = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int64(), C.c_int()
         _check("gp_state_device", lib().gp_state_device(self._h, C.byref(ph), C.byref(mu_), C.byref(pitch),
                                                           C.byref(plane), C.byref(es)))
-        typestr = "<f8" if es.value == 8 else "<f4"
-        mx = int(self.model.mesh_x)
-
-        class _View:
-            def __init__(self, ptr, planes):
-                self.__cuda_array_interface__ = {"shape": (planes, mx, pitch.value), "typestr": typestr,
-                                                 "data": (ptr, False), "version": 3,
-                                                 "strides": (plane.value * es.value, pitch.value * es.value,
-                                                             es.value)}
-        return (torch.as_tensor(_View(ph.value, int(self.model.N)), device="cuda"),
-                torch.as_tensor(_View(mu_.value, int(self.model.K1)), device="cuda"))
+        return _device_views(self.model, ph.value, mu_.value, pitch.value, plane.value, es.value)
 
     def state_changed(self):
         _check("gp_state_changed", lib().gp_state_changed(self._h))
@@ -348,6 +340,21 @@ class Context:
     @property
     def launches(self) -> int:
         return lib().gp_launch_count(self._h)
+
+
+def _device_views(model, ph: int, mu: int, pitch: int, plane: int, esize: int):
+    """torch views [planes, mesh_x, pitch] of a state's phi and mu device buffers."""
+    import torch
+    typestr = "<f8" if esize == 8 else "<f4"
+    mx = int(model.mesh_x)
+
+    class _View:
+        def __init__(self, ptr, planes):
+            self.__cuda_array_interface__ = {"shape": (planes, mx, pitch), "typestr": typestr,
+                                             "data": (ptr, False), "version": 3,
+                                             "strides": (plane * esize, pitch * esize, esize)}
+    return (torch.as_tensor(_View(ph, int(model.N)), device="cuda"),
+            torch.as_tensor(_View(mu, int(model.K1)), device="cuda"))
 
 
 def _stats_dict(st: GpStats, N: int, K1: int) -> dict:
@@ -432,6 +439,17 @@ class Batch:
 
     def scan(self) -> bool:
         return bool(lib().gp_batch_get_scan(self._h))
+
+    def device_state(self, i: int):
+        """(phi, mu) torch views [planes, mesh_x, pitch] of instance i's current
+        device buffers (valid until the next step); call state_changed() after writing."""
+        ph, mu_, pitch, plane, es = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int64(), C.c_int()
+        _check("gp_batch_state_device", lib().gp_batch_state_device(self._h, i, C.byref(ph), C.byref(mu_),
+                                                                      C.byref(pitch), C.byref(plane), C.byref(es)))
+        return _device_views(self.models[i], ph.value, mu_.value, pitch.value, plane.value, es.value)
+
+    def state_changed(self):
+        _check("gp_batch_state_changed", lib().gp_batch_state_changed(self._h))
 
     def set_depth(self, depth: int):
         """Temporal blocking: 1 (single steps) or 2 (blocked pairs; narrow band in list mode)."""

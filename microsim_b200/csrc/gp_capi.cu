@@ -1253,6 +1253,24 @@ extern "C" int gp_batch_kernel_ms(gp_batch* b, double* ms3, int64_t* steps) {
 }
 
 extern "C" void* gp_batch_stream(gp_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+extern "C" int gp_batch_state_device(gp_batch* b, int i, void** phi, void** mu, int64_t* pitch, int64_t* plane,
+                                     int* esize) {
+  if (!b || i < 0 || i >= b->n || !phi || !mu || !pitch || !plane || !esize) return GP_E_ARG;
+  *phi = b->pool + b->off_phi[b->parity][i];
+  *mu = b->pool + b->off_mu[b->parity][i];
+  *pitch = b->pitch[i];
+  *plane = b->plane[i];
+  *esize = 4;
+  return GP_OK;
+}
+
+extern "C" int gp_batch_state_changed(gp_batch* b) {
+  if (!b) return GP_E_ARG;
+  b->have_prev = 0;
+  GP_CUDA(gp_f32_batch_invalidate(b->f32, b->stream));  // stream-ordered: purity words back to "unknown"
+  return GP_OK;
+}
 extern "C" int64_t gp_batch_launch_count(const gp_batch* b) { return b ? b->launches : 0; }
 extern "C" int64_t gp_batch_cells(const gp_batch* b) {
   int64_t c = 0;

@@ -15,9 +15,10 @@ outside [0, M) (periodic x) come from the partner of the reference's periodic
 copy, period M - 1 (microsim_b200/csrc/gp_common.cuh gp_map).
 
 The exchange is written against a small transport: `numpy` (host arrays of a
-process group over torch.distributed: gloo on the CPU, for the oracle) or
-`torch` device tensors (NCCL between GPUs, or local copies when the slabs of
-one process share a GPU).
+process group over torch.distributed: gloo on the CPU, for the oracle), or
+torch tensors (exchange_tensors: NCCL between GPUs, ordered on the stepping
+context's stream with no host synchronisation; the same code on host tensors
+over gloo), or local device copies when the slabs of one process share a GPU.
 """
 from __future__ import annotations
 
@@ -141,51 +142,93 @@ def exchange_numpy(fields, copies, rank: int, world: int):
                 o += n
 
 
+def exchange_tensors(phi, mu, copies, rank: int, stream=None):
+    """Halo rows of one rank's state given as tensors phi [P, rows, ny], mu [Q,
+    rows, ny] (device or host) over torch.distributed: local copies, then one
+    batch of sends and receives per partner (rows packed [phi planes, mu planes]
+    in the order blocks() fixes on both sides), then the received rows
+    unpacked.  With `stream` (a CUDA stream: the stepping context's own), every
+    operation is ordered on it and the host never waits: the NCCL work is
+    joined to the stream (Work.wait() makes the stream, not the host, wait), so
+    the next step launched on that stream sees the new rows.  On host tensors
+    (gloo) the same code runs synchronously."""
+    import contextlib
+    import torch
+    import torch.distributed as dist
+    sends, recvs, local = blocks(copies, rank)
+    P, Q, ny = phi.shape[0], mu.shape[0], phi.shape[2]
+    ctx = torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()
+    with ctx:
+        for (srow, drow) in local:
+            phi[:, drow].copy_(phi[:, srow])
+            mu[:, drow].copy_(mu[:, srow])
+        ops, bufs = [], []
+        for partner in sorted(set(sends) | set(recvs)):
+            if partner in sends:
+                rows = [r for (r, _) in sends[partner]]
+                ops.append(dist.P2POp(dist.isend, torch.cat([phi[:, rows].reshape(-1), mu[:, rows].reshape(-1)]),
+                                      partner))
+            if partner in recvs:
+                t = torch.empty((P + Q) * len(recvs[partner]) * ny, dtype=phi.dtype, device=phi.device)
+                ops.append(dist.P2POp(dist.irecv, t, partner))
+                bufs.append((partner, t))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        for partner, t in bufs:
+            rows = [d for (_, d) in recvs[partner]]
+            n = len(rows)
+            phi[:, rows] = t[: P * n * ny].reshape(P, n, ny)
+            mu[:, rows] = t[P * n * ny:].reshape(Q, n, ny)
+
+
 def exchange_local(ctxs, copies):
     """Halo rows between contexts of one process (the slabs share the GPU):
-    device-to-device copies of whole rows."""
+    device-to-device copies of whole rows, ordered on the GPU (every context's
+    stream is joined into one copy stream and waits on it afterwards; the host
+    does not wait)."""
     import torch
-    for c in ctxs:
-        c.sync()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    streams = [torch.cuda.ExternalStream(c.stream, device=dev) for c in ctxs]
+    cs = torch.cuda.current_stream(dev)
+    for s in streams:
+        ev = torch.cuda.Event()
+        ev.record(s)
+        cs.wait_event(ev)
     views = [c.device_state() for c in ctxs]
-    for (sr, srow, dr, drow) in copies:
-        for k in range(2):  # phi planes, mu planes
-            views[dr][k][:, drow].copy_(views[sr][k][:, srow])
-    torch.cuda.synchronize()
-    for c in ctxs:
+    with torch.cuda.stream(cs):
+        for (sr, srow, dr, drow) in copies:
+            for k in range(2):  # phi planes, mu planes
+                views[dr][k][:, drow].copy_(views[sr][k][:, srow])
+    done = torch.cuda.Event()
+    done.record(cs)
+    for s, c in zip(streams, ctxs):
+        s.wait_event(done)
         c.state_changed()
 
 
-def exchange_nccl(ctx, copies, rank: int):
-    """Halo rows of this rank's context with the other ranks (torch.distributed
-    over NCCL; one process per GPU, the context created after
-    microsim_b200.set_device(local rank))."""
+def exchange_nccl(ctx, copies, rank: int, index: int | None = None):
+    """Halo rows of this rank's state with the other ranks (torch.distributed
+    over NCCL; one process per GPU, the context or batch created after
+    microsim_b200.set_device(local rank)), stream-ordered on the context's (or
+    the batch's) own stream: no host synchronisation.  `ctx` is a Context, or a
+    Batch with `index` the instance holding this rank's slab."""
     import torch
-    import torch.distributed as dist
-    ctx.sync()
-    phi, mu = ctx.device_state()
-    sends, recvs, local = blocks(copies, rank)
-    for (srow, drow) in local:
-        phi[:, drow].copy_(phi[:, srow])
-        mu[:, drow].copy_(mu[:, srow])
-    ops, bufs = [], []
-    for partner in sorted(set(sends) | set(recvs)):
-        if partner in sends:
-            rows = [s for (s, _) in sends[partner]]
-            t = torch.cat([phi[:, rows].reshape(-1), mu[:, rows].reshape(-1)])
-            ops.append(dist.P2POp(dist.isend, t, partner))
-        if partner in recvs:
-            n = len(recvs[partner])
-            t = torch.empty((phi.shape[0] + mu.shape[0]) * n * phi.shape[2], dtype=phi.dtype, device=phi.device)
-            ops.append(dist.P2POp(dist.irecv, t, partner))
-            bufs.append((partner, t))
-    if ops:
-        for req in dist.batch_isend_irecv(ops):
-            req.wait()
-    for partner, t in bufs:
-        rows = [d for (_, d) in recvs[partner]]
-        n, P, Q = len(rows), phi.shape[0], mu.shape[0]
-        phi[:, rows] = t[: P * n * phi.shape[2]].reshape(P, n, phi.shape[2])
-        mu[:, rows] = t[P * n * phi.shape[2]:].reshape(Q, n, mu.shape[2])
-    torch.cuda.synchronize()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    phi, mu = ctx.device_state() if index is None else ctx.device_state(index)
+    exchange_tensors(phi, mu, copies, rank, stream=torch.cuda.ExternalStream(ctx.stream, device=dev))
     ctx.state_changed()
+
+
+def exchange_batch_local(batch, copies):
+    """Halo rows between the instances of one batch (instance r holds slab r; one
+    GPU): device copies ordered on the batch's own stream (no host wait), then
+    the batch's purity words reset (also on its stream)."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    views = [batch.device_state(i) for i in range(len(batch.models))]
+    with torch.cuda.stream(torch.cuda.ExternalStream(batch.stream, device=dev)):
+        for (sr, srow, dr, drow) in copies:
+            for k in range(2):  # phi planes, mu planes
+                views[dr][k][:, drow].copy_(views[sr][k][:, srow])
+    batch.state_changed()

@@ -58,3 +58,31 @@ def test_slabs_equal_the_single_grid(name, world, depth, precision):
     finally:
         for c in ctxs:
             c.close()
+
+
+@pytest.mark.parametrize("depth_blocking", [1, 2])
+def test_slabs_as_instances_of_one_fp32_batch(depth_blocking):
+    """The slabs as the instances of one FP32 batch (narrow band, temporal blocking of
+    the given depth inside the batch), halo rows exchanged on the batch's stream every
+    `depth` steps with no host wait: owned rows equal the single-grid FP32 run."""
+    m, phi, mu = _case("corner_96x64")
+    steps, depth, world = 24, 2, 3
+    with mb.Context(m, mb.GP_FP32) as c:
+        c.upload(phi, mu)
+        c.step(steps)
+        gp, gu = c.download()
+    mx, bc_x = int(m.mesh_x), int(m.bc_phi[0])
+    slabs, copies = S.plan(mx, world, bc_x, depth)
+    with mb.Batch([S.local_model(m, s) for s in slabs]) as b:
+        b.set_depth(depth_blocking)
+        for i, s in enumerate(slabs):
+            rows = [S.gmap(g, mx, bc_x) if (g < 0 or g >= mx) else g for g in range(s.lo, s.hi)]
+            b.upload(i, np.ascontiguousarray(phi[:, rows]), np.ascontiguousarray(mu[:, rows]))
+        for _ in range(steps // depth):
+            b.step(depth)
+            S.exchange_batch_local(b, copies)
+        for i, s in enumerate(slabs):
+            p, u = b.download(i)
+            own = slice(s.own_lo - s.lo, s.own_hi - s.lo)
+            assert np.array_equal(p[:, own], gp[:, s.own_lo:s.own_hi]), (s.rank, np.abs(p[:, own] - gp[:, s.own_lo:s.own_hi]).max())
+            assert np.array_equal(u[:, own], gu[:, s.own_lo:s.own_hi])

@@ -1,6 +1,8 @@
 """One grid split into x-slabs on two gloo ranks (CPU, the oracle as the
 stepper): owned rows after every exchange equal the single-grid run bit for
-bit, for Neumann and periodic x boundaries and halo depths 1 and 2."""
+bit, for Neumann and periodic x boundaries and halo depths 1 and 2, through the
+host-array exchange and through exchange_tensors (the code the GPUs run on
+their contexts' streams over NCCL, here on host tensors over gloo)."""
 import copy
 import multiprocessing as mp
 import os
@@ -31,7 +33,7 @@ def _local_state(gphi, gmu, slab, mx, bc_x):
     return lp, lu
 
 
-def _worker(rank, world, port, case, depth, steps, q):
+def _worker(rank, world, port, case, depth, steps, q, transport="numpy"):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -58,7 +60,11 @@ def _worker(rank, world, port, case, depth, steps, q):
         while done < steps:
             O.step(lm, lp, lu, depth)
             done += depth
-            S.exchange_numpy([lp[:, 3:-3], lu[:, 3:-3]], copies, rank, world)
+            if transport == "numpy":
+                S.exchange_numpy([lp[:, 3:-3], lu[:, 3:-3]], copies, rank, world)
+            else:
+                import torch
+                S.exchange_tensors(torch.from_numpy(lp[:, 3:-3]), torch.from_numpy(lu[:, 3:-3]), copies, rank)
             O.apply_bc(lm, lp, lu)
         own = slice(3 + s.own_lo - s.lo, 3 + s.own_hi - s.lo)
         q.put((rank, s.own_lo, s.own_hi, lp[:, own, 3:-3].copy(), lu[:, own, 3:-3].copy()))
@@ -69,8 +75,11 @@ def _worker(rank, world, port, case, depth, steps, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("case,depth", [("iso_obst_bin", 1), ("iso_obst_bin", 2), ("aniso_obst_bin_per", 1)])
-def test_slabs_on_two_gloo_ranks_equal_the_single_grid(case, depth):
+@pytest.mark.parametrize("case,depth,transport", [("iso_obst_bin", 1, "numpy"), ("iso_obst_bin", 2, "numpy"),
+                                                   ("aniso_obst_bin_per", 1, "numpy"),
+                                                   ("iso_obst_bin", 2, "tensors"),
+                                                   ("aniso_obst_bin_per", 1, "tensors")])
+def test_slabs_on_two_gloo_ranks_equal_the_single_grid(case, depth, transport):
     from conftest import load_golden, oracle_model
     from oracle import gp_oracle as O
     steps = 12
@@ -81,7 +90,7 @@ def test_slabs_on_two_gloo_ranks_equal_the_single_grid(case, depth):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    ps = [ctx.Process(target=_worker, args=(r, 2, port, case, depth, steps, q)) for r in range(2)]
+    ps = [ctx.Process(target=_worker, args=(r, 2, port, case, depth, steps, q, transport)) for r in range(2)]
     for p in ps:
         p.start()
     out = [q.get(timeout=180) for _ in ps]
