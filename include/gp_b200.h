@@ -105,6 +105,22 @@ typedef struct gp_model {
   /* mu of the liquid rows a moving-frame shift appends: Mu(cfill of the liquid)
    * at Filling_temperature (functions/shift.h:24-37) */
   double mu_shift[GP_MAX_K1];
+  /* Non-isothermal frozen gradient (ISOTHERMAL = 0: Tempgrady; microsim_gp.c:77-82, 108-113,
+   * functions/Temperature_gradient.h:4-29): after every step the temperature of ghost-padded row gy
+   * is T = temp_bottom + gy * GRADIENT, GRADIENT = DeltaT * dy / Distance, temp_bottom = base_temp -
+   * BASE_POS * GRADIENT, BASE_POS = gradient_OFFSET / dy + (velocity / dy) * (t * dt).  The cell's T
+   * enters c(mu, T) and mu(c, T) through Beq + dBbdT (T - Teq), and B(T), C(T) of the free energies
+   * (functions/functionF_01.h:62-104, with the constants below). */
+  int32_t nonisothermal; /* 1: ISOTHERMAL = 0 (T above is then only the filling's) */
+  int32_t bc_T[4];       /* boundary copy of T (x-lo, x-hi, y-hi, y-lo): 1 Neumann, 3 periodic, 0 none (ghosts keep the linear T) */
+  int32_t pad1;
+  double tg_base, tg_deltaT, tg_distance, tg_offset, tg_velocity; /* Tempgrady = {base_temp, DeltaT, Distance, gradient_OFFSET, velocity} */
+  double Beq[GP_MAX_PHASES][GP_MAX_K1];   /* B(Teq)                                         */
+  double dBbdT[GP_MAX_PHASES][GP_MAX_K1]; /* dB/dT                                          */
+  double ceq_s[GP_MAX_PHASES][GP_MAX_K1]; /* ceq[a][a][k]                                   */
+  double ceq_l[GP_MAX_PHASES][GP_MAX_K1]; /* ceq[a][N-1][k]                                 */
+  double dC[GP_MAX_PHASES][GP_MAX_K1];    /* DELTA_C[a][k]                                  */
+  double dT_s[GP_MAX_PHASES], dT_l[GP_MAX_PHASES]; /* DELTA_T[a][a], DELTA_T[a][N-1]        */
 } gp_model;
 
 /* Parsed Input.in (+ its BOUNDARY lines) and Filling.in. */
@@ -114,7 +130,8 @@ typedef struct gp_input gp_input;
 typedef struct gp_stats {
   double phi_max[GP_MAX_PHASES], phi_min[GP_MAX_PHASES], rel_change_phi[GP_MAX_PHASES];
   double mu_max[GP_MAX_K1], mu_min[GP_MAX_K1], rel_change_mu[GP_MAX_K1];
-  double solute[GP_MAX_K1]; /* sum over cells of sum_a c_a(mu) h_a(phi) (file_writer.h:203-235 integrand) */
+  double solute[GP_MAX_K1]; /* sum over cells of sum_a c_a(mu, T) h_a(phi) (file_writer.h:203-235 integrand; T the
+                               cell's current one under a frozen gradient) */
   double phase_fraction[GP_MAX_PHASES]; /* sum over cells of phi_a                                      */
   int64_t nonfinite;  /* number of non-finite phi/mu values found                                         */
   /* Energies of the current state, FP64 sums over the interior cells times dx*dy.  The reference
@@ -156,6 +173,10 @@ int gp_fill(const gp_input *in, const gp_model *m, double *phi, double *mu);
 /* Write DATA/<out>_<t>.vtk (solverloop/file_writer.h:23-255), BINARY or ASCII
  * as Input.in's WRITEFORMAT says; Composition_* fields when Writecomposition. */
 int gp_write_vtk(const gp_input *in, const gp_model *m, const char *path, const double *phi, const double *mu);
+/* The same after time step tstep: for a non-isothermal model the Temperature field (and the
+ * Composition fields) use the frozen gradient's temperature after that step. */
+int gp_write_vtk_t(const gp_input *in, const gp_model *m, const char *path, const double *phi, const double *mu,
+                   int64_t tstep);
 /* Read fields back (solverloop/file_writer.h:256-386, restart). */
 int gp_read_vtk(const gp_input *in, const gp_model *m, const char *path, double *phi, double *mu);
 
@@ -175,6 +196,9 @@ int gp_download(gp_ctx *ctx, double *phi, double *mu);
  * Asynchronous on the context's stream; errors of earlier launches surface here
  * or in gp_sync. */
 int gp_step(gp_ctx *ctx, int64_t nsteps);
+/* The context's step count (the frozen temperature gradient's clock: step t uses the temperature
+ * the reference sets after step t - 1).  Starts at 0 on creation; gp_step advances it. */
+int gp_set_time_step(gp_ctx *ctx, int64_t t);
 /* nsteps smoothing pre-steps (the reference runs NSMOOTH - 1 of them before its
  * time loop, microsim_gp.c:97-100; solverloop.h:72-90): the phase-field step
  * without the driving force and with isotropic gradient energy, the

@@ -55,6 +55,12 @@ class GpModel(C.Structure):
         ("inv_eps", C.c_double), ("w_obstacle", C.c_double), ("jat_obst", C.c_double),
         ("jat_well", C.c_double), ("s_well", C.c_double),
         ("mu_shift", C.c_double * _K),
+        ("nonisothermal", C.c_int32), ("bc_T", C.c_int32 * 4), ("pad1", C.c_int32),
+        ("tg_base", C.c_double), ("tg_deltaT", C.c_double), ("tg_distance", C.c_double),
+        ("tg_offset", C.c_double), ("tg_velocity", C.c_double),
+        ("Beq", C.c_double * (_P * _K)), ("dBbdT", C.c_double * (_P * _K)),
+        ("ceq_s", C.c_double * (_P * _K)), ("ceq_l", C.c_double * (_P * _K)), ("dC", C.c_double * (_P * _K)),
+        ("dT_s", C.c_double * _P), ("dT_l", C.c_double * _P),
     ]
 
     def arr(self, name):
@@ -92,6 +98,8 @@ _SIGS = {
     "gp_model_from_input": (C.c_int, [C.c_void_p, C.POINTER(GpModel)]),
     "gp_fill": (C.c_int, [C.c_void_p, C.POINTER(GpModel), C.c_void_p, C.c_void_p]),
     "gp_write_vtk": (C.c_int, [C.c_void_p, C.POINTER(GpModel), C.c_char_p, C.c_void_p, C.c_void_p]),
+    "gp_write_vtk_t": (C.c_int, [C.c_void_p, C.POINTER(GpModel), C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
+    "gp_set_time_step": (C.c_int, [C.c_void_p, C.c_int64]),
     "gp_read_vtk": (C.c_int, [C.c_void_p, C.POINTER(GpModel), C.c_char_p, C.c_void_p, C.c_void_p]),
     "gp_create": (C.c_int, [C.POINTER(GpModel), C.c_int, C.POINTER(C.c_void_p)]),
     "gp_destroy": (C.c_int, [C.c_void_p]),
@@ -241,10 +249,13 @@ class Input:
         _check("gp_fill", lib().gp_fill(self._h, C.byref(m), _ptr(phi), _ptr(mu)))
         return phi, mu
 
-    def write_vtk(self, m: GpModel, path: str, phi: np.ndarray, mu: np.ndarray):
+    def write_vtk(self, m: GpModel, path: str, phi: np.ndarray, mu: np.ndarray, tstep: int = 0):
+        """DATA/<out>_<t>.vtk as the reference writes it; tstep: the step the fields are after (the
+        frozen gradient's temperature of a non-isothermal model)."""
         phi = np.ascontiguousarray(phi, dtype=np.float64)  # held: the C call reads them
         mu = np.ascontiguousarray(mu, dtype=np.float64)
-        _check("gp_write_vtk", lib().gp_write_vtk(self._h, C.byref(m), path.encode(), _ptr(phi), _ptr(mu)))
+        _check("gp_write_vtk_t", lib().gp_write_vtk_t(self._h, C.byref(m), path.encode(), _ptr(phi), _ptr(mu),
+                                                        int(tstep)))
 
     def read_vtk(self, m: GpModel, path: str):
         phi = np.zeros((m.N, m.mesh_x, m.mesh_y))

@@ -96,6 +96,10 @@ class Case:
     components: list = field(default_factory=list)
     writeformat: str = "BINARY"
     writecomposition: int = 0
+    # frozen temperature gradient (ISOTHERMAL = 0): (base_temp, DeltaT, Distance, gradient_OFFSET,
+    # velocity) and the temperature's boundary types (X+, X-, Y+, Y-); None: isothermal
+    tempgrady: tuple | None = None
+    bc_T: tuple | None = None
     fills: list = field(default_factory=list)                  # ("FILLCYLINDER", [..]) ...
 
     def input_text(self) -> str:
@@ -125,11 +129,16 @@ class Case:
         for d in self.diffusivity:
             L.append(f"DIFFUSIVITY = {brace(d)};")
         L += ["R = 1.0;", "V = 1.0;"]
-        for name, t in (("phi", self.bc_phi), ("mu", self.bc_mu), ("c", self.bc_mu), ("T", self.bc_mu)):
+        for name, t in (("phi", self.bc_phi), ("mu", self.bc_mu), ("c", self.bc_mu),
+                        ("T", self.bc_T or self.bc_mu)):
             L.append("BOUNDARY = {" + name + "," + ",".join(str(v) for v in t) + ",0,0};")
         for name in ("phi", "mu", "c", "T"):
             L.append("BOUNDARY_VALUE = {" + name + ",0,0,0,0,0,0};")
-        L.append("ISOTHERMAL = 1;")
+        if self.tempgrady is None:
+            L.append("ISOTHERMAL = 1;")
+        else:
+            L.append("ISOTHERMAL = 0;")
+            L.append(f"Tempgrady = {brace(self.tempgrady)};")
         if self.solver:
             L.append(f"{self.solver} = 1;")
         L += [

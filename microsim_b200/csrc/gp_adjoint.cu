@@ -527,6 +527,10 @@ extern "C" int gp_adj_create(const gp_model* m, int precision, gp_adj** out) {
     return GP_E_UNSUPPORTED;
   }
   if (m->mesh_x < 4 || m->mesh_y < 4) return GP_E_ARG;
+  if (m->nonisothermal) {
+    gp_set_error("adjoint: isothermal models only");
+    return GP_E_UNSUPPORTED;
+  }
   gp_adj* a = new gp_adj();
   int rc;
   if (precision == GP_FP32) {

@@ -19,7 +19,8 @@
 extern "C" void gp_set_error(const char* fmt, ...);
 
 cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch, int64_t rplane, const double* phi,
-                        const double* mu, double* dphi, double* phi_out, double* mu_out, cudaStream_t s, bool smooth = false, const double* ghost_rows = nullptr);
+                        const double* mu, double* dphi, double* phi_out, double* mu_out, cudaStream_t s, bool smooth = false, const double* ghost_rows = nullptr,
+                        const gp_temp_step* temp = nullptr);
 struct gp_f32_batch;
 int gp_f32_supported(const gp_model& m);
 cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** out);
@@ -111,6 +112,7 @@ struct gp_ctx {
   double* reduced;   // statistics: final values (device)
   int red_blocks;
   int64_t launches;
+  int64_t tstep = 0;  // steps taken (the frozen gradient's clock)
   // running extrema (microsim_gp.c prints running values since t = 0)
   double run_phi_max[GP_MAX_PHASES], run_phi_min[GP_MAX_PHASES];
   double run_mu_max[GP_MAX_K1], run_mu_min[GP_MAX_K1];
@@ -313,9 +315,10 @@ extern "C" int gp_step(gp_ctx* c, int64_t nsteps) {
   for (int64_t t = 0; t < nsteps; t++) {
     const int nxt = 1 - c->cur;
     if (c->precision == GP_FP64) {
+      const gp_temp_step ts = gp_temp_after(c->m, c->tstep);  // T reset after the previous step
       GP_CUDA(gp_f64_step(c->m, c->pitch, c->plane, c->rpitch, c->rplane, (const double*)c->phi[c->cur],
                           (const double*)c->mu[c->cur], c->dphi, (double*)c->phi[nxt], (double*)c->mu[nxt],
-                          c->stream, false, c->gov_pending ? c->gov : nullptr));
+                          c->stream, false, c->gov_pending ? c->gov : nullptr, &ts));
       c->gov_pending = 0;
       c->launches += 2;
     } else {
@@ -324,7 +327,14 @@ extern "C" int gp_step(gp_ctx* c, int64_t nsteps) {
     }
     c->cur = nxt;
     c->have_prev = 1;
+    c->tstep++;
   }
+  return GP_OK;
+}
+
+extern "C" int gp_set_time_step(gp_ctx* c, int64_t t) {
+  if (!c || t < 0) return GP_E_ARG;
+  c->tstep = t;
   return GP_OK;
 }
 
@@ -334,9 +344,10 @@ extern "C" int gp_smooth(gp_ctx* c, int64_t nsteps) {
   if (c->precision == GP_FP64) {
     for (int64_t t = 0; t < nsteps; t++) {
       const int nxt = 1 - c->cur;
+      const gp_temp_step ts = gp_temp_after(c->m, 0);  // pre-steps: the initial temperature, ghosts copied
       GP_CUDA(gp_f64_step(c->m, c->pitch, c->plane, c->rpitch, c->rplane, (const double*)c->phi[c->cur],
                           (const double*)c->mu[c->cur], c->dphi, (double*)c->phi[nxt], (double*)c->mu[nxt],
-                          c->stream, true));
+                          c->stream, true, nullptr, c->m.nonisothermal ? &ts : nullptr));
       c->launches += 2;
       c->cur = nxt;
     }
@@ -560,7 +571,7 @@ __device__ __forceinline__ double stat_ac(double dab, double q0, double q1) {
 // e[1] potential (with 1/eps), e[2] sum_a h_a f_a(c_a), e[3] sum_a h_a psi_a (psi_a = f_a - mu.c_a).
 template <typename T>
 __device__ void cell_energy(const gp_model& m, const T* __restrict__ phi, int pitch, int64_t plane, int x, int y,
-                            const double* ph, const double* mm, double* e) {
+                            const double* ph, const double* mm, double* e, Th th) {
   const int N = m.N, K1 = m.K1;
   double gx[GP_MAX_PHASES], gy[GP_MAX_PHASES];
   const int xm = gp_map(x - 1, (int)m.mesh_x, m.bc_phi[0]), xp = gp_map(x + 1, (int)m.mesh_x, m.bc_phi[0]);
@@ -592,14 +603,14 @@ __device__ void cell_energy(const gp_model& m, const T* __restrict__ phi, int pi
       for (int c = b + 1; c < N; c++)
         if (b != a && c != a) s1 += ph[b] * ph[c];
     h += 2.0 * ph[a] * s1;
-    double c[GP_MAX_K1], f = m.C[a], mc = 0.0;
+    double c[GP_MAX_K1], f = C_T(m, th, a), mc = 0.0;
     for (int k = 0; k < K1; k++) {
       c[k] = 0.0;
-      for (int l = 0; l < K1; l++) c[k] += m.cmu[a][k][l] * (mm[l] - m.Beff[a][l]);
+      for (int l = 0; l < K1; l++) c[k] += m.cmu[a][k][l] * (mm[l] - beff(m, th, a, l));
     }
     for (int k = 0; k < K1; k++) {
       for (int l = k; l < K1; l++) f += m.A[a][k][l] * c[k] * c[l];
-      f += m.B[a][k] * c[k];
+      f += B_T(m, th, k, a) * c[k];
       mc += mm[k] * c[k];
     }
     fch += h * f;
@@ -614,7 +625,8 @@ __device__ void cell_energy(const gp_model& m, const T* __restrict__ phi, int pi
 template <typename T>
 __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model m, const T* __restrict__ phi, const T* __restrict__ mu,
                                                const T* __restrict__ phi_prev, const T* __restrict__ mu_prev,
-                                               int have_prev, int pitch, int64_t plane, double* __restrict__ partials) {
+                                               int have_prev, int pitch, int64_t plane, double* __restrict__ partials,
+                                               gp_temp_step temp) {
   const StatLayout L{m.N, m.K1};
   const int S = L.count();
   double acc[kStatSlots];
@@ -646,11 +658,15 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
         acc[L.rel_mu(k)] += d * d;
       }
     }
+    // the cell's temperature: the frozen gradient's current one for a non-isothermal model
+    Th th;
+    th.on = m.nonisothermal;
+    th.T = m.nonisothermal ? temp.bottom + (double)(y + 3) * temp.grad : m.T;
     for (int k = 0; k < m.K1; k++) {
       double comp = 0.0;
       for (int a = 0; a < m.N; a++) {
         double cm = 0.0;
-        for (int l = 0; l < m.K1; l++) cm += m.cmu[a][k][l] * (mm[l] - m.Beff[a][l]);
+        for (int l = 0; l < m.K1; l++) cm += m.cmu[a][k][l] * (mm[l] - beff(m, th, a, l));
         double h = 3.0 * ph[a] * ph[a] - 2.0 * ph[a] * ph[a] * ph[a], s1 = 0.0;
         for (int b = 0; b < m.N; b++)
           for (int c = b + 1; c < m.N; c++)
@@ -661,7 +677,7 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
       acc[L.solute(k)] += comp;
     }
     double e[4];
-    cell_energy<T>(m, phi, pitch, plane, x, y, ph, mm, e);
+    cell_energy<T>(m, phi, pitch, plane, x, y, ph, mm, e, th);
     acc[L.energy(0)] += e[0];
     acc[L.energy(1)] += e[1];
     acc[L.energy(2)] += e[2];
@@ -709,14 +725,15 @@ extern "C" int gp_get_stats(gp_ctx* c, gp_stats* out) {
   if (!c || !out) return GP_E_ARG;
   const gp_model& m = c->m;
   const int cur = c->cur, prv = 1 - c->cur;
+  const gp_temp_step ts = gp_temp_after(m, c->tstep);  // the temperature after the last step
   if (c->precision == GP_FP64)
     k_stats<double><<<c->red_blocks, 256, 0, c->stream>>>(m, (const double*)c->phi[cur], (const double*)c->mu[cur],
                                                          (const double*)c->phi[prv], (const double*)c->mu[prv],
-                                                         c->have_prev, c->pitch, c->plane, c->partials);
+                                                         c->have_prev, c->pitch, c->plane, c->partials, ts);
   else
     k_stats<float><<<c->red_blocks, 256, 0, c->stream>>>(m, (const float*)c->phi[cur], (const float*)c->mu[cur],
                                                         (const float*)c->phi[prv], (const float*)c->mu[prv],
-                                                        c->have_prev, c->pitch, c->plane, c->partials);
+                                                        c->have_prev, c->pitch, c->plane, c->partials, ts);
   GP_CUDA(cudaGetLastError());
   k_stats_final<<<1, 64, 0, c->stream>>>(m.N, m.K1, c->partials, c->red_blocks, c->reduced,
                                          c->f32 ? gp_f32_batch_error_word(c->f32) : nullptr);
@@ -997,7 +1014,7 @@ extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
   const int cur = b->parity, prv = 1 - b->parity;
   k_stats<float><<<b->red_blocks, 256, 0, b->stream>>>(
       m, b->pool + b->off_phi[cur][i], b->pool + b->off_mu[cur][i], b->pool + b->off_phi[prv][i],
-      b->pool + b->off_mu[prv][i], b->have_prev, b->pitch[i], b->plane[i], b->partials);
+      b->pool + b->off_mu[prv][i], b->have_prev, b->pitch[i], b->plane[i], b->partials, gp_temp_after(m, 0));
   GP_CUDA(cudaGetLastError());
   k_stats_final<<<1, 64, 0, b->stream>>>(m.N, m.K1, b->partials, b->red_blocks, b->reduced,
                                          gp_f32_batch_error_word(b->f32));

@@ -2018,6 +2018,7 @@ static bool pick(int N, int K1, int an, int tx, int ty, KernelSet* k) {
 }
 
 int gp_f32_supported(const gp_model& m) {
+  if (m.nonisothermal) return 0;  // the FP32 kernels take the model's single temperature
   KernelSet k;
   return pick(m.N, m.K1, m.anisotropy, 16, 32, &k);
 }

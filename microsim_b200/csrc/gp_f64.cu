@@ -35,7 +35,29 @@ struct Geo {
   // step right after a moving-frame shift, which reads the shifted ghost rows
   // before the boundary copy refreshes them (microsim_gp.c:103-125).
   const double* gov;
+  // non-isothermal frozen gradient: T of ghost-padded row gy = t_bottom + gy * t_grad, for the
+  // step being computed; t_linear: the phase-field half step reads the ghost rows' own linear T
+  // (every step after the first: the reference resets T after the step's last boundary copy),
+  // else their boundary copy
+  int noniso, t_linear;
+  int bc_t;  // boundary copy of T along y: 1 Neumann, 3 periodic, 0 none
+  double t_bottom, t_grad;
 };
+
+
+// T of interior/ghost row y (interior coordinates) in the phase-field half step (linear ghosts, or
+// their boundary copy in the first step) or the concentration half step (boundary copy).
+__device__ __forceinline__ Th th_row(const gp_model& m, const Geo& g, int y, bool linear) {
+  Th t;
+  t.on = g.noniso;
+  if (!g.noniso) {
+    t.T = m.T;
+    return t;
+  }
+  const int yy = (linear || !g.bc_t || (y >= 0 && y < g.my)) ? y : gp_map(y, g.my, g.bc_t);
+  t.T = g.t_bottom + (double)(yy + 3) * g.t_grad;
+  return t;
+}
 
 __device__ __forceinline__ const double* ghost_row(const Geo& g, int x, int y, int xtype, int q) {
   const int slot = y < 0 ? y + 3 : y - g.my + 3;
@@ -105,36 +127,36 @@ __device__ __forceinline__ double dhphi(const double* phi, int b, int a) {
   return sum;
 }
 
-// c_a,i(mu), functions/functionF_01.h:30-37 (Beff = Beq + dBbdT (T - Teq))
+// c_a,i(mu, T), functions/functionF_01.h:30-37
 template <int K1>
-__device__ __forceinline__ double c_mu(const gp_model& m, const double* mu, int a, int i) {
+__device__ __forceinline__ double c_mu(const gp_model& m, Th t, const double* mu, int a, int i) {
   double sum = 0.0;
 #pragma unroll
-  for (int k = 0; k < K1; k++) sum += m.cmu[a][i][k] * (mu[k] - m.Beff[a][k]);
+  for (int k = 0; k < K1; k++) sum += m.cmu[a][i][k] * (mu[k] - beff(m, t, a, k));
   return sum;
 }
 
 // functions/functionF_01.h:19-29
 template <int K1>
-__device__ __forceinline__ double Mu(const gp_model& m, const double* c, int a, int i) {
-  double sum = 2.0 * m.A[a][i][i] * c[i] + m.Beff[a][i];
+__device__ __forceinline__ double Mu(const gp_model& m, Th t, const double* c, int a, int i) {
+  double sum = 2.0 * m.A[a][i][i] * c[i] + beff(m, t, a, i);
 #pragma unroll
   for (int j = 0; j < K1; j++)
     if (i != j) sum += m.A[a][i][j] * c[j];
   return sum;
 }
 
-// functions/functionF_01.h:5-18
-template <int K1>
-__device__ __forceinline__ double free_energy(const gp_model& m, const double* c, int a) {
+// functions/functionF_01.h:5-18, with B and C at the cell's T (init_propertymatrices(T))
+template <int N, int K1>
+__device__ __forceinline__ double free_energy(const gp_model& m, Th t, const double* c, int a) {
   double sum = 0.0;
 #pragma unroll
   for (int i = 0; i < K1; i++) {
 #pragma unroll
     for (int j = i; j < K1; j++) sum += m.A[a][i][j] * c[i] * c[j];
-    sum += m.B[a][i] * c[i];
+    sum += B_Tn<N, K1>(m, t, i, a) * c[i];
   }
-  sum += m.C[a];
+  sum += C_Tn<N, K1>(m, t, a);
   return sum;
 }
 
@@ -152,7 +174,7 @@ __device__ __forceinline__ double gp_ddiv(double x, double d) {
 }
 
 template <int N, int K1>
-__device__ __forceinline__ double dpsi(const gp_model& m, const double* mu, const double* phi, int a) {
+__device__ __forceinline__ double dpsi(const gp_model& m, Th t, const double* mu, const double* phi, int a) {
   double sum = 0.0;
 #pragma unroll
   for (int b = 0; b < N; b++) {
@@ -160,10 +182,10 @@ __device__ __forceinline__ double dpsi(const gp_model& m, const double* mu, cons
     double psi = 0.0;
 #pragma unroll
     for (int k = 0; k < K1; k++) {
-      c[k] = c_mu<K1>(m, mu, b, k);
+      c[k] = c_mu<K1>(m, t, mu, b, k);
       psi -= mu[k] * c[k];
     }
-    psi += free_energy<K1>(m, c, b);
+    psi += free_energy<N, K1>(m, t, c, b);
     sum += psi * dhphi<N>(phi, b, a);
   }
   return sum;
@@ -536,7 +558,8 @@ __global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_dphi(const __grid_const
         lambda[a] = m.epsilon * (t) - m.inv_eps * (m.anisotropy ? dwdphi_smooth<N>(m, ph, divphi, a)
                                                                 : dwdphi<N>(m, ph, divphi, a));
       else
-        lambda[a] = m.epsilon * (t) - m.inv_eps * dwdphi<N>(m, ph, divphi, a) - dpsi<N, K1>(m, muc, ph, a);
+        lambda[a] = m.epsilon * (t) - m.inv_eps * dwdphi<N>(m, ph, divphi, a) -
+                    dpsi<N, K1>(m, th_row(m, g, y, g.t_linear), muc, ph, a);
       sum_lambda += lambda[a];
       active++;
     }
@@ -570,7 +593,7 @@ template <int N, int K1>
 __device__ __forceinline__ void jat_face(const gp_model& m, const double* gn, const double* t_c, const double* t_n,
                                          const double* ph_c, const double* ph_n, const double* mu_c,
                                          const double* mu_n, const double* dp_c, const double* dp_n, bool skip,
-                                         double* j) {
+                                         double* j, Th th_c, Th th_n) {
   constexpr int L = N - 1;
   const double tl = 0.5 * (t_c[L] + t_n[L]);
   const double norm_l = sqrt(tl * tl + gn[L] * gn[L]);
@@ -588,8 +611,8 @@ __device__ __forceinline__ void jat_face(const gp_model& m, const double* gn, co
 #pragma unroll
     for (int k = 0; k < K1; k++) {
       if (normg != 0.0 && !skip) {
-        const double cl_n = c_mu<K1>(m, mu_n, L, k), cl_c = c_mu<K1>(m, mu_c, L, k);
-        const double cs_n = c_mu<K1>(m, mu_n, a, k), cs_c = c_mu<K1>(m, mu_c, a, k);
+        const double cl_n = c_mu<K1>(m, th_n, mu_n, L, k), cl_c = c_mu<K1>(m, th_c, mu_c, L, k);
+        const double cs_n = c_mu<K1>(m, th_n, mu_n, a, k), cs_c = c_mu<K1>(m, th_c, mu_c, a, k);
         double sp = gn[a] * gn[L];
         sp += ta * tl;
         if (norm_l > 0.0) sp /= (norm_l * normg);
@@ -745,12 +768,14 @@ __global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_update(const __grid_con
   // j_at on the four faces; the y-face at ghosted row MESH_Y-2 carries none
   // (calculate_fluxes_concentration.h:65), i.e. interior row my-5
   double jx_c[K1], jx_b[K1], jy_c[K1], jy_l[K1];
+  // the cells' temperatures in the concentration half step (ghosts: their boundary copy)
+  const Th thc = th_row(m, g, y, false), thl = th_row(m, g, y - 1, false), thr = th_row(m, g, y + 1, false);
   if (!SMOOTH) {
-    jat_face<N, K1>(m, gx_c, cy_c, cy_f, P[1][1], P[2][1], Mc, Mf, Dc, Df, false, jx_c);
-    jat_face<N, K1>(m, gx_b, cy_b, cy_c, P[0][1], P[1][1], Mb, Mc, Db, Dc, false, jx_b);
-    jat_face<N, K1>(m, gy_c, cx_c, cx_r, P[1][1], P[1][2], Mc, Mr, Dc, Dr, (y + 3 == g.my - 2), jy_c);
+    jat_face<N, K1>(m, gx_c, cy_c, cy_f, P[1][1], P[2][1], Mc, Mf, Dc, Df, false, jx_c, thc, thc);
+    jat_face<N, K1>(m, gx_b, cy_b, cy_c, P[0][1], P[1][1], Mb, Mc, Db, Dc, false, jx_b, thc, thc);
+    jat_face<N, K1>(m, gy_c, cx_c, cx_r, P[1][1], P[1][2], Mc, Mr, Dc, Dr, (y + 3 == g.my - 2), jy_c, thc, thr);
     jat_face<N, K1>(m, gy_l, cx_l, cx_c, P[1][0], P[1][1], Ml, Mc, Dl, Dc, (y + 2 == g.my - 2) || (y + 2 == 0),
-                    jy_l);
+                    jy_l, thl, thc);
   }
 
   const double* ph = P[1][1];
@@ -767,7 +792,7 @@ __global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_update(const __grid_con
 #pragma unroll
     for (int b = 0; b < N; b++) sdh += dhphi<N>(ph, a, b) * Dc[b];
 #pragma unroll
-    for (int k = 0; k < K1; k++) sum[k] += c_mu<K1>(m, Mc, a, k) * sdh;
+    for (int k = 0; k < K1; k++) sum[k] += c_mu<K1>(m, thc, Mc, a, k) * sdh;
   }
   const double jscale = m.obstacle ? m.jat_obst : m.jat_well;
 #pragma unroll
@@ -804,7 +829,7 @@ __global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_update(const __grid_con
       double co = 0.0;
 #pragma unroll
       for (int a = 0; a < N; a++)
-        if (a == bulk) co = c_mu<K1>(m, Mc, a, k);
+        if (a == bulk) co = c_mu<K1>(m, thc, Mc, a, k);
       cnew[k] = SMOOTH ? co + m.dt * (divflux[k]) : co + m.dt * (divflux[k]) - divjat[k];
     }
 #pragma unroll
@@ -812,7 +837,7 @@ __global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_update(const __grid_con
       double v = 0.0;
 #pragma unroll
       for (int a = 0; a < N; a++)
-        if (a == bulk) v = Mu<K1>(m, cnew, a, k);
+        if (a == bulk) v = Mu<K1>(m, thc, cnew, a, k);
       mnew[k] = v;
     }
   } else if (SMOOTH) {
@@ -904,8 +929,14 @@ cudaError_t launch_step(const gp_model& m, const Geo& g, const double* phi, cons
 // Host entry used by the C ABI (gp_capi.cu).  Two launches per step.
 cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch, int64_t rplane,
                         const double* phi, const double* mu, double* dphi, double* phi_out, double* mu_out,
-                        cudaStream_t s, bool smooth, const double* ghost_rows) {
+                        cudaStream_t s, bool smooth, const double* ghost_rows, const gp_temp_step* temp) {
+  if (m.nonisothermal && !temp) return cudaErrorInvalidValue;  // the step needs its temperature
   Geo g;
+  g.noniso = m.nonisothermal ? 1 : 0;
+  g.t_linear = temp ? temp->linear : 0;
+  g.bc_t = m.bc_T[3];
+  g.t_bottom = temp ? temp->bottom : 0.0;
+  g.t_grad = temp ? temp->grad : 0.0;
   g.mx = (int)m.mesh_x;
   g.my = (int)m.mesh_y;
   g.pitch = pitch;

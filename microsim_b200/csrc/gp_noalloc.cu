@@ -43,7 +43,8 @@ extern "C" void gp_set_error(const char* fmt, ...);
 
 cudaError_t gp_f64_step(const gp_model& m, int pitch, int64_t plane, int rpitch, int64_t rplane,
                         const double* phi, const double* mu, double* dphi, double* phi_out, double* mu_out,
-                        cudaStream_t s, bool smooth = false, const double* ghost_rows = nullptr);
+                        cudaStream_t s, bool smooth = false, const double* ghost_rows = nullptr,
+                        const gp_temp_step* temp = nullptr);
 
 static __device__ __align__(256) double g_noalloc_dphi[GP_NOALLOC_SCRATCH_BYTES / sizeof(double)];
 
@@ -76,6 +77,10 @@ extern "C" int gp_step_f64_noalloc(const gp_model* m, const double* phi, const d
       gp_set_error("gp_step_f64_noalloc: boundary types must be Neumann (1) or periodic (3)");
       return GP_E_UNSUPPORTED;
     }
+  }
+  if (m->nonisothermal) {
+    gp_set_error("gp_step_f64_noalloc: a non-isothermal model needs the step count (gp_create/gp_step)");
+    return GP_E_UNSUPPORTED;
   }
   if (m->bc_phi[0] != m->bc_phi[1] || m->bc_phi[2] != m->bc_phi[3] || m->bc_mu[0] != m->bc_mu[1] ||
       m->bc_mu[2] != m->bc_mu[3] || (m->mu_solver == GP_MU_TERNARY && m->K1 != 2)) {

@@ -71,6 +71,11 @@ int main(int argc, char *argv[]) {
     snprintf(name, sizeof name, "DATA/%s_%lld.vtk", argv[3], (long long)starttime);
     if ((rc = gp_read_vtk(in, &m, name, phi, mu)) != GP_OK) return fail("restart read", rc);
   }
+  if (m.nonisothermal && starttime > 0) {
+    /* microsim_gp.c:68-74 moves gradient_OFFSET on a restart; not on this path */
+    fprintf(stderr, "microsim_gp_b200: a restart (STARTTIME > 0) under a frozen temperature gradient is not supported\n");
+    return 2;
+  }
   if ((rc = gp_create(&m, precision, &ctx)) != GP_OK) return fail("gp_create", rc);
   if ((rc = gp_upload(ctx, phi, mu)) != GP_OK) return fail("gp_upload", rc);
   if (restart == 0 || starttime == 0) {
@@ -128,7 +133,7 @@ int main(int argc, char *argv[]) {
     if (t % saveT == 0) {
       if ((rc = gp_download(ctx, phi, mu)) != GP_OK) return fail("gp_download", rc);
       snprintf(name, sizeof name, "DATA/%s_%lld.vtk", argv[3], (long long)(t + starttime));
-      if ((rc = gp_write_vtk(in, &m, name, phi, mu)) != GP_OK) return fail("vtk write", rc);
+      if ((rc = gp_write_vtk_t(in, &m, name, phi, mu, t)) != GP_OK) return fail("vtk write", rc);
       FILE *fp = fopen("DATA/shift.dat", "a");
       if (fp) {
         fprintf(fp, "%ld %ld\n", (long)(t + starttime), (long)(shift_offset + shift_position));

@@ -566,7 +566,10 @@ int gp_model_from_input(const gp_input *in, gp_model *m) {
   if (N < 2 || N > GP_MAX_PHASES) { gp_set_error("NUMPHASES=%d outside 2..%d", N, GP_MAX_PHASES); return GP_E_UNSUPPORTED; }
   if (K1 < 1 || K1 > GP_MAX_K1) { gp_set_error("NUMCOMPONENTS=%d outside 2..%d", K1 + 1, GP_MAX_K1 + 1); return GP_E_UNSUPPORTED; }
   if (in->MESH_X < 4 || in->MESH_Y < 4) { gp_set_error("MESH_X, MESH_Y must be >= 4"); return GP_E_UNSUPPORTED; }
-  if (!in->ISOTHERMAL) { gp_set_error("ISOTHERMAL=0 (frozen temperature gradient) is not on this path"); return GP_E_UNSUPPORTED; }
+  if (!in->ISOTHERMAL && in->SHIFT) {
+    gp_set_error("ISOTHERMAL=0 with Shift=1 (a moving frame under the frozen gradient) is not on this path");
+    return GP_E_UNSUPPORTED;
+  }
   if (in->FUNCTION_F != 1) { gp_set_error("Function_F=%d: only the quadratic free energy (1) is on this path", in->FUNCTION_F); return GP_E_UNSUPPORTED; }
   if (in->NOISE_PHASEFIELD) { gp_set_error("Noise_phasefield uses rand(); not on this path"); return GP_E_UNSUPPORTED; }
   if (!in->have_gamma || !in->have_tau) { gp_set_error("GAMMA and Tau are required"); return GP_E_PARSE; }
@@ -672,7 +675,37 @@ int gp_model_from_input(const gp_input *in, gp_model *m) {
       for (i = 0; i < K1; i++) {
         m->Beff[a][i] = (Beq[a][i] + dBbdT[a][i] * (in->T - in->Teq));
         m->Bfill[a][i] = (Beq[a][i] + dBbdT[a][i] * (in->Teq - in->Teq));
+        m->Beq[a][i] = Beq[a][i];
+        m->dBbdT[a][i] = dBbdT[a][i];
+        m->ceq_s[a][i] = in->ceq[a][a][i];
+        m->ceq_l[a][i] = in->ceq[a][N - 1][i];
+        m->dC[a][i] = DC[a][i];
       }
+    for (a = 0; a < N; a++) {
+      m->dT_s[a] = DT[a][a];
+      m->dT_l[a] = DT[a][N - 1];
+    }
+    if (!in->ISOTHERMAL) {
+      /* the T copy of boundary_serial.h (field 2): from the proxy rows when the current type is 1 or 3 */
+      for (i = 0; i < 4; i++) {
+        const int tcur = in->bc_type[i][2], tprx = in->bc_proxy_type[i][2];
+        m->bc_T[i] = (tcur == 1 || tcur == 3) ? ((tprx == 1 || tprx == 3) ? tprx : -1) : 0;
+        if (m->bc_T[i] < 0) {
+          gp_set_error("boundary %d (T): no BOUNDARY_VALUE line after its BOUNDARY line", i);
+          return GP_E_PARSE;
+        }
+      }
+      if (m->bc_T[2] != m->bc_T[3]) {
+        gp_set_error("both y sides must share the temperature's boundary type");
+        return GP_E_UNSUPPORTED;
+      }
+      m->nonisothermal = 1;
+      m->tg_base = in->tempgrady[0];
+      m->tg_deltaT = in->tempgrady[1];
+      m->tg_distance = in->tempgrady[2];
+      m->tg_offset = in->tempgrady[3];
+      m->tg_velocity = in->tempgrady[4];
+    }
     /* apply_shiftY's liquid rows, functions/shift.h:24-37 with function_F_01_Mu */
     for (k = 0; k < K1; k++) {
       const int L = N - 1;
@@ -802,12 +835,26 @@ static double be64(double v) {
 }
 
 /* c_a(mu) h_a(phi) summed over phases: the Composition_ field, file_writer.h:203-235 */
-static double composition(const gp_model *m, const double *ph, const double *mu, int k) {
+/* The frozen gradient's temperature of ghost-padded row gy after step t (microsim_gp.c:77-82,
+ * 108-113; functions/Temperature_gradient.h:19), no moving frame. */
+static double temp_after(const gp_model *m, long t, long gy) {
+  const double shift_offset = 0.0;
+  const double base_pos = t == 0 ? (m->tg_offset / m->dy) - shift_offset
+                                 : (m->tg_offset / m->dy) - shift_offset + ((m->tg_velocity / m->dy) * ((double)t * m->dt));
+  const double grad = (m->tg_deltaT) * m->dy / (m->tg_distance);
+  const double bottom = m->tg_base - base_pos * grad;
+  return bottom + (double)gy * grad;
+}
+
+/* sum_a c_a(mu, T) h_a(phi) (file_writer.h:115-133); T only for a non-isothermal model */
+static double composition(const gp_model *m, const double *ph, const double *mu, int k, double T) {
   int a, b2, c2, l, N = m->N, K1 = m->K1;
   double comp = 0.0;
   for (a = 0; a < N; a++) {
     double cm = 0.0, h, s1 = 0.0;
-    for (l = 0; l < K1; l++) cm += m->cmu[a][k][l] * (mu[l] - m->Beff[a][l]);
+    for (l = 0; l < K1; l++)
+      cm += m->cmu[a][k][l] *
+            (mu[l] - (m->nonisothermal ? (m->Beq[a][l] + m->dBbdT[a][l] * (T - m->Teq)) : m->Beff[a][l]));
     h = 3.0 * ph[a] * ph[a] - 2.0 * ph[a] * ph[a] * ph[a];
     for (b2 = 0; b2 < N; b2++)
       for (c2 = b2 + 1; c2 < N; c2++)
@@ -819,6 +866,11 @@ static double composition(const gp_model *m, const double *ph, const double *mu,
 }
 
 int gp_write_vtk(const gp_input *in, const gp_model *m, const char *path, const double *phi, const double *mu) {
+  return gp_write_vtk_t(in, m, path, phi, mu, 0);
+}
+
+int gp_write_vtk_t(const gp_input *in, const gp_model *m, const char *path, const double *phi, const double *mu,
+                   int64_t tstep) {
   FILE *fp;
   long mx, my, np, x, y;
   int a, k;
@@ -866,12 +918,22 @@ int gp_write_vtk(const gp_input *in, const gp_model *m, const char *path, const 
           int l;
           for (l = 0; l < m->N; l++) ph[l] = phi[l * np + x * my + y];
           for (l = 0; l < m->K1; l++) mm[l] = mu[l * np + x * my + y];
-          v = composition(m, ph, mm, k);
+          v = composition(m, ph, mm, k, m->nonisothermal ? temp_after(m, (long)tstep, y + 3) : m->T);
           if (in->ASCII) fprintf(fp, "%le \n", v);
           else { v = be64(v); fwrite(&v, sizeof(double), 1, fp); }
         }
       if (in->ASCII) fprintf(fp, "\n");
     }
+  }
+  if (m->nonisothermal) { /* file_writer.h:138-150 / 238-253: the cells' temperature after step tstep */
+    fprintf(fp, "SCALARS Temperature double 1\n");
+    fprintf(fp, "LOOKUP_TABLE default\n");
+    for (x = 0; x < mx; x++)
+      for (y = 0; y < my; y++) {
+        double v = temp_after(m, (long)tstep, y + 3);
+        if (in->ASCII) fprintf(fp, "%le \n", v);
+        else { v = be64(v); fwrite(&v, sizeof(double), 1, fp); }
+      }
   }
   if (fclose(fp) != 0) return GP_E_IO;
   return GP_OK;

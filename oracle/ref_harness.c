@@ -25,8 +25,9 @@
  *   gp_ref_harness Input.in Filling.in Out - NSTEPS
  *     timing only (no dumps).
  *
- * The shift / temperature-gradient / VTK branches of the reference main are
- * not exercised here: inputs given to the harness use Shift=0, ISOTHERMAL=1.
+ * With ISOTHERMAL = 0 the frozen temperature gradient is set after the
+ * filling and after every step exactly as the reference main does
+ * (microsim_gp.c:77-82, 108-113; no moving frame with it).
  */
 #define main microsim_reference_main
 #include "microsim_gp.c"
@@ -181,6 +182,13 @@ int main(int argc, char *argv[]) {
   initialize_functions_solverloop();
   read_boundary_conditions(argv);
   fill_domain(argv);
+  /* microsim_gp.c:77-82 */
+  if (TEMPGRADY) {
+    BASE_POS    = (temperature_gradientY.gradient_OFFSET/deltay) - shift_OFFSET;
+    GRADIENT    = (temperature_gradientY.DeltaT)*deltay/(temperature_gradientY.Distance);
+    temp_bottom = temperature_gradientY.base_temp - BASE_POS*GRADIENT;
+    apply_temperature_gradientY(gridinfo, shift_OFFSET, 0);
+  }
   apply_boundary_conditions(0);
 
   if (dumping) {
@@ -205,6 +213,13 @@ int main(int argc, char *argv[]) {
     if (dumping && t == 1) dump_state(dumpdir, "dphi", 1, 1);
     solverloop_concentration(start, end);
     apply_boundary_conditions(0);
+    /* microsim_gp.c:108-113: the frozen gradient after the step */
+    if (TEMPGRADY) {
+      BASE_POS    = (temperature_gradientY.gradient_OFFSET/deltay) - shift_OFFSET + ((temperature_gradientY.velocity/deltay)*(t*deltat));
+      GRADIENT    = (temperature_gradientY.DeltaT)*deltay/(temperature_gradientY.Distance);
+      temp_bottom = temperature_gradientY.base_temp - BASE_POS*GRADIENT;
+      apply_temperature_gradientY(gridinfo, shift_OFFSET, t);
+    }
     /* microsim_gp.c:115-125: the moving frame, every 100 steps */
     if (t % 100 == 0 && SHIFT) {
       if (MAX_INTERFACE_POS > shiftj) shift_ON = 1;

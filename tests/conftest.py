@@ -30,6 +30,12 @@ def golden_cases():
                   if not p.endswith(".long.npz"))
 
 
+def isothermal_cases():
+    """Short cases with one temperature throughout (the oracle restatement and the FP32 form take
+    only these; the frozen-gradient cases pin the FP64 plain form to the reference directly)."""
+    return [c for c in golden_cases() if not int(load_golden(c).get("nonisothermal", 0))]
+
+
 def long_cases():
     """Long runs: per-row SHA-256 of the final interior state."""
     return sorted(os.path.basename(p)[: -len(".long.npz")] for p in glob.glob(os.path.join(GOLDEN, "*.long.npz")))

@@ -121,6 +121,31 @@ def cases():
     c.fills = [("FILLCUBE", [0, 0, 0, 0, 23, 14, 0])]
     c.shift, c.shiftj = 1, 20
     out["shift_planar"] = (c, [1, 100, 200, 300, 400])
+    # frozen temperature gradient (ISOTHERMAL = 0, Tempgrady): anisotropic obstacle binary, the
+    # gradient moving along +y; ASCII output with composition and the Temperature field
+    c = C.binary_case(32, 40, gap=1.0, supersat=0.5, eps=4.0, delta=0.03, theta=10.0, dt=0.05, tau=1.7776,
+                      seed=(16, 10, 6.0), steps=60)
+    c.tempgrady = (0.97, 0.08, 40.0, 2.0, 0.5)
+    c.writeformat = "ASCII"
+    c.writecomposition = 1
+    out["tempgrad_aniso_bin"] = (c, [1, 30, 60])
+    # frozen gradient, three phases, well potential, periodic x; the temperature's y ghosts not copied
+    c = configs.Case(mesh_x=28, mesh_y=24, dx=1.0, dt=0.04, N=3, K=2, ntimesteps=40, epsilon=4.0, tau=1.0,
+                     gamma=[1.0, 1.0, 1.0], tau_ab=[1.5, 1.5, 1.5], aniso=0, dab=[0.0, 0.0, 0.0],
+                     function_w=2, gamma_abc=[5.0],
+                     diffusivity=[(1, 0, 0.0), (1, 1, 0.0), (1, 2, 1.0)], A=[(0, 1.0), (1, 1.0), (2, 1.0)],
+                     ceq=[(0, 0, 0.78), (0, 2, 0.5), (2, 0, 0.5), (1, 1, 0.21), (1, 2, 0.5), (2, 1, 0.5),
+                          (2, 2, 0.5)],
+                     cfill=[(0, 0, 0.78), (0, 2, 0.5), (2, 0, 0.5), (1, 1, 0.21), (1, 2, 0.5), (2, 1, 0.5),
+                            (2, 2, 0.45)],
+                     slopes=[(0, 0, 0.45), (0, 2, 0.45), (2, 0, 0.45), (1, 1, -0.45), (1, 2, -0.45),
+                             (2, 1, -0.45)],
+                     T=0.98, bc_phi=(3, 3, 1, 1), bc_mu=(3, 3, 1, 1), solver="BINARY",
+                     phases=["alpha", "beta", "liquid"], components=["Al", "Cu"],
+                     fills=[("FILLCUBE", [0, 0, 0, 0, 13, 5, 0]), ("FILLCUBE", [1, 14, 0, 0, 27, 5, 0])])
+    c.tempgrady = (0.96, 0.05, 24.0, 0.0, 0.2)
+    c.bc_T = (3, 3, 0, 0)
+    out["tempgrad_three_phase_well"] = (c, [1, 20, 40])
     return out
 
 
@@ -132,7 +157,7 @@ def run_case(name, case, dump_steps):
         nsteps = max(dump_steps)
         stdout = O.run_reference_harness(td, "Input.in", "Filling.in", nsteps, dump_steps, dumpdir=dd)
         data = {"input_text": np.array(case.input_text()), "filling_text": np.array(case.filling_text()),
-                "dump_steps": np.array(dump_steps)}
+                "dump_steps": np.array(dump_steps), "nonisothermal": np.array(int(case.tempgrady is not None))}
         for k, v in O.read_consts(os.path.join(dd, "consts.txt")).items():
             data["c_" + k] = v
         phi, mu = O.read_state(os.path.join(dd, "state_0.bin"))

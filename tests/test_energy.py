@@ -13,7 +13,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import golden_cases, interior, load_golden, write_inputs
+from conftest import isothermal_cases, interior, load_golden, write_inputs
 import microsim_b200 as mb
 from oracle import gp_oracle as O
 
@@ -96,7 +96,7 @@ def _check(got, want, ncell):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", golden_cases())
+@pytest.mark.parametrize("case", isothermal_cases())
 def test_device_energies_match_the_checker_fp64(case):
     m, phi, mu = _case_state(case)
     with mb.Context(m, mb.GP_FP64) as ctx:
@@ -107,7 +107,7 @@ def test_device_energies_match_the_checker_fp64(case):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", golden_cases())
+@pytest.mark.parametrize("case", isothermal_cases())
 def test_device_energies_match_the_checker_fp32_batch(case):
     m, phi, mu = _case_state(case)
     try:

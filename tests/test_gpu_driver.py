@@ -2,7 +2,7 @@
 on the reference fixtures' own input files, its VTK output read back and
 compared with the reference's state (FP64: bit-exact; the binary VTK stores
 big-endian doubles, so nothing is lost).  Covers the smoothing pre-steps of
-inputs with NSMOOTH > 1."""
+inputs with NSMOOTH > 1 and a frozen temperature gradient (ISOTHERMAL = 0)."""
 import os
 import subprocess
 import tempfile
@@ -16,7 +16,8 @@ import microsim_b200 as mb
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("case", ["iso_obst_bin", "aniso_obst_bin_per", "four_phase_ternary", "smooth_aniso_obst"])
+@pytest.mark.parametrize("case", ["iso_obst_bin", "aniso_obst_bin_per", "four_phase_ternary", "smooth_aniso_obst",
+                                  "tempgrad_three_phase_well"])
 def test_driver_output_matches_reference(case):
     assert case in golden_cases()
     g = load_golden(case)

@@ -18,7 +18,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import golden_cases, interior, load_golden, presmooth, write_inputs
+from conftest import golden_cases, interior, isothermal_cases, load_golden, presmooth, write_inputs
 import microsim_b200 as mb
 from microsim_b200 import configs
 
@@ -62,7 +62,7 @@ def test_four_phase_ternary_within_tolerance():
     np.testing.assert_allclose(s32["solute"], s64["solute"], rtol=1e-4)
 
 
-@pytest.mark.parametrize("case", [c for c in golden_cases()
+@pytest.mark.parametrize("case", [c for c in isothermal_cases()
                                   if c != "c1_literal_small" and "shifts" not in load_golden(c)])
 def test_golden_cases_within_tolerance_of_reference(case):
     g = load_golden(case)

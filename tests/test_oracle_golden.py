@@ -7,7 +7,7 @@ the interior and on the Delta-phi ring the interior reads.
 import numpy as np
 import pytest
 
-from conftest import golden_cases, interior, load_golden, oracle_model
+from conftest import isothermal_cases, interior, load_golden, oracle_model
 from oracle import gp_oracle as O
 
 
@@ -20,7 +20,7 @@ def start_state(g, m):
     return phi, mu
 
 
-@pytest.mark.parametrize("case", [c for c in golden_cases() if "nsmooth" in load_golden(c)])
+@pytest.mark.parametrize("case", [c for c in isothermal_cases() if "nsmooth" in load_golden(c)])
 def test_smoothing_pre_steps_bitexact(case):
     g = load_golden(case)
     phi, mu = start_state(g, oracle_model(g))
@@ -29,7 +29,7 @@ def test_smoothing_pre_steps_bitexact(case):
     assert np.array_equal(phi, g["phi_smoothed"]) and np.array_equal(mu, g["mu_smoothed"])  # ghosts too
 
 
-@pytest.mark.parametrize("case", golden_cases())
+@pytest.mark.parametrize("case", isothermal_cases())
 def test_dphi_first_step_bitexact(case):
     g = load_golden(case)
     m = oracle_model(g)
@@ -72,7 +72,7 @@ def liquid_fill_mu(g):
     return np.array(mdl.mu_shift[: mdl.K1])
 
 
-@pytest.mark.parametrize("case", golden_cases())
+@pytest.mark.parametrize("case", isothermal_cases())
 def test_states_bitexact(case):
     """Including the moving frame: the interface row of every 100th step equals
     the reference's, and shifting the ghost-padded fields as the reference does
@@ -99,7 +99,7 @@ def test_states_bitexact(case):
         assert np.array_equal(interior(mu), interior(g[f"mu_{t}"])), f"mu differs after step {t}"
 
 
-@pytest.mark.parametrize("case", golden_cases())
+@pytest.mark.parametrize("case", isothermal_cases())
 def test_ghost_fill_matches(case):
     """Ghost layers after the boundary copy equal the reference's (t = 0 and later)."""
     g = load_golden(case)
