@@ -199,7 +199,7 @@ def run_reference_arm(args, world, rank):
 
 # --------------------------------------------------------------------------------------------- our arm
 
-def prepare(models, fields, steps):
+def prepare(models, fields, steps, compensated=False):
     """Advance the synthetic initial state `steps` steps with the FP32 form (input
     preparation, before any timing): the benchmark state is the workload part-way
     through its run, where the interface has grown, instead of the first steps of a
@@ -208,6 +208,7 @@ def prepare(models, fields, steps):
     if steps <= 0:
         return fields
     with mb.Batch(models) as b:
+        b.set_compensated(compensated)
         for i, (p, u) in enumerate(fields):
             b.upload(i, p, u)
         b.step(steps)
@@ -303,7 +304,8 @@ def run_ours(args, world, rank, local):
     loaded = [mb.load_case(c) for c in cases]
     models = [m for m, _, _ in loaded]
     prep = args.prep_steps if args.prep_steps >= 0 else {"c2": 25000, "c1": 5000, "c4": 2500}[args.workload]
-    fields = prepare(models, [(p, u) for _, p, u in loaded], prep)
+    comp = args.compensated == 1
+    fields = prepare(models, [(p, u) for _, p, u in loaded], prep, comp)
     cells = sum(m.mesh_x * m.mesh_y for m in models)
     N, K1 = models[0].N, models[0].K1
     peak, peak_kind = measured_peaks()
@@ -311,6 +313,7 @@ def run_ours(args, world, rank, local):
 
     # ---- the chosen form (FP32 batch: narrow band, CUDA-graph replay)
     ctx = mb.Batch(models)
+    ctx.set_compensated(comp)
     for i, f in enumerate(fields):
         ctx.upload(i, *f)
     tile = ctx.autotune(args.tune_cache) if not args.no_autotune else (16, 32)
@@ -353,6 +356,7 @@ def run_ours(args, world, rank, local):
     ctx.set_timing(False)
     gen_cells = cells - lean_cells
     depth = ctx.depth()
+    grids = ctx.grids()
     if depth == 2:  # per blocked pair (two steps): kernel_ms reports per step
         kernels = {
             "k_lean2": {"ms": 2 * kt["lean"], "bytes": 2 * lean_cells * 2 * K1 * 4,
@@ -407,6 +411,26 @@ def run_ours(args, world, rank, local):
         ctx.set_narrowband(True)
         ctx.set_depth(nb_depth)
 
+    # ---- the other FP32 accumulation mode on the same configuration (its cost per step)
+    other = None
+    if not args.no_fp64:
+        ctx.set_compensated(not comp)
+        ctx.prepare()
+        ctx.step(args.warmup)
+        ctx.sync()
+        eo0, eo1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            eo0.record(stream)
+        ctx.step(args.steps)
+        with torch.cuda.stream(stream):
+            eo1.record(stream)
+        ctx.sync()
+        oms = allmax(eo0.elapsed_time(eo1), world)
+        other = {"accumulation": "plain" if comp else "compensated (TwoSum/TwoProduct)",
+                 "value": cells_all * args.steps / (oms / 1e3), "unit": UNIT, "ms_per_step": oms / args.steps,
+                 "note": "same tiles, grids and depth as the headline; graphs recaptured for this mode"}
+        ctx.set_compensated(comp)
+
     # ---- FP64 plain on the same workload
     fp64 = None
     if not args.no_fp64:
@@ -457,7 +481,9 @@ def run_ours(args, world, rank, local):
                        "state_prepared_steps": prep,
                        "parallelism": (f"instances sharded over {world} ranks" if len(models) > 1 else
                                        f"replicas{world}") if world > 1 else "single", "l2": l2,
-                       "tile": list(tile), "lean_tiles": lean_tiles, "tiles": tiles, "depth": depth},
+                       "tile": list(tile), "lean_tiles": lean_tiles, "tiles": tiles, "depth": depth,
+                       "blocks_per_sm": {"lean": grids[0], "full": grids[1]},
+                       "accumulation": "compensated (TwoSum/TwoProduct)" if comp else "plain"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None, "traffic": traffic,
                          "bytes_per_launch": d["bytes"], "ms_per_launch": d["ms"],
@@ -469,6 +495,7 @@ def run_ours(args, world, rank, local):
                               "note": "dense-step definition: read+write phi and mu once per cell-update; the "
                                       "narrow band skips phi traffic of pure tiles, so this can exceed 1"},
             "kernels_ms_per_step": {k: v["ms"] for k, v in kernels.items()},
+            ("fp32_compensated" if not comp else "fp32_plain_accumulation"): other,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": state_bytes / args.steps + 64 * 8},
@@ -500,6 +527,9 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=50)
     ap.add_argument("--prep-steps", type=int, default=-1,
                     help="steps of the FP32 form run before timing to reach a mid-run state (-1: half the run)")
+    ap.add_argument("--compensated", type=int, default=0, choices=[0, 1],
+                    help="FP32 accumulation of the headline: plain (0, default) or compensated (1); the other "
+                         "mode is timed on the same configuration beside it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")

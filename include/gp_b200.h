@@ -199,6 +199,16 @@ int gp_step(gp_ctx *ctx, int64_t nsteps);
 /* The context's step count (the frozen temperature gradient's clock: step t uses the temperature
  * the reference sets after step t - 1).  Starts at 0 on creation; gp_step advances it. */
 int gp_set_time_step(gp_ctx *ctx, int64_t t);
+/* FP32 only (no counterpart in the reference, whose step is FP64): compensated
+ * accumulation.  The net face flux of every cell's concentration update, the
+ * interface source sum and the bulk and pure-phase increments of mu are summed
+ * with error-free transforms (TwoSum, TwoProduct on the fused multiply-add), their
+ * rounding errors carried apart and added once, so the update keeps the
+ * increments that plain FP32 sums lose against mu's scale.  Off by default; a
+ * step costs more arithmetic and no extra memory traffic.  GP_E_ARG on an FP64
+ * context. */
+int gp_set_compensated(gp_ctx *ctx, int on);
+int gp_get_compensated(gp_ctx *ctx);
 /* nsteps smoothing pre-steps (the reference runs NSMOOTH - 1 of them before its
  * time loop, microsim_gp.c:97-100; solverloop.h:72-90): the phase-field step
  * without the driving force and with isotropic gradient energy, the
@@ -291,6 +301,9 @@ int gp_batch_get_scan(gp_batch *b);
  * rel_change_* of gp_batch_get_stats covers the pair's two steps. */
 int gp_batch_set_depth(gp_batch *b, int depth);
 int gp_batch_get_depth(gp_batch *b);
+/* Compensated accumulation for every instance of the batch (gp_set_compensated). */
+int gp_batch_set_compensated(gp_batch *b, int on);
+int gp_batch_get_compensated(gp_batch *b);
 /* Failure-detection test (no counterpart in the reference): the next step's
  * lean kernel leaves one staged tile box unissued; its wait gives up after one
  * second, the kernel returns, and the next gp_batch_get_stats reports GP_E_TIMEOUT.
@@ -306,10 +319,12 @@ int gp_batch_set_timing(gp_batch *b, int on);
 int gp_batch_kernel_ms(gp_batch *b, double *ms3, int64_t *steps);
 /* Measured sweep over the tile shapes, each with full-kernel blocks of 256
  * and (binary alloys) 512 threads, the list or scan way of finding the
- * interface tiles, depth 1 or 2 (list mode), and the lean grid at its occupancy
- * and one block per SM below it, on the batch's own state (restored
+ * interface tiles, depth 1 or 2 (list mode), the lean grid at its occupancy,
+ * one block per SM below it or half of it, and the full kernel's grid at its
+ * occupancy or one block per SM below it, on the batch's own state (restored
  * afterwards); the winner is applied and cached in cache_path (may be NULL)
- * per batch signature, read back on the next call. */
+ * per batch signature (phases, components, anisotropy, cells, instances and the
+ * accumulation mode), read back on the next call. */
 int gp_batch_autotune(gp_batch *b, const char *cache_path, int *tx, int *ty);
 void *gp_batch_stream(gp_batch *b);
 /* The current state buffers of instance i on the device (FP32: esize 4), as

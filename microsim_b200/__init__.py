@@ -100,6 +100,8 @@ _SIGS = {
     "gp_write_vtk": (C.c_int, [C.c_void_p, C.POINTER(GpModel), C.c_char_p, C.c_void_p, C.c_void_p]),
     "gp_write_vtk_t": (C.c_int, [C.c_void_p, C.POINTER(GpModel), C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "gp_set_time_step": (C.c_int, [C.c_void_p, C.c_int64]),
+    "gp_set_compensated": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_get_compensated": (C.c_int, [C.c_void_p]),
     "gp_read_vtk": (C.c_int, [C.c_void_p, C.POINTER(GpModel), C.c_char_p, C.c_void_p, C.c_void_p]),
     "gp_create": (C.c_int, [C.POINTER(GpModel), C.c_int, C.POINTER(C.c_void_p)]),
     "gp_destroy": (C.c_int, [C.c_void_p]),
@@ -132,6 +134,8 @@ _SIGS = {
                                         C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
     "gp_batch_state_changed": (C.c_int, [C.c_void_p]),
     "gp_batch_get_depth": (C.c_int, [C.c_void_p]),
+    "gp_batch_set_compensated": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_batch_get_compensated": (C.c_int, [C.c_void_p]),
     "gp_batch_test_lose_box": (C.c_int, [C.c_void_p]),
     "gp_batch_get_grids": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
@@ -313,6 +317,17 @@ class Context:
         """nsteps smoothing pre-steps (NSMOOTH - 1 in the reference's main)."""
         _check("gp_smooth", lib().gp_smooth(self._h, int(nsteps)))
 
+    def set_time_step(self, t: int):
+        """The step count the frozen temperature gradient is evaluated at."""
+        _check("gp_set_time_step", lib().gp_set_time_step(self._h, int(t)))
+
+    def set_compensated(self, on: bool):
+        """FP32 only: compensated (error-free transform) accumulation of the updates."""
+        _check("gp_set_compensated", lib().gp_set_compensated(self._h, int(bool(on))))
+
+    def compensated(self) -> bool:
+        return bool(lib().gp_get_compensated(self._h))
+
     def device_state(self):
         """(phi, mu) torch views [planes, mesh_x, pitch] of the current device
         buffers (valid until the next step); call state_changed() after writing."""
@@ -468,6 +483,13 @@ class Batch:
 
     def depth(self) -> int:
         return lib().gp_batch_get_depth(self._h)
+
+    def set_compensated(self, on: bool):
+        """Compensated (error-free transform) accumulation of the FP32 updates."""
+        _check("gp_batch_set_compensated", lib().gp_batch_set_compensated(self._h, int(bool(on))))
+
+    def compensated(self) -> bool:
+        return bool(lib().gp_batch_get_compensated(self._h))
 
     def prepare(self):
         """Capture the step graphs now (no step is taken)."""

@@ -51,6 +51,8 @@ int gp_f32_batch_launches_per_step(const gp_f32_batch* b);
 void gp_f32_batch_bind_x(gp_f32_batch* b, int i, float* phiX, float* muX);
 bool gp_f32_batch_set_depth(gp_f32_batch* b, int depth);
 int gp_f32_batch_depth(const gp_f32_batch* b);
+cudaError_t gp_f32_batch_set_compensated(gp_f32_batch* b, int on);
+int gp_f32_batch_compensated(const gp_f32_batch* b);
 cudaError_t gp_f32_batch_launch_pair(gp_f32_batch* b, int parity, cudaStream_t s);
 int gp_f32_batch_launches_per_pair(const gp_f32_batch* b);
 int gp_f32_tile_shape_count();
@@ -330,6 +332,21 @@ extern "C" int gp_step(gp_ctx* c, int64_t nsteps) {
     c->tstep++;
   }
   return GP_OK;
+}
+
+extern "C" int gp_set_compensated(gp_ctx* c, int on) {
+  if (!c) return GP_E_ARG;
+  if (c->precision != GP_FP32) {
+    gp_set_error("gp_set_compensated: FP32 contexts only (the FP64 step is the reference's own arithmetic)");
+    return GP_E_ARG;
+  }
+  GP_CUDA(cudaStreamSynchronize(c->stream));
+  GP_CUDA(gp_f32_batch_set_compensated(c->f32, on));
+  return GP_OK;
+}
+
+extern "C" int gp_get_compensated(gp_ctx* c) {
+  return c && c->precision == GP_FP32 ? gp_f32_batch_compensated(c->f32) : 0;
 }
 
 extern "C" int gp_set_time_step(gp_ctx* c, int64_t t) {
@@ -1064,18 +1081,19 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   for (const gp_model& m : b->models) cells += m.mesh_x * m.mesh_y;
   const gp_model& m0 = b->models[0];
   char key[128];
-  snprintf(key, sizeof key, "%d %d %d %lld %d", m0.N, m0.K1, m0.anisotropy, (long long)cells, b->n);
+  const int comp = gp_f32_batch_compensated(b->f32);
+  snprintf(key, sizeof key, "%d %d %d %lld %d %d", m0.N, m0.K1, m0.anisotropy, (long long)cells, b->n, comp);
   if (cache_path) {
     FILE* f = fopen(cache_path, "r");
     if (f) {
       char line[256];
       while (fgets(line, sizeof line, f)) {
-        int N, K1, an, n, tx, ty, lp, th, sc, dp;
+        int N, K1, an, n, cp, tx, ty, lp, gq, th, sc, dp;
         long long c;
         double ms;
-        if (sscanf(line, "%d %d %d %lld %d %d %d %d %d %d %d %lf", &N, &K1, &an, &c, &n, &tx, &ty, &lp, &th, &sc, &dp,
-                   &ms) == 12 &&
-            N == m0.N && K1 == m0.K1 && an == m0.anisotropy && c == cells && n == b->n) {
+        if (sscanf(line, "%d %d %d %lld %d %d %d %d %d %d %d %d %d %lf", &N, &K1, &an, &c, &n, &cp, &tx, &ty, &lp,
+                   &gq, &th, &sc, &dp, &ms) == 14 &&
+            N == m0.N && K1 == m0.K1 && an == m0.anisotropy && c == cells && n == b->n && cp == comp) {
           fclose(f);
           if (tx_out) *tx_out = tx;
           if (ty_out) *ty_out = ty;
@@ -1083,7 +1101,7 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
           if (rc == GP_OK) rc = gp_batch_set_block(b, th);
           if (rc == GP_OK) rc = gp_batch_set_scan(b, sc);
           if (rc == GP_OK) rc = gp_batch_set_depth(b, dp);
-          return rc == GP_OK ? gp_batch_set_grids(b, lp, 0) : rc;
+          return rc == GP_OK ? gp_batch_set_grids(b, lp, gq) : rc;
         }
       }
       fclose(f);
@@ -1097,28 +1115,29 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   cudaEvent_t e0, e1;
   GP_CUDA(cudaEventCreate(&e0));
   GP_CUDA(cudaEventCreate(&e1));
-  int best_tx = b->tx, best_ty = b->ty, best_lp = 0, best_th = 256, best_sc = 0, best_dp = 1;
+  int best_tx = b->tx, best_ty = b->ty, best_lp = 0, best_gq = 0, best_th = 256, best_sc = 0, best_dp = 1;
   float best = 1e30f;
   const bool nb = b->narrowband_on != 0;
   for (int s = 0; s < gp_f32_tile_shape_count(); s++) {
     int tx, ty;
     gp_f32_tile_shape(s, &tx, &ty);
     if (gp_batch_set_tile(b, tx, ty) != GP_OK) continue;
-    // full-kernel blocks of 256 and (binary alloys) 512 threads; lean grid at occupancy, or
-    // one block per SM short of it (room for full-kernel blocks); the interface tiles listed by
-    // the list kernel, or found by the full kernel's blocks themselves; single steps, or blocked
-    // pairs (two steps per lean box; list mode only)
-    for (int v = 0; v < 16; v++) {
-      const int th = v & 1 ? 512 : 256, c = (v >> 1) & 1, sc = (v >> 2) & 1, dp = v & 8 ? 2 : 1;
+    // full-kernel blocks of 256 and (binary alloys) 512 threads; lean grid at occupancy, one
+    // block per SM short of it, or half of it (room for full-kernel blocks, which share the SMs
+    // with the lean blocks); full-kernel grid at its occupancy or one block per SM short of it;
+    // the interface tiles listed by the list kernel, or found by the full kernel's blocks
+    // themselves; single steps, or blocked pairs (two steps per lean box; list mode only)
+    for (int v = 0; v < 48; v++) {
+      const int th = v & 1 ? 512 : 256, sc = (v >> 1) & 1, dp = v & 4 ? 2 : 1, cg = (v >> 3) & 1, c = v >> 4;
       if (th == 512 && !gp_f32_batch_has_wide_step(b->f32)) continue;
       if (dp == 2 && (sc || !nb)) continue;
       if (!gp_f32_batch_set_depth(b->f32, dp)) continue;
+      gp_f32_batch_set_step_threads(b->f32, th);
       int lp0, gp0, occ_l, occ_g;
       gp_f32_batch_get_grids(b->f32, &lp0, &gp0, &occ_l, &occ_g);
-      if (c && occ_l < 2) continue;
-      const int lp = c ? occ_l - 1 : 0;
-      gp_f32_batch_set_step_threads(b->f32, th);
-      gp_f32_batch_set_grids(b->f32, lp, 0);
+      if ((c == 1 && occ_l < 2) || (c == 2 && occ_l / 2 >= occ_l - 1) || (cg && occ_g < 2)) continue;
+      const int lp = c == 0 ? 0 : (c == 1 ? occ_l - 1 : occ_l / 2), gq = cg ? occ_g - 1 : 0;
+      gp_f32_batch_set_grids(b->f32, lp, gq);
       gp_f32_batch_set_scan(b->f32, sc);
       // timed as the steps run: one replay of the step graph (graph_steps steps) to warm up, four timed
       batch_drop_graphs(b);
@@ -1134,12 +1153,13 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
       ms *= 10.0f / (float)(4 * b->graph_steps);  // per 10 steps, as the cache records
       b->launches += (int64_t)5 * (b->graph_steps / dp) * batch_launches(b);
       batch_drop_graphs(b);
-      // a reduced lean grid must win by 3%: at equal speed the kernels keep their occupancy
-      if (c ? ms < 0.97f * best : ms < best) {
+      // a reduced grid must win by 3%: at equal speed the kernels keep their occupancy
+      if ((c || cg) ? ms < 0.97f * best : ms < best) {
         best = ms;
         best_tx = tx;
         best_ty = ty;
         best_lp = lp;
+        best_gq = gq;
         best_th = th;
         best_sc = sc;
         best_dp = dp;
@@ -1160,13 +1180,13 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   if (rc == GP_OK) rc = gp_batch_set_block(b, best_th);
   if (rc == GP_OK) rc = gp_batch_set_scan(b, best_sc);
   if (rc == GP_OK) rc = gp_batch_set_depth(b, best_dp);
-  if (rc == GP_OK) rc = gp_batch_set_grids(b, best_lp, 0);
+  if (rc == GP_OK) rc = gp_batch_set_grids(b, best_lp, best_gq);
   if (rc != GP_OK) return rc;
   if (cache_path) {
     FILE* f = fopen(cache_path, "a");
     if (f) {
-      fprintf(f, "%s %d %d %d %d %d %d %.6f\n", key, best_tx, best_ty, best_lp, best_th, best_sc, best_dp,
-              best / 10.0f);
+      fprintf(f, "%s %d %d %d %d %d %d %d %.6f\n", key, best_tx, best_ty, best_lp, best_gq, best_th, best_sc,
+              best_dp, best / 10.0f);
       fclose(f);
     }
   }
@@ -1226,6 +1246,16 @@ extern "C" int gp_batch_set_depth(gp_batch* b, int depth) {
 }
 
 extern "C" int gp_batch_get_depth(gp_batch* b) { return b ? gp_f32_batch_depth(b->f32) : 0; }
+
+extern "C" int gp_batch_set_compensated(gp_batch* b, int on) {
+  if (!b) return GP_E_ARG;
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  GP_CUDA(gp_f32_batch_set_compensated(b->f32, on));
+  batch_drop_graphs(b);  // the graphs hold the lean kernels of the previous mode
+  return GP_OK;
+}
+
+extern "C" int gp_batch_get_compensated(gp_batch* b) { return b ? gp_f32_batch_compensated(b->f32) : 0; }
 
 extern "C" int gp_batch_test_lose_box(gp_batch* b) {
   if (!b) return GP_E_ARG;

@@ -22,6 +22,7 @@
 
 #include <cuda.h>
 #include <stdio.h>
+#include <stddef.h>
 #include <string.h>
 
 #include <vector>
@@ -55,6 +56,8 @@ struct alignas(16) Model {
   float DC[MP][MK][MK];  // sum_k Diff[b][i][k] * cmu[b][k][j]: D(phi) = sum_b DC_b phi_b
   float atf[MP][MK];     // 1 - Diff[a][k][k] / Diff[N-1][k][k]
   float H[MP][MK][MK];   // d mu / d c of phase b (2 A_kk on the diagonal, A_kl off it): bulk mu += H dc
+  int comp;              // compensated flux accumulation (error-free transforms, gp_batch_set_compensated)
+  int pad3[3];
   float Gx[MP][MK][MK];  // pure-phase update: mu += Gx Lx + Gy Ly, Gx = H (2 DC) dt / (2 dx^2)
   float Gy[MP][MK][MK];
   float pad2[2];
@@ -194,18 +197,55 @@ __device__ __forceinline__ float flux_div(float fxp, float fxm, float fyp, float
   return __fadd_rn(__fsub_rn(fxp, fxm), __fsub_rn(fyp, fym));
 }
 
+// Error-free transforms (Knuth's TwoSum; TwoProduct with the fused multiply-add), explicit
+// round-to-nearest: s + e == a + b and p + e == a * b exactly.
+__device__ __forceinline__ float two_sum(float a, float b, float& e) {
+  const float s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+  return s;
+}
+__device__ __forceinline__ float two_prod(float a, float b, float& e) {
+  const float p = __fmul_rn(a, b);
+  e = __fmaf_rn(a, b, -p);
+  return p;
+}
+
+// Compensated flux accumulation: the net face flux with the rounding errors of its three
+// additions summed separately and added once (the flux differences cancel in smooth fields).
+__device__ __forceinline__ float flux_div_c(float fxp, float fxm, float fyp, float fym) {
+  float e1, e2, e3;
+  const float a = two_sum(fxp, -fxm, e1), b = two_sum(fyp, -fym, e2);
+  const float s = two_sum(a, b, e3);
+  return __fadd_rn(s, __fadd_rn(__fadd_rn(e1, e2), e3));
+}
+
 // Bulk cell of phase b whose face fluxes dc were evaluated (a neighbour is not
 // pure b): c -> c + dc, mu = dF/dc (calculate_divergence_concentration.h:216-224)
 // is, for quadratic free energies, mu + H dc with H = d mu / d c of the phase;
 // the FP32 form evaluates it that way (one rounding at mu's scale).
 template <int K1>
 __device__ __forceinline__ void bulk_update_h(const float (&H)[MK][MK], const float* mu, const float* dc,
-                                              float* mnew) {
+                                              float* mnew, bool comp = false) {
 #pragma unroll
   for (int k = 0; k < K1; k++) {
-    float s = __fmul_rn(H[k][0], dc[0]);
+    float s, c = 0.f;
+    if (comp) {  // compensated dot product (Dot2): products and sums error-free, errors summed apart
+      float ep, es;
+      s = two_prod(H[k][0], dc[0], ep);
+      c = ep;
 #pragma unroll
-    for (int l = 1; l < K1; l++) s = __fmaf_rn(H[k][l], dc[l], s);
+      for (int l = 1; l < K1; l++) {
+        const float p = two_prod(H[k][l], dc[l], ep);
+        s = two_sum(s, p, es);
+        c = __fadd_rn(c, __fadd_rn(ep, es));
+      }
+      s = __fadd_rn(s, c);
+    } else {
+      s = __fmul_rn(H[k][0], dc[0]);
+#pragma unroll
+      for (int l = 1; l < K1; l++) s = __fmaf_rn(H[k][l], dc[l], s);
+    }
     mnew[k] = __fadd_rn(mu[k], s);
   }
 }
@@ -221,8 +261,38 @@ __device__ __forceinline__ void bulk_update_h(const float (&H)[MK][MK], const fl
 template <int K1>
 __device__ __forceinline__ void pure_update(const float (&gx)[MK][MK], const float (&gy)[MK][MK], const float* mu,
                                             const float* dxp, const float* dxm, const float* dyp, const float* dym,
-                                            float* mnew) {
+                                            float* mnew, bool comp = false) {
   float Lx[K1], Ly[K1];
+  if (comp) {
+    // compensated: the Laplacians' rounding errors and the increment's products and sums are
+    // carried separately (TwoSum, TwoProduct) and added to the increment once
+    float eLx[K1], eLy[K1];
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      Lx[k] = two_sum(dxp[k], -dxm[k], eLx[k]);
+      Ly[k] = two_sum(dyp[k], -dym[k], eLy[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      float ep, es, c;
+      float s = two_prod(gy[k][0], Ly[0], ep);
+      c = __fmaf_rn(gy[k][0], eLy[0], ep);
+      float p = two_prod(gx[k][0], Lx[0], ep);
+      s = two_sum(s, p, es);
+      c = __fadd_rn(c, __fadd_rn(__fmaf_rn(gx[k][0], eLx[0], ep), es));
+#pragma unroll
+      for (int l = 1; l < K1; l++) {
+        p = two_prod(gy[k][l], Ly[l], ep);
+        s = two_sum(s, p, es);
+        c = __fadd_rn(c, __fadd_rn(__fmaf_rn(gy[k][l], eLy[l], ep), es));
+        p = two_prod(gx[k][l], Lx[l], ep);
+        s = two_sum(s, p, es);
+        c = __fadd_rn(c, __fadd_rn(__fmaf_rn(gx[k][l], eLx[l], ep), es));
+      }
+      mnew[k] = __fadd_rn(mu[k], __fadd_rn(s, c));
+    }
+    return;
+  }
 #pragma unroll
   for (int k = 0; k < K1; k++) {
     Lx[k] = __fsub_rn(dxp[k], dxm[k]);
@@ -540,7 +610,7 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
           dyp[k] = __fsub_rn(mr[k], mc[k]);
           dym[k] = __fsub_rn(mc[k], ml[k]);
         }
-        pure_update<K1>(gx, gy, mc, dxp, dxm, dyp, dym, mnew);
+        pure_update<K1>(gx, gy, mc, dxp, dxm, dyp, dym, mnew, m.comp);
         const int64_t o = (int64_t)x * I.pitch + y;
 #pragma unroll
         for (int k = 0; k < K1; k++) I.mu_out[o + k * I.plane] = mnew[k];
@@ -937,8 +1007,9 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
 #pragma unroll
       for (int k = 0; k < K1; k++) {
         mu[k] = MU(k, i1, j1);
-        dc[k] = flux_div(sfx[(k * (TX + 1) + ti + 1) * TY + tj], sfx[(k * (TX + 1) + ti) * TY + tj],
-                         sfy[(k * TX + ti) * (TY + 1) + tj + 1], sfy[(k * TX + ti) * (TY + 1) + tj]);
+        const float fxp_ = sfx[(k * (TX + 1) + ti + 1) * TY + tj], fxm_ = sfx[(k * (TX + 1) + ti) * TY + tj];
+        const float fyp_ = sfy[(k * TX + ti) * (TY + 1) + tj + 1], fym_ = sfy[(k * TX + ti) * (TY + 1) + tj];
+        dc[k] = m.comp ? flux_div_c(fxp_, fxm_, fyp_, fym_) : flux_div(fxp_, fxm_, fyp_, fym_);
       }
       int bulk = -1;
 #pragma unroll
@@ -965,14 +1036,16 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
             dyp[k] = __fsub_rn(MU(k, i1, j1 + 1), mu[k]);
             dym[k] = __fsub_rn(mu[k], MU(k, i1, j1 - 1));
           }
-          pure_update<K1>(gx, gy, mu, dxp, dxm, dyp, dym, mnew);
+          pure_update<K1>(gx, gy, mu, dxp, dxm, dyp, dym, mnew, m.comp);
         } else {
           float hb[MK][MK];
           phase_mat<N, K1>(m.H, bulk, hb);
-          bulk_update_h<K1>(hb, mu, dc, mnew);
+          bulk_update_h<K1>(hb, mu, dc, mnew, m.comp);
         }
       } else {
-        float hh[N];
+        float hh[N], dce[K1];
+#pragma unroll
+        for (int k = 0; k < K1; k++) dce[k] = 0.f;
 #pragma unroll
         for (int a = 0; a < N; a++) hh[a] = hphi<N>(ph, a);
         // dc -= sum_a c_a(mu) * dh_a/dt
@@ -982,8 +1055,20 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
 #pragma unroll
           for (int b = 0; b < N; b++) sdh += dhphi<N>(ph, a, b) * dp[b];
 #pragma unroll
-          for (int k = 0; k < K1; k++) dc[k] -= c_mu<K1>(m, mu, a, k) * sdh;
+          for (int k = 0; k < K1; k++) {
+            if (m.comp) {  // compensated: the product and the difference error-free, errors kept in dce
+              float ep, es;
+              const float pr = two_prod(c_mu<K1>(m, mu, a, k), sdh, ep);
+              dc[k] = two_sum(dc[k], -pr, es);
+              dce[k] = __fadd_rn(dce[k], __fsub_rn(es, ep));
+            } else {
+              dc[k] -= c_mu<K1>(m, mu, a, k) * sdh;
+            }
+          }
         }
+        if (m.comp)
+#pragma unroll
+          for (int k = 0; k < K1; k++) dc[k] = __fadd_rn(dc[k], dce[k]);
         if (K1 == 1) {
           float d = 0.f;
 #pragma unroll
@@ -1255,7 +1340,7 @@ __device__ __forceinline__ void lean_ghosts(bool on, const Inst& I, int x0, int 
 // index in the tile).  A tile inside the grid stores its rows without bounds
 // tests; an edge tile tests rows and columns.  The phi of a tile whose output
 // buffer does not hold the one-hot field of b yet is written in a second pass.
-template <int N, int K1, int TX, int TY>
+template <int N, int K1, int TX, int TY, bool COMP>
 __device__ __forceinline__ void lean_compute(const Inst& I, const LeanConst& C, bool write_phi, int b, int x0, int y0,
                                              const float* buf, int sub) {
   using S = Lean<N, K1, TX, TY>;
@@ -1310,7 +1395,7 @@ __device__ __forceinline__ void lean_compute(const Inst& I, const LeanConst& C, 
       float dxp[K1];
 #pragma unroll
       for (int k = 0; k < K1; k++) dxp[k] = __fsub_rn(nx[j][k], cur[j][k]);
-      pure_update<K1>(gx, gy, cur[j], dxp, dxm[j], dy[j + 1], dy[j], mnew[j]);
+      pure_update<K1>(gx, gy, cur[j], dxp, dxm[j], dy[j + 1], dy[j], mnew[j], COMP);
 #pragma unroll
       for (int k = 0; k < K1; k++) dxm[j][k] = dxp[k];
     }
@@ -1374,7 +1459,7 @@ __device__ __forceinline__ void lean_compute(const Inst& I, const LeanConst& C, 
 // starts on the tiles the previous step wrote last, whose mu is still in L2.  A stage whose boxes
 // have not arrived after one second sets *err; the warp then waits (bounded)
 // for its other boxes and returns.
-template <int N, int K1, int TX, int TY>
+template <int N, int K1, int TX, int TY, bool COMP>
 __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
     k_lean32(const Inst* __restrict__ insts, const LeanConst* __restrict__ lconst,
              const CUtensorMap* __restrict__ tmaps, const int4* __restrict__ tile_desc,
@@ -1473,7 +1558,7 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
     float* buf = slots + (s * TPW + q) * (S::SLOT / 4);
     const bool edge = own && (e.z == 0 || e.z + TX >= I.mx || e.w == 0 || e.w + TY >= I.my);
     if (__any_sync(0xffffffffu, edge)) lean_ghosts<N, K1, TX, TY>(edge, I, e.z, e.w, buf, sub);
-    if (own) lean_compute<N, K1, TX, TY>(I, C, write_phi, b, e.z, e.w, buf, sub);
+    if (own) lean_compute<N, K1, TX, TY, COMP>(I, C, write_phi, b, e.z, e.w, buf, sub);
     __syncwarp();
     if (own && sub == 0) flags_out[e.x] = pf_all(1 + b);
   }
@@ -1530,7 +1615,7 @@ struct Lean2 {
 // Every lane runs RS rows (the shuffles need the whole warp); rows at or past
 // r1 are computed from clamped rows and not stored.  put(r, mnew) stores a
 // row's four new cells.
-template <int K1, int R, int W, int RS, typename Put>
+template <int K1, int R, int W, int RS, bool COMP, typename Put>
 __device__ __forceinline__ void lean_sweep(const float* __restrict__ src, int c0, int r0, int r1, bool ld_left,
                                            bool ld_right, const float (&gx)[MK][MK], const float (&gy)[MK][MK],
                                            Put put) {
@@ -1577,7 +1662,7 @@ __device__ __forceinline__ void lean_sweep(const float* __restrict__ src, int c0
       float dxp[K1];
 #pragma unroll
       for (int k = 0; k < K1; k++) dxp[k] = __fsub_rn(nx[j][k], cur[j][k]);
-      pure_update<K1>(gx, gy, cur[j], dxp, dxm[j], dy[j + 1], dy[j], mnew[j]);
+      pure_update<K1>(gx, gy, cur[j], dxp, dxm[j], dy[j + 1], dy[j], mnew[j], COMP);
 #pragma unroll
       for (int k = 0; k < K1; k++) dxm[j][k] = dxp[k];
     }
@@ -1674,7 +1759,7 @@ __global__ void __launch_bounds__(256) k_adj_list(const int4* __restrict__ tile_
 // mu_out, purity words flags_x) for the full kernel's second pass.  Otherwise
 // the lean tiles not next to the list, found by scanning.  Bounded waits as
 // k_lean32.
-template <int N, int K1, int TX, int TY>
+template <int N, int K1, int TX, int TY, bool COMP>
 __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
     k_lean2(const Inst* __restrict__ insts, const Inst* __restrict__ insts_x, const LeanConst* __restrict__ lconst,
             const CUtensorMap* __restrict__ tmaps, const int4* __restrict__ tile_desc,
@@ -1785,7 +1870,7 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
         gy[k][l] = C.gy[k][l];
       }
     // sub-step 1: rows x0-1 .. x0+TX of step t+1 into mid
-    lean_sweep<K1, R2, W, S::RS1>(box, c1, a1, e1, false, false, gx, gy, [&](int r, const float (&v)[4][K1]) {
+    lean_sweep<K1, R2, W, S::RS1, COMP>(box, c1, a1, e1, false, false, gx, gy, [&](int r, const float (&v)[4][K1]) {
 #pragma unroll
       for (int k = 0; k < K1; k++)
         *reinterpret_cast<float4*>(mid + (k * R1 + r) * W + c1) = make_float4(v[0][k], v[1][k], v[2][k], v[3][k]);
@@ -1825,7 +1910,7 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
       const int yb = y0 + 4 * g2;
       const bool full = x0 + TX <= mx && y0 + TY <= my;
       float* const out = I.mu_out + (int64_t)x0 * I.pitch + yb;
-      lean_sweep<K1, R1, W, S::RS2>(
+      lean_sweep<K1, R1, W, S::RS2, COMP>(
           mid, 4 + 4 * g2, a2, e2, g2 == 0, g2 == Q2 - 1, gx, gy, [&](int r, const float (&v)[4][K1]) {
             if (full) {
 #pragma unroll
@@ -1982,6 +2067,10 @@ struct KernelSet {
                 uint32_t*, uint32_t*, const uint8_t*, int, int, const int4*, const int*, int*);
   void (*list)(const int4*, const uint32_t*, int, int2*, int*, uint8_t*, int);
   size_t smem_general, smem_lean, smem_lean2;
+  // the lean kernels with compensated accumulation (a template switch: the plain ones keep
+  // their registers)
+  decltype(lean) lean_c;
+  decltype(lean2) lean2_c;
 };
 
 template <int N, int K1, bool AN, int TX, int TY>
@@ -1990,8 +2079,10 @@ static KernelSet make_set() {
   k.general = k_step32<N, K1, AN, TX, TY>;
   k.general_wide = nullptr;
   if constexpr (N == 2 && K1 == 1) k.general_wide = k_step32<N, K1, AN, TX, TY, 512>;
-  k.lean = k_lean32<N, K1, TX, TY>;
-  k.lean2 = k_lean2<N, K1, TX, TY>;
+  k.lean = k_lean32<N, K1, TX, TY, false>;
+  k.lean2 = k_lean2<N, K1, TX, TY, false>;
+  k.lean_c = k_lean32<N, K1, TX, TY, true>;
+  k.lean2_c = k_lean2<N, K1, TX, TY, true>;
   k.list = k_general_list<TX, TY>;
   k.smem_general = Tile<N, K1, AN, TX, TY>::bytes;
   k.smem_lean = Lean<N, K1, TX, TY>::smem;
@@ -2040,6 +2131,7 @@ struct gp_f32_batch {
   int narrowband = 1;    // send the tiles lean_phase accepts to the lean kernel
   int depth = 1;         // steps per blocked launch: 1, or 2 (lean tiles two steps per box; needs X)
   int has_x = 0;         // intermediate buffers X bound (gp_f32_batch_bind_x)
+  int comp = 0;          // compensated accumulation (Model::comp of every instance, lean_c / lean2_c)
   std::vector<Inst> hinst_x1[2], hinst_x2[2];  // [parity] buffer p -> X, X -> buffer p^1
   Inst* dinst_x1[2] = {nullptr, nullptr};
   Inst* dinst_x2[2] = {nullptr, nullptr};
@@ -2049,6 +2141,7 @@ struct gp_f32_batch {
   cudaEvent_t ev_list = nullptr, ev_adj = nullptr;
   cudaStream_t side2 = nullptr;  // blocked pairs: the lean tiles next to the full kernel's list
   int grid_lean2 = 0, occ_lean2 = 0;
+  int occ_lean_by[2] = {1, 1}, occ_lean2_by[2] = {1, 1};  // plain, compensated lean kernels
   int lose_box = 0;      // failure-detection test: the next lean launch loses one stage's boxes
   std::vector<gp_model> gm;
   std::vector<Inst> hinst[2];  // [buffer parity]
@@ -2316,6 +2409,25 @@ void gp_f32_batch_get_grids(const gp_f32_batch* b, int* lean_per_sm, int* genera
 
 // Steps per blocked launch: 1, or 2 (needs the intermediate buffers X and the
 // list way of finding the interface tiles).  False if unavailable.
+// Compensated accumulation on or off: the comp word of every instance's Model (read by the
+// full kernel; synchronous copies: the caller has drained the batch's streams) and the lean
+// kernels' template variant (the caller drops graphs captured with the other one).
+cudaError_t gp_f32_batch_set_compensated(gp_f32_batch* b, int on) {
+  const int v = on ? 1 : 0;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < b->n && e == cudaSuccess; i++)
+    e = cudaMemcpy(reinterpret_cast<char*>(b->dmodel + i) + offsetof(Model, comp), &v, sizeof v,
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    b->comp = v;
+    b->occ_lean = b->occ_lean_by[v];
+    b->occ_lean2 = b->occ_lean2_by[v];
+    if (b->sms) set_grids(b);
+  }
+  return e;
+}
+int gp_f32_batch_compensated(const gp_f32_batch* b) { return b->comp; }
+
 bool gp_f32_batch_set_depth(gp_f32_batch* b, int depth) {
   if (depth != 1 && !(depth == 2 && b->has_x)) return false;
   b->depth = depth;
@@ -2397,14 +2509,25 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
       e = cudaFuncSetAttribute(ks.general_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_general);
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_w, ks.general_wide, 512, ks.smem_general);
   }
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(ks.lean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_lean);
-  if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, ks.lean, 32 * GP_LEAN_WARPS, ks.smem_lean);
   int occ_l2 = 0;
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(ks.lean2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_lean2);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l2, ks.lean2, 32 * 4, ks.smem_lean2);
+  for (int c = 0; c < 2 && e == cudaSuccess; c++) {
+    const void* fl = c ? (const void*)ks.lean_c : (const void*)ks.lean;
+    const void* fl2 = c ? (const void*)ks.lean2_c : (const void*)ks.lean2;
+    int ol = 0, ol2 = 0;
+    if (c) e = cudaFuncSetAttribute(fl, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (c && e == cudaSuccess)
+      e = cudaFuncSetAttribute(fl2, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_lean);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ol, fl, 32 * GP_LEAN_WARPS, ks.smem_lean);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(fl2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.smem_lean2);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ol2, fl2, 32 * 4, ks.smem_lean2);
+    b->occ_lean_by[c] = ol > 0 ? ol : 1;
+    b->occ_lean2_by[c] = ol2 > 0 ? ol2 : 1;
+  }
   if (e != cudaSuccess) return e;
+  occ_l = b->occ_lean_by[b->comp];
+  occ_l2 = b->occ_lean2_by[b->comp];
   b->occ_lean2 = occ_l2 > 0 ? occ_l2 : 1;
   b->sms = sms;
   b->occ_general_by[0] = occ_g > 0 ? occ_g : 1;
@@ -2515,7 +2638,7 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   if (E && ((e = cudaEventRecord(E[0], ls)) != cudaSuccess)) return e;
   if (b->lose_box)  // failure-detection test: a nonzero token, taken by one warp
     if ((e = cudaMemsetAsync(b->derr + 1, 1, sizeof(int), ls)) != cudaSuccess) return e;
-  k.lean<<<b->grid_lean, 32 * GP_LEAN_WARPS, k.smem_lean, ls>>>(b->dinst[p], b->dlconst, b->dtmap[p], b->dtile_desc, flags_in,
+  (b->comp ? k.lean_c : k.lean)<<<b->grid_lean, 32 * GP_LEAN_WARPS, k.smem_lean, ls>>>(b->dinst[p], b->dlconst, b->dtmap[p], b->dtile_desc, flags_in,
                                                  flags_out, b->total_tiles, p, b->lose_box, b->derr);
   b->lose_box = 0;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -2574,7 +2697,7 @@ cudaError_t gp_f32_batch_launch_pair(gp_f32_batch* b, int parity, cudaStream_t s
                                                            b->dalist, b->dcnt);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   for (int adj = 1; adj >= 0; adj--) {
-    k.lean2<<<b->grid_lean2, 128, k.smem_lean2, adj ? as : ls>>>(
+    (b->comp ? k.lean2_c : k.lean2)<<<b->grid_lean2, 128, k.smem_lean2, adj ? as : ls>>>(
         b->dinst[p], b->dinst_x1[p], b->dlconst, b->dtmap2[p], b->dtile_desc, flags_in, flags_out, flags_x, b->dgen,
         b->total_tiles, p, adj ? b->dalist : nullptr, adj ? b->dcnt + 4 : nullptr, b->derr);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -3,7 +3,8 @@
 
     python -m microsim_b200.profile_step [--workload c4|c2|c1] [--state FILE]
                                          [--tile TX TY] [--steps S] [--full]
-                                         [--depth 1|2] [--lean-per-sm L] [--fp64]
+                                         [--depth 1|2] [--lean-per-sm L] [--general-per-sm G]
+                                         [--compensated 0|1] [--fp64]
 
 The workload's state is first advanced as the benchmark does (the batched
 sweep 2,500 steps, the 1024^2 dendrite 25,000, the 200^2 seed 5,000); with
@@ -11,7 +12,9 @@ sweep 2,500 steps, the 1024^2 dendrite 25,000, the 200^2 seed 5,000); with
 later ones, so a profiled run launches only a handful of kernels before the
 range.  --full switches the narrow band off (every tile through the full
 kernel); --depth 2 steps in blocked pairs (two steps per lean box);
---lean-per-sm sets the lean grid's blocks per SM (0: occupancy); --fp64
+--lean-per-sm and --general-per-sm set the lean and full kernels' blocks per
+SM (0: occupancy); --compensated 1 the compensated FP32 accumulation (default
+0, plain, as the benchmark's headline); --fp64
 profiles the plain FP64 step of the workload's first instance instead.
 """
 from __future__ import annotations
@@ -35,6 +38,8 @@ def main(argv=None):
     ap.add_argument("--full", action="store_true")
     ap.add_argument("--depth", type=int, default=1, choices=[1, 2])
     ap.add_argument("--lean-per-sm", type=int, default=0)
+    ap.add_argument("--general-per-sm", type=int, default=0)
+    ap.add_argument("--compensated", type=int, default=0, choices=[0, 1])
     ap.add_argument("--fp64", action="store_true")
     a = ap.parse_args(argv)
     cases = {"c4": configs.c4, "c2": lambda: [configs.c2(literal=False, steps=50000)],
@@ -47,6 +52,7 @@ def main(argv=None):
     else:
         prep = {"c4": 2500, "c2": 25000, "c1": 5000}[a.workload]
         with mb.Batch(models) as b:
+            b.set_compensated(a.compensated == 1)
             for i, (_, p, u) in enumerate(loaded):
                 b.upload(i, p, u)
             b.step(prep)
@@ -71,7 +77,8 @@ def main(argv=None):
         b.set_narrowband(not a.full)
         if not a.full:
             b.set_depth(a.depth)
-        b.set_grids(a.lean_per_sm, 0)
+        b.set_grids(a.lean_per_sm, a.general_per_sm)
+        b.set_compensated(a.compensated == 1)
         for i, f in enumerate(fields):
             b.upload(i, *f)
         b.step(3)

@@ -152,7 +152,7 @@ def test_autotune_restores_state_and_caches(tmp_path):
         after = b.download(0)
         assert (tx, ty) in [(16, 32), (8, 32), (32, 32), (16, 64)]
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
-        assert os.path.exists(cache) and len(open(cache).read().split()) == 12
+        assert os.path.exists(cache) and len(open(cache).read().split()) == 14
         assert b.autotune(cache) == (tx, ty)  # read back from the cache
 
 
@@ -274,7 +274,7 @@ def test_two_step_blocking_is_bit_identical_to_single_steps():
             assert b.depth() == depth
             for i, (_, p, u) in enumerate(loaded):
                 b.upload(i, p, u)
-            b.step(150)  # 16-step graphs of both parities (9 replays), then pairs
+            b.step(150)  # 4-step graphs of both parities, then pairs
             if reupload:
                 for i, st in enumerate([b.download(i) for i in range(len(models))]):
                     b.upload(i, *st)
@@ -297,6 +297,59 @@ def test_two_step_blocking_is_bit_identical_to_single_steps():
             b.step(120)
             res.append(b.download(0))
     assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+def test_compensated_accumulation():
+    """Compensated (TwoSum/TwoProduct) accumulation: on for a context and a batch,
+    refused for FP64; the results change bits, stay within the FP32 tolerances of
+    the FP64 form, and stay bit-identical across the narrow band, tile shapes and
+    two-step blocking (every kernel shares the compensated pure-phase rule)."""
+    m, phi, mu = mb.load_case(BINARY["aniso_corner"])
+    with mb.Context(m, mb.GP_FP64) as c64:
+        with pytest.raises(RuntimeError):
+            c64.set_compensated(True)
+        assert not c64.compensated()
+        c64.upload(phi, mu)
+        c64.step(400)
+        p64, u64 = c64.download()
+        s64 = c64.stats()
+    res = {}
+    for comp in (False, True):
+        with mb.Context(m, mb.GP_FP32) as c:
+            c.set_compensated(comp)
+            assert c.compensated() == comp
+            c.upload(phi, mu)
+            c.step(400)
+            res[comp] = (*c.download(), c.stats())
+    assert not np.array_equal(res[True][1], res[False][1])
+    p32, u32, s32 = res[True]
+    assert np.abs(p32 - p64).max() <= 2e-5
+    assert np.abs(u32 - u64).max() <= 1e-4
+    np.testing.assert_allclose(s32["solute"], s64["solute"], rtol=1e-4)
+
+    cases = [configs.binary_case(200, 150, gap=1.0, supersat=0.55, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
+                                 seed=(0, 0, 8.0)),
+             configs.binary_case(129, 161, gap=1.0, supersat=0.5, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
+                                 seed=(128, 160, 10.0))]
+    loaded = [mb.load_case(c) for c in cases]
+    models = [mm for mm, _, _ in loaded]
+
+    def run(nb, depth, tile):
+        with mb.Batch(models) as b:
+            b.set_compensated(True)
+            assert b.compensated()
+            b.set_tile(*tile)
+            b.set_narrowband(nb)
+            b.set_depth(depth)
+            for i, (_, p, u) in enumerate(loaded):
+                b.upload(i, p, u)
+            b.step(101)
+            return [b.download(i) for i in range(len(models))]
+
+    ref = run(False, 1, (16, 32))
+    for nb, depth, tile in [(True, 1, (16, 32)), (True, 2, (16, 32)), (True, 2, (8, 32)), (True, 1, (32, 32))]:
+        for (p1, u1), (p0, u0) in zip(run(nb, depth, tile), ref):
+            assert np.array_equal(p1, p0) and np.array_equal(u1, u0), (nb, depth, tile)
 
 
 def test_two_step_blocking_timing_and_stats():
