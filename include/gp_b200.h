@@ -301,6 +301,11 @@ int gp_batch_get_scan(gp_batch *b);
  * rel_change_* of gp_batch_get_stats covers the pair's two steps. */
 int gp_batch_set_depth(gp_batch *b, int depth);
 int gp_batch_get_depth(gp_batch *b);
+/* The frozen temperature gradient's clock of a batch (gp_set_time_step for a
+ * context): the number of steps taken, which the next step's temperature
+ * depends on (microsim_gp.c:108-113).  Counted by gp_batch_step; set it when
+ * resuming a run. */
+int gp_batch_set_time_step(gp_batch *b, int64_t t);
 /* Compensated accumulation for every instance of the batch (gp_set_compensated). */
 int gp_batch_set_compensated(gp_batch *b, int on);
 int gp_batch_get_compensated(gp_batch *b);

@@ -135,6 +135,7 @@ _SIGS = {
     "gp_batch_state_changed": (C.c_int, [C.c_void_p]),
     "gp_batch_get_depth": (C.c_int, [C.c_void_p]),
     "gp_batch_set_compensated": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_batch_set_time_step": (C.c_int, [C.c_void_p, C.c_int64]),
     "gp_batch_get_compensated": (C.c_int, [C.c_void_p]),
     "gp_batch_test_lose_box": (C.c_int, [C.c_void_p]),
     "gp_batch_get_grids": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -483,6 +484,10 @@ class Batch:
 
     def depth(self) -> int:
         return lib().gp_batch_get_depth(self._h)
+
+    def set_time_step(self, t: int):
+        """The step count the frozen temperature gradient is evaluated at (steps taken)."""
+        _check("gp_batch_set_time_step", lib().gp_batch_set_time_step(self._h, int(t)))
 
     def set_compensated(self, on: bool):
         """Compensated (error-free transform) accumulation of the FP32 updates."""

@@ -53,6 +53,7 @@ bool gp_f32_batch_set_depth(gp_f32_batch* b, int depth);
 int gp_f32_batch_depth(const gp_f32_batch* b);
 cudaError_t gp_f32_batch_set_compensated(gp_f32_batch* b, int on);
 int gp_f32_batch_compensated(const gp_f32_batch* b);
+cudaError_t gp_f32_batch_set_tstep(gp_f32_batch* b, long long t, cudaStream_t s);
 cudaError_t gp_f32_batch_launch_pair(gp_f32_batch* b, int parity, cudaStream_t s);
 int gp_f32_batch_launches_per_pair(const gp_f32_batch* b);
 int gp_f32_tile_shape_count();
@@ -352,6 +353,7 @@ extern "C" int gp_get_compensated(gp_ctx* c) {
 extern "C" int gp_set_time_step(gp_ctx* c, int64_t t) {
   if (!c || t < 0) return GP_E_ARG;
   c->tstep = t;
+  if (c->precision == GP_FP32) GP_CUDA(gp_f32_batch_set_tstep(c->f32, (long long)t, c->stream));
   return GP_OK;
 }
 
@@ -804,6 +806,7 @@ struct gp_batch {
   int have_prev = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_steps = 4;  // steps per captured graph (two blocked pairs at depth 2)
+  int64_t tstep = 0;    // steps taken (the frozen gradient's clock)
   double* partials = nullptr;
   double* reduced = nullptr;
   double* stage = nullptr;  // device staging of FP64 host fields (kept between copies)
@@ -971,6 +974,7 @@ static int batch_capture(gp_batch* b, int parity) {
 
 extern "C" int gp_batch_step(gp_batch* b, int64_t nsteps) {
   if (!b || nsteps < 0) return GP_E_ARG;
+  b->tstep += nsteps;
   if (b->lose_pending && nsteps > 0) {  // failure-detection test: one direct step that loses a box
     b->lose_pending = 0;
     gp_f32_batch_test_lose_box(b->f32);
@@ -1031,7 +1035,7 @@ extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
   const int cur = b->parity, prv = 1 - b->parity;
   k_stats<float><<<b->red_blocks, 256, 0, b->stream>>>(
       m, b->pool + b->off_phi[cur][i], b->pool + b->off_mu[cur][i], b->pool + b->off_phi[prv][i],
-      b->pool + b->off_mu[prv][i], b->have_prev, b->pitch[i], b->plane[i], b->partials, gp_temp_after(m, 0));
+      b->pool + b->off_mu[prv][i], b->have_prev, b->pitch[i], b->plane[i], b->partials, gp_temp_after(m, b->tstep));
   GP_CUDA(cudaGetLastError());
   k_stats_final<<<1, 64, 0, b->stream>>>(m.N, m.K1, b->partials, b->red_blocks, b->reduced,
                                          gp_f32_batch_error_word(b->f32));
@@ -1176,6 +1180,7 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   GP_CUDA(cudaFreeAsync(backup, b->stream));
   b->parity = saved_parity;
   b->have_prev = saved_prev;
+  GP_CUDA(gp_f32_batch_set_tstep(b->f32, (long long)b->tstep, b->stream));  // the trial steps advanced it
   int rc = gp_batch_set_tile(b, best_tx, best_ty);
   if (rc == GP_OK) rc = gp_batch_set_block(b, best_th);
   if (rc == GP_OK) rc = gp_batch_set_scan(b, best_sc);
@@ -1246,6 +1251,14 @@ extern "C" int gp_batch_set_depth(gp_batch* b, int depth) {
 }
 
 extern "C" int gp_batch_get_depth(gp_batch* b) { return b ? gp_f32_batch_depth(b->f32) : 0; }
+
+extern "C" int gp_batch_set_time_step(gp_batch* b, int64_t t) {
+  if (!b || t < 0) return GP_E_ARG;
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  b->tstep = t;
+  GP_CUDA(gp_f32_batch_set_tstep(b->f32, (long long)t, b->stream));
+  return GP_OK;
+}
 
 extern "C" int gp_batch_set_compensated(gp_batch* b, int on) {
   if (!b) return GP_E_ARG;

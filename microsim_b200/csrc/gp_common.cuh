@@ -55,7 +55,7 @@ struct gp_temp_step {
 
 // temp_bottom and GRADIENT after step t (t = 0: the initial temperature), microsim_gp.c:77-82 and
 // 108-113 in their operation order (no moving frame: shift_OFFSET = 0).
-static inline gp_temp_step gp_temp_after(const gp_model &m, int64_t t) {
+__host__ __device__ inline gp_temp_step gp_temp_after(const gp_model &m, int64_t t) {
   gp_temp_step s;
   const double shift_offset = 0.0;
   const double base_pos = t == 0 ? (m.tg_offset / m.dy) - shift_offset

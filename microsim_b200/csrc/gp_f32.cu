@@ -78,6 +78,10 @@ struct alignas(16) Inst {
   int model;       // index into the model array
   int tiles_x;     // tiles along x
   gp_bc bc;
+  // non-isothermal frozen gradient (nullptr when isothermal): the instance's FP64 model and the
+  // batch's step counter (the step the kernels compute; advanced after every full-kernel pass)
+  const gp_model* gm;
+  const long long* tstep;
 };
 
 template <int N>
@@ -124,6 +128,17 @@ __device__ __forceinline__ float c_mu(const Model& m, const float* mu, int a, in
   float s = 0.f;
 #pragma unroll
   for (int k = 0; k < K1; k++) s += m.cmu[a][i][k] * (mu[k] - m.Beff[a][k]);
+  return s;
+}
+
+// c_mu at a cell's temperature: beff = the Beff(T)[N][K1] block of the cell's row of the tile's
+// temperature table, or nullptr (isothermal: the model's Beff)
+template <int K1>
+__device__ __forceinline__ float c_mu_t(const Model& m, const float* mu, int a, int i, const float* beff) {
+  if (!beff) return c_mu<K1>(m, mu, a, i);
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < K1; k++) s += m.cmu[a][i][k] * (mu[k] - beff[a * K1 + k]);
   return s;
 }
 
@@ -346,6 +361,13 @@ struct Tile {
   static constexpr int o_act = o_list + X1 * Y1;                  // active flags (ints) [X1*Y1]
   static constexpr int total = o_act + X1 * Y1;
   static constexpr size_t bytes = total * sizeof(float);
+  // non-isothermal instances only (added to the launch's dynamic shared memory): the
+  // T-dependent constants of the tile's columns y0-1 .. y0+TY, [2][Y1][RT] -- variant 0 for the
+  // phase-field half step, 1 for the concentration half step (they differ on ghost columns) --
+  // a row holding Beff(T)[N][K1], B(T)[N][K1], C(T)[N]
+  static constexpr int RT = 2 * N * K1 + N;
+  static constexpr int o_temp = total;
+  static constexpr size_t bytes_temp = (size_t)2 * Y1 * RT * sizeof(float);
 };
 
 // Asynchronous global -> shared copies (cp.async), completed per thread by
@@ -627,6 +649,34 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
   // flagged and compacted into a list; gradient-energy brackets are evaluated
   // only on faces next to an active cell; Delta-phi is computed for the listed
   // cells (calculate_divergence_phasefield.h:4-62).
+  // Non-isothermal instances first tabulate the T-dependent constants of the tile's columns:
+  // T of ghost-padded column gy = bottom + gy * grad at the step being computed, the ghost
+  // columns' own linear T in the phase-field half step after the first step and their boundary
+  // copy otherwise (Temperature_gradient.h:19, microsim_gp.c:77-82, 108-113); Beff, B(T), C(T) in
+  // FP64 in the reference's order (functionF_01.h:62-104), stored as FP32.  Read after the
+  // barriers below.
+  float* const ttab = I.gm ? sm + T::o_temp : nullptr;
+  if (ttab) {
+    const gp_model& g = *I.gm;
+    const gp_temp_step ts = gp_temp_after(g, __ldcg(I.tstep));
+    for (int e = threadIdx.x; e < 2 * Y1 * N; e += nt) {
+      const int v = e / (Y1 * N), j = (e / N) % Y1, a = e % N, y = y0 - 1 + j;
+      const bool linear = v == 0 && ts.linear;
+      const int yy = (linear || !g.bc_T[3] || (y >= 0 && y < my)) ? y : gp_map(y, my, g.bc_T[3]);
+      Th th;
+      th.on = 1;
+      th.T = ts.bottom + (double)(yy + 3) * ts.grad;
+      float* r = ttab + (v * Y1 + j) * T::RT;
+#pragma unroll
+      for (int k = 0; k < K1; k++) {
+        r[a * K1 + k] = (float)beff(g, th, a, k);
+        r[N * K1 + a * K1 + k] = (float)B_Tn<N, K1>(g, th, k, a);
+      }
+      r[2 * N * K1 + a] = (float)C_Tn<N, K1>(g, th, a);
+    }
+  }
+  // the table row of region-1 column j: v = 0 phase-field half step, 1 concentration half step
+  auto trow = [&](int v, int j) -> const float* { return ttab ? ttab + (v * Y1 + j) * T::RT : nullptr; };
   int* s_list = reinterpret_cast<int*>(sm + T::o_list);
   int* s_act = reinterpret_cast<int*>(sm + T::o_act);
   float* sbx = sm + T::o_bx;
@@ -802,18 +852,19 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
 #pragma unroll
     for (int k = 0; k < K1; k++) mu[k] = MU(k, i1, j1);
     float psi[N];
+    const float* tp = trow(0, j1);
 #pragma unroll
     for (int b = 0; b < N; b++) {
       float c[K1], sv = 0.f;
 #pragma unroll
-      for (int k = 0; k < K1; k++) c[k] = c_mu<K1>(m, mu, b, k);
+      for (int k = 0; k < K1; k++) c[k] = c_mu_t<K1>(m, mu, b, k, tp);
 #pragma unroll
       for (int k = 0; k < K1; k++) {
 #pragma unroll
         for (int l = k; l < K1; l++) sv += m.A[b][k][l] * c[k] * c[l];
-        sv += (m.B[b][k] - mu[k]) * c[k];
+        sv += ((tp ? tp[N * K1 + b * K1 + k] : m.B[b][k]) - mu[k]) * c[k];
       }
-      psi[b] = sv + m.C[b];
+      psi[b] = sv + (tp ? tp[2 * N * K1 + b] : m.C[b]);
     }
     float lambda[N], dp[N], sum_l = 0.f;
     int active = 0;
@@ -940,6 +991,8 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
       any |= (gn[a] != 0.f) | (tc[a] != 0.f) | (tn[a] != 0.f);
     }
     if (!any) return;
+    const float* trc = trow(1, jc);  // the two cells' temperatures (concentration half step)
+    const float* trn = trow(1, jn);
     const float tl = 0.5f * (tc[L] + tn[L]);
     const float norm_l = sqrtf(tl * tl + gn[L] * gn[L]);
 #pragma unroll
@@ -960,8 +1013,8 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
       const float pref = fabsf(sp) * (m.obstacle ? 0.5f : m.s_well) * gn[a] * rn;
 #pragma unroll
       for (int k = 0; k < K1; k++) {
-        const float dcn = c_mu<K1>(m, mun, L, k) - c_mu<K1>(m, mun, a, k);
-        const float dcc = c_mu<K1>(m, muc, L, k) - c_mu<K1>(m, muc, a, k);
+        const float dcn = c_mu_t<K1>(m, mun, L, k, trn) - c_mu_t<K1>(m, mun, a, k, trn);
+        const float dcc = c_mu_t<K1>(m, muc, L, k, trc) - c_mu_t<K1>(m, muc, a, k, trc);
         const float jt = m.atf[a][k] * pref * (sn * dcn * dpn + sc * dcc * dpc);
         out[k] = __fsub_rn(out[k], __fmul_rn(xface ? m.jsx : m.jsy, jt));
       }
@@ -1044,6 +1097,7 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
         }
       } else {
         float hh[N], dce[K1];
+        const float* tu = trow(1, j1);
 #pragma unroll
         for (int k = 0; k < K1; k++) dce[k] = 0.f;
 #pragma unroll
@@ -1058,11 +1112,11 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS 
           for (int k = 0; k < K1; k++) {
             if (m.comp) {  // compensated: the product and the difference error-free, errors kept in dce
               float ep, es;
-              const float pr = two_prod(c_mu<K1>(m, mu, a, k), sdh, ep);
+              const float pr = two_prod(c_mu_t<K1>(m, mu, a, k, tu), sdh, ep);
               dc[k] = two_sum(dc[k], -pr, es);
               dce[k] = __fadd_rn(dce[k], __fsub_rn(es, ep));
             } else {
-              dc[k] -= c_mu<K1>(m, mu, a, k) * sdh;
+              dc[k] -= c_mu_t<K1>(m, mu, a, k, tu) * sdh;
             }
           }
         }
@@ -1565,7 +1619,16 @@ __global__ void __launch_bounds__(32 * GP_LEAN_WARPS)
 }
 
 // ---------------------------------------------------------------- two steps per staged box (depth 2)
-//
+
+// Floats per staged row of the two-step lean kernel's box and intermediate rows: the W = TY + 8
+// columns it computes, padded for 16x32 tiles to 44 (eleven 16-byte quads).  There a warp's
+// sweep puts three row segments of six rows side by side in its lanes (ten float4 column groups
+// each); with 40-float rows the segments' quads overlap inside an 8-lane phase of a float4
+// access (bank-conflict replays), with 44 the segments' quads are offset by 2 (11 x 6 = 66 = 2
+// mod 8) and each phase touches eight distinct quads.  The TMA box loads the padding columns
+// too (unused).
+__host__ __device__ constexpr int lean2_stride(int tx, int ty) { return (tx == 16 && ty == 32) ? ty + 12 : ty + 8; }
+
 // A cell's update is the pure-phase one (pure_update: diffusion of mu in phase
 // b, phi kept) when phi is the one-hot field of b on the cell's 3x3
 // neighbourhood, and then its phi stays one-hot: the pure region shrinks by at
@@ -1588,15 +1651,16 @@ struct Lean2 {
   static constexpr int R2 = TX + 4;                        // box rows x0-2 .. x0+TX+1
   static constexpr int R1 = TX + 2;                        // intermediate rows x0-1 .. x0+TX
   static constexpr int W = TY + 8;                         // columns y0-4 .. y0+TY+3
+  static constexpr int WS = lean2_stride(TX, TY);          // floats per staged row (box and intermediate)
   static constexpr int Q1 = W / 4;                         // column groups of sub-step 1
   static constexpr int Q2 = TY / 4;                        // column groups of sub-step 2 (the tile)
   static constexpr int S1 = 32 / Q1 > 0 ? 32 / Q1 : 1;     // row segments of sub-step 1
   static constexpr int RS1 = (R1 + S1 - 1) / S1;           // rows per segment
   static constexpr int S2 = 32 / Q2;
   static constexpr int RS2 = (TX + S2 - 1) / S2;
-  static constexpr int BYTES = K1 * R2 * W * 4;            // one box
+  static constexpr int BYTES = K1 * R2 * WS * 4;           // one box
   static constexpr int SLOT = (BYTES + 127) / 128 * 128;
-  static constexpr int MID = (K1 * R1 * W * 4 + 127) / 128 * 128;
+  static constexpr int MID = (K1 * R1 * WS * 4 + 127) / 128 * 128;
   static constexpr int STAGES = 2;
   static constexpr int WARPS = 4;
   static constexpr int CTRL = 128;                         // barriers, ring entries
@@ -1615,7 +1679,7 @@ struct Lean2 {
 // Every lane runs RS rows (the shuffles need the whole warp); rows at or past
 // r1 are computed from clamped rows and not stored.  put(r, mnew) stores a
 // row's four new cells.
-template <int K1, int R, int W, int RS, bool COMP, typename Put>
+template <int K1, int R, int W, int WS, int RS, bool COMP, typename Put>
 __device__ __forceinline__ void lean_sweep(const float* __restrict__ src, int c0, int r0, int r1, bool ld_left,
                                            bool ld_right, const float (&gx)[MK][MK], const float (&gy)[MK][MK],
                                            Put put) {
@@ -1624,7 +1688,7 @@ __device__ __forceinline__ void lean_sweep(const float* __restrict__ src, int c0
     r = r < R - 1 ? r : R - 1;
 #pragma unroll
     for (int k = 0; k < K1; k++) {
-      const float4 q = *reinterpret_cast<const float4*>(src + (k * R + r) * W + c0);
+      const float4 q = *reinterpret_cast<const float4*>(src + (k * R + r) * WS + c0);
       v[0][k] = q.x;
       v[1][k] = q.y;
       v[2][k] = q.z;
@@ -1650,8 +1714,8 @@ __device__ __forceinline__ void lean_sweep(const float* __restrict__ src, int c0
 #pragma unroll
     for (int k = 0; k < K1; k++) {
       float left = __shfl_up_sync(0xffffffffu, cur[3][k], 1), right = __shfl_down_sync(0xffffffffu, cur[0][k], 1);
-      if (ld_left) left = src[(k * R + rr) * W + cl];
-      if (ld_right) right = src[(k * R + rr) * W + cr];
+      if (ld_left) left = src[(k * R + rr) * WS + cl];
+      if (ld_right) right = src[(k * R + rr) * WS + cr];
       dy[0][k] = __fsub_rn(cur[0][k], left);
 #pragma unroll
       for (int j = 1; j < 4; j++) dy[j][k] = __fsub_rn(cur[j][k], cur[j - 1][k]);
@@ -1675,12 +1739,12 @@ __device__ __forceinline__ void lean_sweep(const float* __restrict__ src, int c0
 }
 
 // Cells of a staged mu array (rows gx0 .. gx0+R-1, columns gy0 .. gy0+W-1 of
-// instance I, K1 planes) on the grid's first ghost row or column (-1, M) get
+// instance I, K1 planes, WS floats per stored row) on the grid's first ghost row or column (-1, M) get
 // their boundary-map source: from the array when the source lies in it, else
 // from `gmu` (the state the array holds; the periodic partner of a row or
 // column the array crosses).  Ghost rows over the grid's columns first, then
 // ghost columns over the grid's rows.  Called by the whole warp.
-template <int K1, int R, int W>
+template <int K1, int R, int W, int WS>
 __device__ __forceinline__ void lean2_ghosts(const Inst& I, int gx0, int gy0, float* buf, const float* gmu,
                                              int lane) {
   const int mx = I.mx, my = I.my;
@@ -1694,8 +1758,8 @@ __device__ __forceinline__ void lean2_ghosts(const Inst& I, int gx0, int gy0, fl
     for (int gy = ylo + lane; gy < yhi; gy += 32)
 #pragma unroll
       for (int k = 0; k < K1; k++)
-        buf[(k * R + dr) * W + (gy - gy0)] =
-            in_buf ? buf[(k * R + sr) * W + (gy - gy0)] : gmu[k * I.plane + (int64_t)src * I.pitch + gy];
+        buf[(k * R + dr) * WS + (gy - gy0)] =
+            in_buf ? buf[(k * R + sr) * WS + (gy - gy0)] : gmu[k * I.plane + (int64_t)src * I.pitch + gy];
   }
   __syncwarp();
   for (int side = 0; side < 2; side++) {
@@ -1707,8 +1771,8 @@ __device__ __forceinline__ void lean2_ghosts(const Inst& I, int gx0, int gy0, fl
     for (int gx = xlo + lane; gx < xhi; gx += 32)
 #pragma unroll
       for (int k = 0; k < K1; k++)
-        buf[(k * R + (gx - gx0)) * W + dc] =
-            in_buf ? buf[(k * R + (gx - gx0)) * W + sc] : gmu[k * I.plane + (int64_t)gx * I.pitch + src];
+        buf[(k * R + (gx - gx0)) * WS + dc] =
+            in_buf ? buf[(k * R + (gx - gx0)) * WS + sc] : gmu[k * I.plane + (int64_t)gx * I.pitch + src];
   }
   __syncwarp();
 }
@@ -1728,6 +1792,10 @@ __device__ __forceinline__ bool next_to_full(const uint8_t* __restrict__ gen, ui
   f |= xp && yp && gen[t + ny + 1];
   return f;
 }
+
+// The frozen temperature gradient's clock, one step on: launched after every full-kernel pass of
+// a non-isothermal batch (that pass read the step it computed at its tiles' start).
+__global__ void k_tick(long long* t) { *t += 1; }
 
 // The lean tiles of a blocked pair that border a tile of the full kernel's list,
 // as entries {tile, inst * 8 + phase, x0, y0} (count in cnt[4]).
@@ -1767,7 +1835,7 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
             const uint8_t* __restrict__ gen, int total, int reverse, const int4* __restrict__ alist,
             const int* __restrict__ acnt, int* __restrict__ err) {
   using S = Lean2<N, K1, TX, TY>;
-  constexpr int R1 = S::R1, R2 = S::R2, W = S::W, STAGES = S::STAGES, Q1 = S::Q1, Q2 = S::Q2;
+  constexpr int R1 = S::R1, R2 = S::R2, W = S::W, WS = S::WS, STAGES = S::STAGES, Q1 = S::Q1, Q2 = S::Q2;
   extern __shared__ __align__(16) unsigned char lsm_raw[];
   unsigned char* lsm = lsm_raw + ((128 - (smem_u32(lsm_raw) & 127)) & 127);
   const int lane = threadIdx.x & 31;
@@ -1829,11 +1897,14 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
     }
   };
   // lane layouts of the two sub-steps (lanes outside every segment run a dummy sweep: no stores)
-  const int g1 = lane % Q1, seg1 = lane / Q1, g2 = lane % Q2, seg2 = lane / Q2;
+  const int seg1 = lane / Q1, g2 = lane % Q2, seg2 = lane / Q2;
   const bool live1 = seg1 < S::S1, live2 = seg2 < S::S2;
-  const int a1 = live1 ? seg1 * S::RS1 : 0, e1 = live1 ? min(R1, a1 + S::RS1) : 0;
+  // a dead lane of sub-step 1 reads what the live lane two below it reads (the same 8-lane phase
+  // for 16x32 tiles: no extra shared-memory wavefront) and stores nothing (e1 = 0)
+  const int l1 = live1 ? lane : (lane >= 2 ? lane - 2 : 0);
+  const int a1 = (l1 / Q1) * S::RS1, e1 = live1 ? min(R1, a1 + S::RS1) : 0;
   const int a2 = live2 ? seg2 * S::RS2 : 0, e2 = live2 ? min(TX, a2 + S::RS2) : 0;
-  const int c1 = live1 ? 4 * g1 : 0;
+  const int c1 = 4 * (l1 % Q1);
   for (int s = 0; s < STAGES - 1; s++) fill(s);
   __syncwarp();
   uint32_t phase = 0;
@@ -1860,7 +1931,7 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
     const int ex = min(TX, mx - x0), ey = min(TY, my - y0);
     // the box's cells on the grid's first ghost row/column: boundary map of step t
     if (x0 - 2 < 0 || x0 + TX + 2 > mx || y0 - 4 < 0 || y0 + TY + 4 > my)
-      lean2_ghosts<K1, R2, W>(I, x0 - 2, y0 - 4, box, I.mu, lane);
+      lean2_ghosts<K1, R2, W, WS>(I, x0 - 2, y0 - 4, box, I.mu, lane);
     float gx[MK][MK], gy[MK][MK];
 #pragma unroll
     for (int k = 0; k < K1; k++)
@@ -1870,15 +1941,15 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
         gy[k][l] = C.gy[k][l];
       }
     // sub-step 1: rows x0-1 .. x0+TX of step t+1 into mid
-    lean_sweep<K1, R2, W, S::RS1, COMP>(box, c1, a1, e1, false, false, gx, gy, [&](int r, const float (&v)[4][K1]) {
+    lean_sweep<K1, R2, W, WS, S::RS1, COMP>(box, c1, a1, e1, false, false, gx, gy, [&](int r, const float (&v)[4][K1]) {
 #pragma unroll
       for (int k = 0; k < K1; k++)
-        *reinterpret_cast<float4*>(mid + (k * R1 + r) * W + c1) = make_float4(v[0][k], v[1][k], v[2][k], v[3][k]);
+        *reinterpret_cast<float4*>(mid + (k * R1 + r) * WS + c1) = make_float4(v[0][k], v[1][k], v[2][k], v[3][k]);
     });
     __syncwarp();
     // step t+1 ghosts of a tile at the grid edge (Neumann: sources inside mid)
     if (x0 == 0 || x0 + ex == mx || y0 == 0 || y0 + ey == my)
-      lean2_ghosts<K1, R1, W>(I, x0 - 1, y0 - 4, mid, nullptr, lane);
+      lean2_ghosts<K1, R1, W, WS>(I, x0 - 1, y0 - 4, mid, nullptr, lane);
     if (adjm) {  // the tile at step t+1 into X for the full kernel's second pass
       const Inst& X = insts_x[inst];
       for (int e3 = lane; e3 < ex * Q2; e3 += 32) {
@@ -1887,7 +1958,7 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
         const int64_t o = (int64_t)(x0 + r) * X.pitch + yb;
 #pragma unroll
         for (int k = 0; k < K1; k++) {
-          const float* v = mid + (k * R1 + r + 1) * W + 4 + 4 * g;
+          const float* v = mid + (k * R1 + r + 1) * WS + 4 + 4 * g;
           if (yb + 3 < my) {
             *reinterpret_cast<float4*>(X.mu_out + o + k * X.plane) = *reinterpret_cast<const float4*>(v);
           } else {
@@ -1910,7 +1981,7 @@ __global__ void __launch_bounds__(32 * Lean2<N, K1, TX, TY>::WARPS)
       const int yb = y0 + 4 * g2;
       const bool full = x0 + TX <= mx && y0 + TY <= my;
       float* const out = I.mu_out + (int64_t)x0 * I.pitch + yb;
-      lean_sweep<K1, R1, W, S::RS2, COMP>(
+      lean_sweep<K1, R1, W, WS, S::RS2, COMP>(
           mid, 4 + 4 * g2, a2, e2, g2 == 0, g2 == Q2 - 1, gx, gy, [&](int r, const float (&v)[4][K1]) {
             if (full) {
 #pragma unroll
@@ -2067,6 +2138,7 @@ struct KernelSet {
                 uint32_t*, uint32_t*, const uint8_t*, int, int, const int4*, const int*, int*);
   void (*list)(const int4*, const uint32_t*, int, int2*, int*, uint8_t*, int);
   size_t smem_general, smem_lean, smem_lean2;
+  size_t smem_temp;  // the full kernel's temperature table (non-isothermal batches add it to smem_general)
   // the lean kernels with compensated accumulation (a template switch: the plain ones keep
   // their registers)
   decltype(lean) lean_c;
@@ -2085,6 +2157,7 @@ static KernelSet make_set() {
   k.lean2_c = k_lean2<N, K1, TX, TY, true>;
   k.list = k_general_list<TX, TY>;
   k.smem_general = Tile<N, K1, AN, TX, TY>::bytes;
+  k.smem_temp = Tile<N, K1, AN, TX, TY>::bytes_temp;
   k.smem_lean = Lean<N, K1, TX, TY>::smem;
   k.smem_lean2 = Lean2<N, K1, TX, TY>::smem;
   return k;
@@ -2109,7 +2182,6 @@ static bool pick(int N, int K1, int an, int tx, int ty, KernelSet* k) {
 }
 
 int gp_f32_supported(const gp_model& m) {
-  if (m.nonisothermal) return 0;  // the FP32 kernels take the model's single temperature
   KernelSet k;
   return pick(m.N, m.K1, m.anisotropy, 16, 32, &k);
 }
@@ -2147,6 +2219,9 @@ struct gp_f32_batch {
   std::vector<Inst> hinst[2];  // [buffer parity]
   Inst* dinst[2] = {nullptr, nullptr};
   Model* dmodel = nullptr;
+  int noniso = 0;                 // some instance has the frozen temperature gradient
+  gp_model* dgm = nullptr;        // [n] the instances' FP64 models (non-isothermal batches)
+  long long* dtstep = nullptr;    // the step the next full-kernel pass computes
   LeanConst* dlconst = nullptr;                 // [n][N] lean-update constants of each phase
   CUtensorMap* dtmap[2] = {nullptr, nullptr};  // [parity][n] mu boxes of the lean kernel
   int* derr = nullptr;                          // lean kernel: a staged box did not arrive
@@ -2229,6 +2304,13 @@ cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** ou
   if (e == cudaSuccess) e = cudaMemset(b->derr, 0, 2 * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&b->dcnt, 8 * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(b->dcnt, 0, 8 * sizeof(int));
+  for (int i = 0; i < n; i++) b->noniso |= models[i].nonisothermal ? 1 : 0;
+  if (e == cudaSuccess && b->noniso) {
+    e = cudaMalloc(&b->dgm, sizeof(gp_model) * n);
+    if (e == cudaSuccess) e = cudaMemcpy(b->dgm, models, sizeof(gp_model) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&b->dtstep, sizeof(long long));
+    if (e == cudaSuccess) e = cudaMemset(b->dtstep, 0, sizeof(long long));
+  }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
@@ -2265,6 +2347,8 @@ void gp_f32_batch_destroy(gp_f32_batch* b) {
     cudaFree(b->dtmap2[p]);
   }
   cudaFree(b->dlconst);
+  cudaFree(b->dgm);
+  cudaFree(b->dtstep);
   cudaFree(b->derr);
   free_tiles(b);
   cudaFree(b->dcnt);
@@ -2296,6 +2380,8 @@ void gp_f32_batch_bind(gp_f32_batch* b, int i, float* phiA, float* muA, float* p
     I.my = (int)b->gm[i].mesh_y;
     I.model = i;
     I.bc = gp_bc_of(b->gm[i]);
+    I.gm = b->gm[i].nonisothermal ? b->dgm + i : nullptr;
+    I.tstep = b->dtstep;
   }
 }
 
@@ -2354,7 +2440,8 @@ static cudaError_t encode_boxes(gp_f32_batch* b, int p, int halo = 1) {
     const Inst& I = b->hinst[p][i];
     const cuuint64_t dim[3] = {(cuuint64_t)I.my, (cuuint64_t)I.mx, (cuuint64_t)b->K1};
     const cuuint64_t stride[2] = {(cuuint64_t)I.pitch * 4, (cuuint64_t)I.plane * 4};
-    const cuuint32_t box[3] = {(cuuint32_t)b->ty + 8, (cuuint32_t)b->tx + 2 * halo, (cuuint32_t)b->K1};
+    const cuuint32_t box[3] = {(cuuint32_t)(halo == 2 ? lean2_stride(b->tx, b->ty) : b->ty + 8),
+                               (cuuint32_t)b->tx + 2 * halo, (cuuint32_t)b->K1};
     const cuuint32_t estride[3] = {1, 1, 1};
     if (enc(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)I.mu, dim, stride, box, estride,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -2441,6 +2528,7 @@ cudaError_t gp_f32_batch_set_tiles(gp_f32_batch* b, int tx, int ty) {
   if (!pick(b->N, b->K1, b->aniso, tx, ty, &ks)) return cudaErrorInvalidValue;
   b->tx = tx;
   b->ty = ty;
+  if (b->noniso) ks.smem_general += ks.smem_temp;
   b->ks = ks;
   int t = 0;
   std::vector<int> tile_inst;
@@ -2622,6 +2710,10 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
     (b->step_threads == 512 ? k.general_wide : k.general)<<<b->total_tiles, b->step_threads, k.smem_general, s>>>(
         b->dinst[p], b->dmodel, b->dtile_inst, nullptr, nullptr, flags_out, b->total_tiles, nullptr, nullptr, 0);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (b->noniso) {
+      k_tick<<<1, 1, 0, s>>>(b->dtstep);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     if (E) {
       if ((e = cudaEventRecord(E[5], s)) != cudaSuccess) return e;
       if ((e = cudaEventRecord(E[1], s)) != cudaSuccess) return e;
@@ -2655,6 +2747,10 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
       b->dinst[p], b->dmodel, b->dtile_inst, b->scan ? nullptr : b->dglist, b->scan ? nullptr : b->dcnt, flags_out,
       b->total_tiles, b->scan ? b->dtile_desc : nullptr, b->scan ? flags_in : nullptr, 0);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (b->noniso) {
+    k_tick<<<1, 1, 0, s>>>(b->dtstep);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   if (E) return cudaEventRecord(E[5], s);
   if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess) return e;
   return cudaStreamWaitEvent(s, b->ev_join, 0);
@@ -2708,10 +2804,18 @@ cudaError_t gp_f32_batch_launch_pair(gp_f32_batch* b, int parity, cudaStream_t s
   full<<<b->grid_general, b->step_threads, k.smem_general, s>>>(b->dinst_x1[p], b->dmodel, b->dtile_inst, b->dglist,
                                                                  b->dcnt, flags_x, b->total_tiles, nullptr, nullptr, 1);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (b->noniso) {
+    k_tick<<<1, 1, 0, s>>>(b->dtstep);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   if (!E && (e = cudaStreamWaitEvent(s, b->ev_adj, 0)) != cudaSuccess) return e;
   full<<<b->grid_general, b->step_threads, k.smem_general, s>>>(b->dinst_x2[p], b->dmodel, b->dtile_inst, b->dglist,
                                                                  b->dcnt, flags_out, b->total_tiles, nullptr, nullptr, 0);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (b->noniso) {
+    k_tick<<<1, 1, 0, s>>>(b->dtstep);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   if (E) return cudaEventRecord(E[5], s);
   if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess) return e;
   return cudaStreamWaitEvent(s, b->ev_join, 0);
@@ -2753,6 +2857,18 @@ void gp_f32_batch_test_lose_box(gp_f32_batch* b) { b->lose_box = 1; }
 const int* gp_f32_batch_error_word(const gp_f32_batch* b) { return b->derr; }
 
 // kernel launches one gp_f32_batch_launch issues
-int gp_f32_batch_launches_per_step(const gp_f32_batch* b) { return b->narrowband ? (b->scan ? 2 : 3) : 1; }
+int gp_f32_batch_launches_per_step(const gp_f32_batch* b) {
+  return (b->narrowband ? (b->scan ? 2 : 3) : 1) + (b->noniso ? 1 : 0);
+}
 // kernel launches one gp_f32_batch_launch_pair issues (two steps)
-int gp_f32_batch_launches_per_pair(const gp_f32_batch*) { return 6; }
+int gp_f32_batch_launches_per_pair(const gp_f32_batch* b) { return 6 + (b->noniso ? 2 : 0); }
+
+// The step count of the frozen temperature gradient (non-isothermal batches): the step the next
+// full-kernel pass computes.  Stream-ordered on s.
+cudaError_t gp_f32_batch_set_tstep(gp_f32_batch* b, long long t, cudaStream_t s) {
+  if (!b->dtstep) return cudaSuccess;
+  static thread_local long long v;
+  v = t;
+  cudaError_t e = cudaMemcpyAsync(b->dtstep, &v, sizeof v, cudaMemcpyHostToDevice, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}

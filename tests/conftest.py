@@ -31,8 +31,8 @@ def golden_cases():
 
 
 def isothermal_cases():
-    """Short cases with one temperature throughout (the oracle restatement and the FP32 form take
-    only these; the frozen-gradient cases pin the FP64 plain form to the reference directly)."""
+    """Short cases with one temperature throughout (the oracle restatement takes only these; the
+    frozen-gradient cases pin the GPU forms to the reference directly)."""
     return [c for c in golden_cases() if not int(load_golden(c).get("nonisothermal", 0))]
 
 

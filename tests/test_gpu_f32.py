@@ -18,7 +18,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import golden_cases, interior, isothermal_cases, load_golden, presmooth, write_inputs
+from conftest import golden_cases, interior, load_golden, presmooth, write_inputs
 import microsim_b200 as mb
 from microsim_b200 import configs
 
@@ -62,7 +62,7 @@ def test_four_phase_ternary_within_tolerance():
     np.testing.assert_allclose(s32["solute"], s64["solute"], rtol=1e-4)
 
 
-@pytest.mark.parametrize("case", [c for c in isothermal_cases()
+@pytest.mark.parametrize("case", [c for c in golden_cases()
                                   if c != "c1_literal_small" and "shifts" not in load_golden(c)])
 def test_golden_cases_within_tolerance_of_reference(case):
     g = load_golden(case)
@@ -297,6 +297,65 @@ def test_two_step_blocking_is_bit_identical_to_single_steps():
             b.step(120)
             res.append(b.download(0))
     assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+def _golden_model(name):
+    g = load_golden(name)
+    with tempfile.TemporaryDirectory() as d:
+        ip, fp = write_inputs(g, d)
+        inp = mb.Input(ip, fp)
+        m = inp.model()
+        phi, mu = inp.fill(m)
+    return g, m, phi, mu
+
+
+def test_nonisothermal_batch_equals_contexts_and_resumes():
+    """The frozen temperature gradient in the FP32 batch: two instances with their own gradients
+    (one moving), single steps and blocked pairs, equal FP32 contexts bit for bit; the
+    statistics see each instance's temperature; a batch resumed at step 20 with
+    set_time_step(20) continues the run bit for bit; and it stays within the FP32 tolerance
+    of the FP64 form."""
+    g, m, phi, mu = _golden_model("tempgrad_aniso_bin")
+    m2 = m.copy()
+    m2.tg_velocity = 0.0  # a second instance with a frozen (not moving) gradient
+    m2.tg_offset = m.tg_offset + 3.0
+    models, steps = [m, m2], 41
+    ref = []
+    for mm in models:
+        with mb.Context(mm, mb.GP_FP32) as c:
+            c.upload(phi, mu)
+            c.step(steps)
+            ref.append((*c.download(), c.stats()))
+    for depth in (1, 2):
+        with mb.Batch(models) as b:
+            b.set_depth(depth)
+            for i in range(2):
+                b.upload(i, phi, mu)
+            b.step(steps)
+            for i in range(2):
+                p, u = b.download(i)
+                assert np.array_equal(p, ref[i][0]) and np.array_equal(u, ref[i][1]), (depth, i)
+                np.testing.assert_allclose(b.stats(i)["solute"], ref[i][2]["solute"], rtol=1e-12)
+    assert not np.array_equal(ref[0][1], ref[1][1])  # the two gradients differ
+    with mb.Batch(models) as b:
+        for i in range(2):
+            b.upload(i, phi, mu)
+        b.step(20)
+        mid = [b.download(i) for i in range(2)]
+    with mb.Batch(models) as b:
+        for i in range(2):
+            b.upload(i, *mid[i])
+        b.set_time_step(20)
+        b.step(steps - 20)
+        for i in range(2):
+            p, u = b.download(i)
+            assert np.array_equal(p, ref[i][0]) and np.array_equal(u, ref[i][1]), i
+    with mb.Context(m, mb.GP_FP64) as c64:
+        c64.upload(phi, mu)
+        c64.step(steps)
+        p64, u64 = c64.download()
+    assert np.abs(ref[0][0] - p64).max() <= 1e-4
+    assert np.abs(ref[0][1] - u64).max() <= 1e-3
 
 
 def test_compensated_accumulation():
