@@ -29,13 +29,16 @@ sum over ranks of the cells (microsim_b200/ranks.py).
 The reference arm (--impl reference) times the reference serial solver,
 compiled from its own sources (oracle/_ref/gp_ref_harness), on the host's
 cores: one process per core, each on one instance of the workload (distinct
-instances for the batched sweep) for a bounded number of steps.
+instances for the batched sweep) for a bounded number of steps, starting from
+the same advanced state as the GPU arm (handed over as the reference's own
+restart files; the CPU baseline of the GPU arm does the same).
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -142,20 +145,34 @@ def barrier(world: int):
 
 # --------------------------------------------------------------------------------------------- reference arm
 
-def reference_rate(cases, steps: int, procs: int, timeout: float = 900.0):
+def reference_rate(cases, steps: int, procs: int, timeout: float = 900.0, start=None):
     """Run the reference (compiled from source) on `procs` host cores, `steps` steps each.
-    Returns (cell-updates/s aggregate, sample description)."""
+    With start = (t, fields): every process starts from its instance's state after t steps
+    (fields[i] = (phi, mu)), handed to the reference as its own restart file (DATA/out_<t>.vtk in
+    the input's WRITEFORMAT, read by its RESTART path), so it times the same workload state as
+    the GPU arm.  Returns (cell-updates/s aggregate, sample description)."""
     from oracle import gp_oracle as O
     if not os.path.exists(O.HARNESS_PATH):
         return None, "oracle/_ref/gp_ref_harness missing"
     # one instance per process: the workload's instances in turn (a single-instance workload repeats it)
-    chosen = [cases[i % len(cases)] for i in range(procs)]
+    idx = [i % len(cases) for i in range(procs)]
+    chosen = [cases[i] for i in idx]
     with tempfile.TemporaryDirectory() as td:
         ps = []
         for i, case in enumerate(chosen):
             wd = os.path.join(td, f"w{i}")
             os.makedirs(wd)
-            case.write(wd)
+            ip, fp = case.write(wd)
+            if start is not None:
+                import microsim_b200 as mb
+                t0, fields = start
+                text = open(ip).read()
+                text = re.sub(r"(?m)^STARTTIME\s*=\s*\d+;", f"STARTTIME = {t0};", text)
+                text = re.sub(r"(?m)^RESTART\s*=\s*\d+;", "RESTART = 1;", text)
+                open(ip, "w").write(text)
+                os.makedirs(os.path.join(wd, "DATA"), exist_ok=True)
+                inp = mb.Input(ip, fp)
+                inp.write_vtk(inp.model(), os.path.join(wd, "DATA", f"out_{t0}.vtk"), *fields[idx[i]], t0)
             ps.append(subprocess.Popen([O.HARNESS_PATH, "Input.in", "Filling.in", "out", "-", str(steps)], cwd=wd,
                                        stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
         secs = []
@@ -168,8 +185,10 @@ def reference_rate(cases, steps: int, procs: int, timeout: float = 900.0):
         return None, "reference harness failed"
     rate = sum(c.cells for c in chosen) * steps / max(secs)
     sides = sorted({f"{c.mesh_x}x{c.mesh_y}" for c in chosen})
+    state = (f"from the state after {start[0]} steps (the GPU arm's, as the reference's restart file)"
+             if start is not None else "from the initial filling")
     return rate, (f"{procs} processes (one per core), one instance each ({', '.join(sides)}), "
-                  f"{steps} steps per process; rate = cells x steps / slowest process")
+                  f"{steps} steps per process {state}; rate = cells x steps / slowest process")
 
 
 def run_reference_arm(args, world, rank):
@@ -179,10 +198,21 @@ def run_reference_arm(args, world, rank):
     procs = max(1, min(os.cpu_count() or 1, 64))
     steps = max(1, args.ref_steps)
     t0 = time.time()
+    # input preparation, outside every timed region: the workload state the GPU arm times (its
+    # instances advanced by the FP32 form), handed to the reference as its own restart files; the
+    # timed runs are the reference alone
+    start = None
+    prep = args.prep_steps if args.prep_steps >= 0 else {"c2": 25000, "c1": 5000, "c4": 2500}[args.workload]
+    try:
+        import microsim_b200 as mb
+        loaded = [mb.load_case(c) for c in cases[:procs]]
+        start = (prep, prepare([m for m, _, _ in loaded], [(p, u) for _, p, u in loaded], prep))
+    except Exception:  # no GPU or library: the reference starts from the initial filling (said in `sample`)
+        start = None
     rates = []
     sample = ""
     for _ in range(args.steps):
-        r, sample = reference_rate(cases, steps, procs)
+        r, sample = reference_rate(cases, steps, procs, start=start)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": sample}))
             return
@@ -468,7 +498,7 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         procs = max(1, min(os.cpu_count() or 1, 64))
-        r, sample = reference_rate(cases, args.ref_steps, procs)
+        r, sample = reference_rate(cases, args.ref_steps, procs, start=(prep, fields))
         if r is not None:
             cpu = {"value": r, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample}
     ctx.close()
