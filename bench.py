@@ -482,12 +482,12 @@ def run_ours(args, world, rank, local):
     with torch.cuda.stream(stream):
         e0.record(stream)
     for i, (p, u) in enumerate(pinned):
-        ctx.upload(i, p, u)
+        ctx.upload(i, p, u, wait=False)  # queued back to back; the first step waits for them on the stream
     for _ in range(args.steps):
         ctx.step(1)
-        ctx.stats(0, allow_nonfinite=True)
+        ctx.stats(0, allow_nonfinite=True)  # the step's result read back to the host
     for i, (p, u) in enumerate(pinned_out):
-        ctx.download(i, p, u)
+        ctx.download(i, p, u, wait=False)
     with torch.cuda.stream(stream):
         e1.record(stream)
     e1.synchronize()

@@ -258,6 +258,13 @@ int gp_batch_create(const gp_model *models, int n, gp_batch **out);
 int gp_batch_destroy(gp_batch *b);
 int gp_batch_upload(gp_batch *b, int i, const double *phi, const double *mu);
 int gp_batch_download(gp_batch *b, int i, double *phi, double *mu);
+/* As gp_batch_upload / gp_batch_download, but queued on the batch's stream
+ * without waiting: the host arrays must stay untouched (and, for a download,
+ * unread) until gp_batch_sync or a call that waits.  Copies of consecutive
+ * instances then run back to back (with page-locked host arrays at the link's
+ * speed) instead of one host round trip per instance. */
+int gp_batch_upload_async(gp_batch *b, int i, const double *phi, const double *mu);
+int gp_batch_download_async(gp_batch *b, int i, double *phi, double *mu);
 int gp_batch_step(gp_batch *b, int64_t nsteps);
 /* Capture the step graphs of both buffer parities now, without stepping (the
  * first gp_batch_step would otherwise capture them). */

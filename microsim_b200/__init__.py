@@ -118,6 +118,8 @@ _SIGS = {
     "gp_batch_destroy": (C.c_int, [C.c_void_p]),
     "gp_batch_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "gp_batch_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "gp_batch_upload_async": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "gp_batch_download_async": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "gp_batch_step": (C.c_int, [C.c_void_p, C.c_int64]),
     "gp_batch_sync": (C.c_int, [C.c_void_p]),
     "gp_batch_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(GpStats)]),
@@ -420,18 +422,31 @@ class Batch:
     def __len__(self):
         return len(self.models)
 
-    def upload(self, i: int, phi: np.ndarray, mu: np.ndarray):
+    def upload(self, i: int, phi: np.ndarray, mu: np.ndarray, wait: bool = True):
+        """Instance i's state from float64 arrays.  wait=False queues the copy on the batch's
+        stream and returns (the arrays must then be C-contiguous float64, ideally page-locked,
+        and stay untouched until sync())."""
+        if not wait:
+            for a in (phi, mu):
+                if a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise ValueError("upload(wait=False) needs C-contiguous float64 arrays")
+            _check("gp_batch_upload_async", lib().gp_batch_upload_async(self._h, i, _ptr(phi), _ptr(mu)))
+            return
         phi = np.ascontiguousarray(phi, dtype=np.float64)  # held: the C call reads them
         mu = np.ascontiguousarray(mu, dtype=np.float64)
         _check("gp_batch_upload", lib().gp_batch_upload(self._h, i, _ptr(phi), _ptr(mu)))
 
-    def download(self, i: int, phi: np.ndarray | None = None, mu: np.ndarray | None = None):
+    def download(self, i: int, phi: np.ndarray | None = None, mu: np.ndarray | None = None, wait: bool = True):
         """Instance i's state as float64 arrays (into phi / mu when given: C-contiguous
-        float64 of the instance's shapes, e.g. views of pinned host memory)."""
+        float64 of the instance's shapes, e.g. views of pinned host memory).  wait=False
+        queues the copy on the batch's stream: the arrays hold the state after sync()."""
         m = self.models[i]
         phi = _out(phi, (m.N, m.mesh_x, m.mesh_y))
         mu = _out(mu, (m.K1, m.mesh_x, m.mesh_y))
-        _check("gp_batch_download", lib().gp_batch_download(self._h, i, _ptr(phi), _ptr(mu)))
+        if not wait:
+            _check("gp_batch_download_async", lib().gp_batch_download_async(self._h, i, _ptr(phi), _ptr(mu)))
+        else:
+            _check("gp_batch_download", lib().gp_batch_download(self._h, i, _ptr(phi), _ptr(mu)))
         return phi, mu
 
     def step(self, nsteps: int = 1):

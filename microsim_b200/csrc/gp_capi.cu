@@ -920,22 +920,38 @@ static int batch_copy(gp_batch* b, int i, const double* host, int nplanes, bool 
   return GP_OK;
 }
 
-extern "C" int gp_batch_upload(gp_batch* b, int i, const double* phi, const double* mu) {
+static int batch_upload(gp_batch* b, int i, const double* phi, const double* mu, bool wait) {
   if (!b || i < 0 || i >= b->n || !phi || !mu) return GP_E_ARG;
   int rc = batch_copy(b, i, phi, b->models[i].N, true, true);
   if (rc == GP_OK) rc = batch_copy(b, i, mu, b->models[i].K1, false, true);
   if (rc == GP_OK) GP_CUDA(gp_f32_batch_invalidate(b->f32, b->stream));
-  if (rc == GP_OK) GP_CUDA(cudaStreamSynchronize(b->stream));
+  if (rc == GP_OK && wait) GP_CUDA(cudaStreamSynchronize(b->stream));
   b->have_prev = 0;
   return rc;
 }
 
-extern "C" int gp_batch_download(gp_batch* b, int i, double* phi, double* mu) {
+static int batch_download(gp_batch* b, int i, double* phi, double* mu, bool wait) {
   if (!b || i < 0 || i >= b->n || !phi || !mu) return GP_E_ARG;
   int rc = batch_copy(b, i, phi, b->models[i].N, true, false);
   if (rc == GP_OK) rc = batch_copy(b, i, mu, b->models[i].K1, false, false);
-  if (rc == GP_OK) GP_CUDA(cudaStreamSynchronize(b->stream));
+  if (rc == GP_OK && wait) GP_CUDA(cudaStreamSynchronize(b->stream));
   return rc;
+}
+
+extern "C" int gp_batch_upload(gp_batch* b, int i, const double* phi, const double* mu) {
+  return batch_upload(b, i, phi, mu, true);
+}
+
+extern "C" int gp_batch_download(gp_batch* b, int i, double* phi, double* mu) {
+  return batch_download(b, i, phi, mu, true);
+}
+
+extern "C" int gp_batch_upload_async(gp_batch* b, int i, const double* phi, const double* mu) {
+  return batch_upload(b, i, phi, mu, false);
+}
+
+extern "C" int gp_batch_download_async(gp_batch* b, int i, double* phi, double* mu) {
+  return batch_download(b, i, phi, mu, false);
 }
 
 // One launch call of the configured depth: a single step, or a blocked pair

@@ -358,6 +358,29 @@ def test_nonisothermal_batch_equals_contexts_and_resumes():
     assert np.abs(ref[0][1] - u64).max() <= 1e-3
 
 
+def test_async_upload_download_equal_the_waiting_ones():
+    """Queued uploads and downloads of every instance (no host wait between instances, one sync)
+    give the state the waiting calls give."""
+    cases = [configs.binary_case(96, 64, gap=1.0, supersat=0.55, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
+                                 seed=(0, 0, 8.0)),
+             configs.binary_case(160, 128, gap=1.0, supersat=0.5, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
+                                 seed=(80, 64, 9.0))]
+    loaded = [mb.load_case(c) for c in cases]
+    models = [m for m, _, _ in loaded]
+    res = []
+    for wait in (True, False):
+        held = [(np.ascontiguousarray(p), np.ascontiguousarray(u)) for _, p, u in loaded]  # alive until sync
+        with mb.Batch(models) as b:
+            for i, (p, u) in enumerate(held):
+                b.upload(i, p, u, wait=wait)
+            b.step(30)
+            outs = [b.download(i, wait=wait) for i in range(len(models))]
+            b.sync()
+            res.append([(p.copy(), u.copy()) for p, u in outs])
+    for (p1, u1), (p0, u0) in zip(res[1], res[0]):
+        assert np.array_equal(p1, p0) and np.array_equal(u1, u0)
+
+
 def test_compensated_accumulation():
     """Compensated (TwoSum/TwoProduct) accumulation: on for a context and a batch,
     refused for FP64; the results change bits, stay within the FP32 tolerances of
