@@ -477,17 +477,20 @@ def run_ours(args, world, rank, local):
         pinned.append((pt.numpy(), ut.numpy()))
     pinned_out = [(torch.empty(p.shape, dtype=torch.float64, pin_memory=True).numpy(),
                    torch.empty(u.shape, dtype=torch.float64, pin_memory=True).numpy()) for p, u in fields]
+    # one untimed round trip through the same page-locked buffers first (warm-up: the first
+    # transfer from freshly page-locked memory runs at about half the link's speed)
+    ctx.upload_all(pinned)
+    ctx.download_all(pinned_out)
+    ctx.sync()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         e0.record(stream)
-    for i, (p, u) in enumerate(pinned):
-        ctx.upload(i, p, u, wait=False)  # queued back to back; the first step waits for them on the stream
+    ctx.upload_all(pinned)  # every instance in one queued conversion launch reading the host arrays
     for _ in range(args.steps):
         ctx.step(1)
         ctx.stats(0, allow_nonfinite=True)  # the step's result read back to the host
-    for i, (p, u) in enumerate(pinned_out):
-        ctx.download(i, p, u, wait=False)
+    ctx.download_all(pinned_out)
     with torch.cuda.stream(stream):
         e1.record(stream)
     e1.synchronize()

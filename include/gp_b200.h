@@ -261,10 +261,18 @@ int gp_batch_download(gp_batch *b, int i, double *phi, double *mu);
 /* As gp_batch_upload / gp_batch_download, but queued on the batch's stream
  * without waiting: the host arrays must stay untouched (and, for a download,
  * unread) until gp_batch_sync or a call that waits.  Copies of consecutive
- * instances then run back to back (with page-locked host arrays at the link's
- * speed) instead of one host round trip per instance. */
+ * instances then run back to back instead of one host round trip per instance.
+ * Page-locked host arrays (cudaHostAlloc, cudaHostRegister, torch pin_memory)
+ * are read or written by the FP64 <-> FP32 conversion kernel itself across the
+ * link, with no staging copy; they must then hold the instance's whole state
+ * (N, resp. K-1, planes of mesh_x * mesh_y doubles). */
 int gp_batch_upload_async(gp_batch *b, int i, const double *phi, const double *mu);
 int gp_batch_download_async(gp_batch *b, int i, double *phi, double *mu);
+/* Every instance at once (phi[i], mu[i] for i < n), queued like the _async
+ * calls: page-locked arrays move in one conversion launch over all instances,
+ * pageable ones through the staging copies.  gp_batch_sync waits. */
+int gp_batch_upload_all(gp_batch *b, const double *const *phi, const double *const *mu);
+int gp_batch_download_all(gp_batch *b, double *const *phi, double *const *mu);
 int gp_batch_step(gp_batch *b, int64_t nsteps);
 /* Capture the step graphs of both buffer parities now, without stepping (the
  * first gp_batch_step would otherwise capture them). */

@@ -120,6 +120,8 @@ _SIGS = {
     "gp_batch_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "gp_batch_upload_async": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "gp_batch_download_async": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "gp_batch_upload_all": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gp_batch_download_all": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "gp_batch_step": (C.c_int, [C.c_void_p, C.c_int64]),
     "gp_batch_sync": (C.c_int, [C.c_void_p]),
     "gp_batch_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(GpStats)]),
@@ -448,6 +450,27 @@ class Batch:
         else:
             _check("gp_batch_download", lib().gp_batch_download(self._h, i, _ptr(phi), _ptr(mu)))
         return phi, mu
+
+    def upload_all(self, fields):
+        """Every instance's state from [(phi, mu), ...], queued (sync() waits): C-contiguous
+        float64 arrays, read in place by one conversion launch when page-locked."""
+        for a in (x for f in fields for x in f):
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("upload_all needs C-contiguous float64 arrays")
+        ptrs = (C.c_void_p * len(fields))
+        _check("gp_batch_upload_all", lib().gp_batch_upload_all(
+            self._h, ptrs(*[f[0].ctypes.data for f in fields]), ptrs(*[f[1].ctypes.data for f in fields])))
+
+    def download_all(self, fields):
+        """Every instance's state into [(phi, mu), ...] (writeable C-contiguous float64 arrays of the
+        instances' shapes), queued: the arrays hold it after sync()."""
+        for i, (p, u) in enumerate(fields):
+            m = self.models[i]
+            _out(p, (m.N, m.mesh_x, m.mesh_y))
+            _out(u, (m.K1, m.mesh_x, m.mesh_y))
+        ptrs = (C.c_void_p * len(fields))
+        _check("gp_batch_download_all", lib().gp_batch_download_all(
+            self._h, ptrs(*[f[0].ctypes.data for f in fields]), ptrs(*[f[1].ctypes.data for f in fields])))
 
     def step(self, nsteps: int = 1):
         _check("gp_batch_step", lib().gp_batch_step(self._h, int(nsteps)))

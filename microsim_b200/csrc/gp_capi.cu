@@ -252,6 +252,32 @@ __global__ void k_unpack(const T* __restrict__ src, double* __restrict__ dst, in
   }
 }
 
+// One field of one batch instance moved in a batch-wide conversion: dense FP64 host planes
+// (device-reachable page-locked memory) <-> the instance's pitched FP32 planes.
+struct CopyJob {
+  double* host;
+  float* dev;
+  int mx, my, pitch, nplanes;
+  int64_t plane;
+};
+
+// Every job of a batch-wide upload (up) or download in one launch: blockIdx.y is the job, the
+// blocks along x stride over its elements (each element read and written once; host memory
+// reached across the link).
+__global__ void __launch_bounds__(256) k_convert_jobs(const CopyJob* __restrict__ jobs, int up) {
+  const CopyJob J = jobs[blockIdx.y];
+  const int64_t cells = (int64_t)J.mx * J.my, n = cells * J.nplanes;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / cells, r = i % cells;
+    const int x = (int)(r / J.my), y = (int)(r % J.my);
+    float* const d = J.dev + p * J.plane + (int64_t)x * J.pitch + y;
+    if (up)
+      *d = (float)J.host[i];
+    else
+      J.host[i] = (double)*d;
+  }
+}
+
 static int copy_planes(gp_ctx* c, const double* host, void* dev, int nplanes, bool up) {
   const int64_t mx = c->m.mesh_x, my = c->m.mesh_y;
   if (c->precision == GP_FP64) {
@@ -719,16 +745,31 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
   }
 }
 
-// Fixed-order final combine of the block partials (deterministic).
-__global__ void k_stats_final(int N, int K1, const double* __restrict__ partials, int nblocks,
-                              double* __restrict__ out, const int* __restrict__ err) {
+// Final combine of the block partials, one block per slot (launched with 64 blocks of
+// kFinalThreads): thread t combines partials t, t + kFinalThreads, ... in that order, then a
+// fixed tree in shared memory -- the same order every call (deterministic) and a few dependent
+// loads per thread instead of one chain over all partials.
+constexpr int kFinalThreads = 128;
+__global__ void __launch_bounds__(kFinalThreads) k_stats_final(int N, int K1, const double* __restrict__ partials,
+                                                               int nblocks, double* __restrict__ out,
+                                                               const int* __restrict__ err) {
   const StatLayout L{N, K1};
-  const int s = threadIdx.x;
-  if (s == 63) out[63] = err ? (double)*err : 0.0;  // the FP32 form's lean-kernel error word
+  const int s = blockIdx.x, t = threadIdx.x;
+  if (s == 63) {
+    if (t == 0) out[63] = err ? (double)*err : 0.0;  // the FP32 form's lean-kernel error word
+    return;
+  }
   if (s >= L.count()) return;
-  double v = partials[s];
-  for (int b = 1; b < nblocks; b++) v = combine(L, s, v, partials[(int64_t)b * 64 + s]);
-  out[s] = v;
+  __shared__ double red[kFinalThreads];
+  double v = ident(L, s);
+  for (int b = t; b < nblocks; b += kFinalThreads) v = combine(L, s, v, partials[(int64_t)b * 64 + s]);
+  red[t] = v;
+  __syncthreads();
+  for (int w = kFinalThreads / 2; w > 0; w >>= 1) {
+    if (t < w) red[t] = combine(L, s, red[t], red[t + w]);
+    __syncthreads();
+  }
+  if (t == 0) out[s] = red[0];
 }
 
 // The energy sums of the reduction vector, integrated (times dx * dy).
@@ -754,7 +795,7 @@ extern "C" int gp_get_stats(gp_ctx* c, gp_stats* out) {
                                                         (const float*)c->phi[prv], (const float*)c->mu[prv],
                                                         c->have_prev, c->pitch, c->plane, c->partials, ts);
   GP_CUDA(cudaGetLastError());
-  k_stats_final<<<1, 64, 0, c->stream>>>(m.N, m.K1, c->partials, c->red_blocks, c->reduced,
+  k_stats_final<<<64, kFinalThreads, 0, c->stream>>>(m.N, m.K1, c->partials, c->red_blocks, c->reduced,
                                          c->f32 ? gp_f32_batch_error_word(c->f32) : nullptr);
   GP_CUDA(cudaGetLastError());
   c->launches += 2;
@@ -811,6 +852,7 @@ struct gp_batch {
   double* reduced = nullptr;
   double* stage = nullptr;  // device staging of FP64 host fields (kept between copies)
   size_t stage_bytes = 0;
+  CopyJob* djobs[2] = {nullptr, nullptr};  // batch-wide upload / download job tables (2 per instance)
   int red_blocks = 296;
   int64_t launches = 0;
   int tx = 16, ty = 32;
@@ -834,6 +876,8 @@ extern "C" int gp_batch_destroy(gp_batch* b) {
   if (b->pool) cudaFree(b->pool);
   if (b->partials) cudaFree(b->partials);
   if (b->stage) cudaFree(b->stage);
+  for (CopyJob* j : b->djobs)
+    if (j) cudaFree(j);
   if (b->reduced) cudaFree(b->reduced);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -901,11 +945,35 @@ extern "C" int gp_batch_create(const gp_model* models, int n, gp_batch** out) {
   return GP_OK;
 }
 
-static int batch_copy(gp_batch* b, int i, const double* host, int nplanes, bool is_phi, bool up) {
+// The device address of page-locked host memory the device can reach (mapped), or nullptr
+// (pageable memory: copied through the staging buffer).
+static double* mapped_host(const double* host) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? static_cast<double*>(a.devicePointer) : nullptr;
+}
+
+static int batch_copy(gp_batch* b, int i, const double* host, int nplanes, bool is_phi, bool up,
+                      bool direct = false) {
   const gp_model& m = b->models[i];
   const int64_t mx = m.mesh_x, my = m.mesh_y;
   float* dev = b->pool + (is_phi ? b->off_phi[b->parity][i] : b->off_mu[b->parity][i]);
   const size_t bytes = (size_t)nplanes * mx * my * sizeof(double);
+  // queued copies of page-locked host arrays: the conversion kernel reads (writes) the host
+  // array itself across the link, with no staging copy between the two
+  double* const hdev = direct ? mapped_host(host) : nullptr;
+  if (hdev) {
+    if (up)
+      k_pack<float><<<592, 256, 0, b->stream>>>(hdev, dev, (int)mx, (int)my, b->pitch[i], b->plane[i], nplanes);
+    else
+      k_unpack<float><<<592, 256, 0, b->stream>>>(dev, hdev, (int)mx, (int)my, b->pitch[i], b->plane[i], nplanes);
+    b->launches++;
+    GP_CUDA(cudaGetLastError());
+    return GP_OK;
+  }
   GP_CUDA(ensure_stage(&b->stage, &b->stage_bytes, bytes, b->stream));
   double* const stage = b->stage;
   if (up) {
@@ -922,8 +990,8 @@ static int batch_copy(gp_batch* b, int i, const double* host, int nplanes, bool 
 
 static int batch_upload(gp_batch* b, int i, const double* phi, const double* mu, bool wait) {
   if (!b || i < 0 || i >= b->n || !phi || !mu) return GP_E_ARG;
-  int rc = batch_copy(b, i, phi, b->models[i].N, true, true);
-  if (rc == GP_OK) rc = batch_copy(b, i, mu, b->models[i].K1, false, true);
+  int rc = batch_copy(b, i, phi, b->models[i].N, true, true, !wait);
+  if (rc == GP_OK) rc = batch_copy(b, i, mu, b->models[i].K1, false, true, !wait);
   if (rc == GP_OK) GP_CUDA(gp_f32_batch_invalidate(b->f32, b->stream));
   if (rc == GP_OK && wait) GP_CUDA(cudaStreamSynchronize(b->stream));
   b->have_prev = 0;
@@ -932,8 +1000,8 @@ static int batch_upload(gp_batch* b, int i, const double* phi, const double* mu,
 
 static int batch_download(gp_batch* b, int i, double* phi, double* mu, bool wait) {
   if (!b || i < 0 || i >= b->n || !phi || !mu) return GP_E_ARG;
-  int rc = batch_copy(b, i, phi, b->models[i].N, true, false);
-  if (rc == GP_OK) rc = batch_copy(b, i, mu, b->models[i].K1, false, false);
+  int rc = batch_copy(b, i, phi, b->models[i].N, true, false, !wait);
+  if (rc == GP_OK) rc = batch_copy(b, i, mu, b->models[i].K1, false, false, !wait);
   if (rc == GP_OK && wait) GP_CUDA(cudaStreamSynchronize(b->stream));
   return rc;
 }
@@ -952,6 +1020,58 @@ extern "C" int gp_batch_upload_async(gp_batch* b, int i, const double* phi, cons
 
 extern "C" int gp_batch_download_async(gp_batch* b, int i, double* phi, double* mu) {
   return batch_download(b, i, phi, mu, false);
+}
+
+// Every instance at once, queued: page-locked host arrays move in one conversion launch over
+// all of them; an instance with a pageable array goes through the staging copies instead.
+static int batch_all(gp_batch* b, const double* const* phi, const double* const* mu, bool up) {
+  if (!b || !phi || !mu) return GP_E_ARG;
+  for (int i = 0; i < b->n; i++)
+    if (!phi[i] || !mu[i]) return GP_E_ARG;
+  std::vector<CopyJob> jobs;
+  jobs.reserve(2 * (size_t)b->n);
+  for (int i = 0; i < b->n; i++) {
+    double* hp = mapped_host(phi[i]);
+    double* hm = mapped_host(mu[i]);
+    const gp_model& m = b->models[i];
+    if (!hp || !hm) {  // pageable: the per-instance path
+      int rc = up ? batch_upload(b, i, phi[i], mu[i], false) : batch_download(b, i, (double*)phi[i], (double*)mu[i], false);
+      if (rc != GP_OK) return rc;
+      continue;
+    }
+    for (int f = 0; f < 2; f++) {
+      CopyJob J;
+      J.host = f ? hm : hp;
+      J.dev = b->pool + (f ? b->off_mu[b->parity][i] : b->off_phi[b->parity][i]);
+      J.mx = (int)m.mesh_x;
+      J.my = (int)m.mesh_y;
+      J.pitch = b->pitch[i];
+      J.nplanes = f ? m.K1 : m.N;
+      J.plane = b->plane[i];
+      jobs.push_back(J);
+    }
+  }
+  if (!jobs.empty()) {
+    CopyJob*& dj = b->djobs[up ? 0 : 1];
+    if (!dj) GP_CUDA(cudaMalloc(&dj, sizeof(CopyJob) * 2 * (size_t)b->n));
+    GP_CUDA(cudaMemcpyAsync(dj, jobs.data(), sizeof(CopyJob) * jobs.size(), cudaMemcpyHostToDevice, b->stream));
+    k_convert_jobs<<<dim3(32, (unsigned)jobs.size()), 256, 0, b->stream>>>(dj, up ? 1 : 0);
+    GP_CUDA(cudaGetLastError());
+    b->launches++;
+  }
+  if (up) {
+    GP_CUDA(gp_f32_batch_invalidate(b->f32, b->stream));
+    b->have_prev = 0;
+  }
+  return GP_OK;
+}
+
+extern "C" int gp_batch_upload_all(gp_batch* b, const double* const* phi, const double* const* mu) {
+  return batch_all(b, phi, mu, true);
+}
+
+extern "C" int gp_batch_download_all(gp_batch* b, double* const* phi, double* const* mu) {
+  return batch_all(b, (const double* const*)phi, (const double* const*)mu, false);
 }
 
 // One launch call of the configured depth: a single step, or a blocked pair
@@ -1053,7 +1173,7 @@ extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
       m, b->pool + b->off_phi[cur][i], b->pool + b->off_mu[cur][i], b->pool + b->off_phi[prv][i],
       b->pool + b->off_mu[prv][i], b->have_prev, b->pitch[i], b->plane[i], b->partials, gp_temp_after(m, b->tstep));
   GP_CUDA(cudaGetLastError());
-  k_stats_final<<<1, 64, 0, b->stream>>>(m.N, m.K1, b->partials, b->red_blocks, b->reduced,
+  k_stats_final<<<64, kFinalThreads, 0, b->stream>>>(m.N, m.K1, b->partials, b->red_blocks, b->reduced,
                                          gp_f32_batch_error_word(b->f32));
   GP_CUDA(cudaGetLastError());
   b->launches += 2;

@@ -359,26 +359,48 @@ def test_nonisothermal_batch_equals_contexts_and_resumes():
 
 
 def test_async_upload_download_equal_the_waiting_ones():
-    """Queued uploads and downloads of every instance (no host wait between instances, one sync)
-    give the state the waiting calls give."""
+    """Queued uploads and downloads of every instance (no host wait between instances, one sync),
+    through the staging buffer (pageable arrays) or read and written in place by the conversion
+    kernels (page-locked arrays), give the state the waiting calls give."""
     cases = [configs.binary_case(96, 64, gap=1.0, supersat=0.55, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
                                  seed=(0, 0, 8.0)),
              configs.binary_case(160, 128, gap=1.0, supersat=0.5, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
                                  seed=(80, 64, 9.0))]
     loaded = [mb.load_case(c) for c in cases]
     models = [m for m, _, _ in loaded]
+    import torch
+
+    def pinned(a):  # page-locked host array: the queued copies read / write it in place
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+
     res = []
-    for wait in (True, False):
-        held = [(np.ascontiguousarray(p), np.ascontiguousarray(u)) for _, p, u in loaded]  # alive until sync
+    for wait, pin in ((True, False), (False, False), (False, True)):
+        held = [((pinned(p), pinned(u)) if pin else (np.ascontiguousarray(p), np.ascontiguousarray(u)))
+                for _, p, u in loaded]  # alive until sync
         with mb.Batch(models) as b:
             for i, (p, u) in enumerate(held):
                 b.upload(i, p, u, wait=wait)
             b.step(30)
-            outs = [b.download(i, wait=wait) for i in range(len(models))]
+            outs = [b.download(i, *((pinned(np.zeros_like(p)), pinned(np.zeros_like(u))) if pin else (None, None)),
+                               wait=wait) for i, (p, u) in enumerate(held)]
             b.sync()
             res.append([(p.copy(), u.copy()) for p, u in outs])
-    for (p1, u1), (p0, u0) in zip(res[1], res[0]):
-        assert np.array_equal(p1, p0) and np.array_equal(u1, u0)
+    # every instance at once: one page-locked instance and one pageable, mixed
+    held = [(pinned(loaded[0][1]), pinned(loaded[0][2])),
+            (np.ascontiguousarray(loaded[1][1]), np.ascontiguousarray(loaded[1][2]))]
+    outs = [(pinned(np.zeros_like(held[0][0])), pinned(np.zeros_like(held[0][1]))),
+            (np.zeros_like(held[1][0]), np.zeros_like(held[1][1]))]
+    with mb.Batch(models) as b:
+        b.upload_all(held)
+        b.step(30)
+        b.download_all(outs)
+        b.sync()
+        res.append([(p.copy(), u.copy()) for p, u in outs])
+    for r in res[1:]:
+        for (p1, u1), (p0, u0) in zip(r, res[0]):
+            assert np.array_equal(p1, p0) and np.array_equal(u1, u0)
 
 
 def test_compensated_accumulation():
