@@ -571,19 +571,19 @@ extern "C" int64_t gp_launch_count(const gp_ctx* c) { return c ? c->launches : 0
 // slots of the reduction vector
 struct StatLayout {
   int N, K1;
-  __host__ __device__ int phi_max(int a) const { return a; }
-  __host__ __device__ int phi_min(int a) const { return N + a; }
-  __host__ __device__ int rel_phi(int a) const { return 2 * N + a; }
-  __host__ __device__ int phase(int a) const { return 3 * N + a; }
-  __host__ __device__ int mu_max(int k) const { return 4 * N + k; }
-  __host__ __device__ int mu_min(int k) const { return 4 * N + K1 + k; }
-  __host__ __device__ int rel_mu(int k) const { return 4 * N + 2 * K1 + k; }
-  __host__ __device__ int solute(int k) const { return 4 * N + 3 * K1 + k; }
-  __host__ __device__ int nonfinite() const { return 4 * N + 4 * K1; }
-  __host__ __device__ int energy(int e) const { return 4 * N + 4 * K1 + 1 + e; }  // gradient, potential, chemical, grand
-  __host__ __device__ int count() const { return 4 * N + 4 * K1 + 5; }
-  __host__ __device__ bool is_max(int s) const { return s < N || (s >= 4 * N && s < 4 * N + K1); }
-  __host__ __device__ bool is_min(int s) const {
+  __host__ __device__ constexpr int phi_max(int a) const { return a; }
+  __host__ __device__ constexpr int phi_min(int a) const { return N + a; }
+  __host__ __device__ constexpr int rel_phi(int a) const { return 2 * N + a; }
+  __host__ __device__ constexpr int phase(int a) const { return 3 * N + a; }
+  __host__ __device__ constexpr int mu_max(int k) const { return 4 * N + k; }
+  __host__ __device__ constexpr int mu_min(int k) const { return 4 * N + K1 + k; }
+  __host__ __device__ constexpr int rel_mu(int k) const { return 4 * N + 2 * K1 + k; }
+  __host__ __device__ constexpr int solute(int k) const { return 4 * N + 3 * K1 + k; }
+  __host__ __device__ constexpr int nonfinite() const { return 4 * N + 4 * K1; }
+  __host__ __device__ constexpr int energy(int e) const { return 4 * N + 4 * K1 + 1 + e; }  // gradient, potential, chemical, grand
+  __host__ __device__ constexpr int count() const { return 4 * N + 4 * K1 + 5; }
+  __host__ __device__ constexpr bool is_max(int s) const { return s < N || (s >= 4 * N && s < 4 * N + K1); }
+  __host__ __device__ constexpr bool is_min(int s) const {
     return (s >= N && s < 2 * N) || (s >= 4 * N + K1 && s < 4 * N + 2 * K1);
   }
 };
@@ -614,10 +614,9 @@ __device__ __forceinline__ double stat_ac(double dab, double q0, double q1) {
 // Energy densities of interior cell (x, y) (the integrands of gp_stats' energies), FP64 from the
 // stored state; neighbours of edge cells by the boundary map of phi.  e[0] gradient (with eps),
 // e[1] potential (with 1/eps), e[2] sum_a h_a f_a(c_a), e[3] sum_a h_a psi_a (psi_a = f_a - mu.c_a).
-template <typename T>
-__device__ void cell_energy(const gp_model& m, const T* __restrict__ phi, int pitch, int64_t plane, int x, int y,
-                            const double* ph, const double* mm, double* e, Th th) {
-  const int N = m.N, K1 = m.K1;
+template <typename T, int N, int K1>
+__device__ __forceinline__ void cell_energy(const gp_model& m, const T* __restrict__ phi, int pitch, int64_t plane,
+                                            int x, int y, const double* ph, const double* mm, double* e, Th th) {
   double gx[GP_MAX_PHASES], gy[GP_MAX_PHASES];
   const int xm = gp_map(x - 1, (int)m.mesh_x, m.bc_phi[0]), xp = gp_map(x + 1, (int)m.mesh_x, m.bc_phi[0]);
   const int ym = gp_map(y - 1, (int)m.mesh_y, m.bc_phi[3]), yp = gp_map(y + 1, (int)m.mesh_y, m.bc_phi[3]);
@@ -648,14 +647,14 @@ __device__ void cell_energy(const gp_model& m, const T* __restrict__ phi, int pi
       for (int c = b + 1; c < N; c++)
         if (b != a && c != a) s1 += ph[b] * ph[c];
     h += 2.0 * ph[a] * s1;
-    double c[GP_MAX_K1], f = C_T(m, th, a), mc = 0.0;
+    double c[GP_MAX_K1], f = C_Tn<N, K1>(m, th, a), mc = 0.0;
     for (int k = 0; k < K1; k++) {
       c[k] = 0.0;
       for (int l = 0; l < K1; l++) c[k] += m.cmu[a][k][l] * (mm[l] - beff(m, th, a, l));
     }
     for (int k = 0; k < K1; k++) {
       for (int l = k; l < K1; l++) f += m.A[a][k][l] * c[k] * c[l];
-      f += B_T(m, th, k, a) * c[k];
+      f += B_Tn<N, K1>(m, th, k, a) * c[k];
       mc += mm[k] * c[k];
     }
     fch += h * f;
@@ -667,22 +666,26 @@ __device__ void cell_energy(const gp_model& m, const T* __restrict__ phi, int pi
 
 // One pass over the interior: each block writes its partial vector.
 // The solute integrand is sum_a c_a(mu) h_a(phi) (file_writer.h:203-235).
-template <typename T>
+template <typename T, int N, int K1>
 __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model m, const T* __restrict__ phi, const T* __restrict__ mu,
                                                const T* __restrict__ phi_prev, const T* __restrict__ mu_prev,
                                                int have_prev, int pitch, int64_t plane, double* __restrict__ partials,
                                                gp_temp_step temp) {
-  const StatLayout L{m.N, m.K1};
-  const int S = L.count();
-  double acc[kStatSlots];
+  // the phase and component counts fixed at compile time: every slot index is a constant and the
+  // accumulators stay in registers
+  constexpr StatLayout L{N, K1};
+  constexpr int S = L.count();
+  double acc[S];
+#pragma unroll
   for (int s = 0; s < S; s++) acc[s] = ident(L, s);
   const int64_t ncell = (int64_t)m.mesh_x * m.mesh_y;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncell; i += (int64_t)gridDim.x * blockDim.x) {
     const int x = (int)(i / m.mesh_y), y = (int)(i % m.mesh_y);
     const int64_t o = (int64_t)x * pitch + y;
-    double ph[GP_MAX_PHASES], mm[GP_MAX_K1];
+    double ph[N], mm[K1];
     bool bad = false;
-    for (int a = 0; a < m.N; a++) {
+#pragma unroll
+    for (int a = 0; a < N; a++) {
       ph[a] = (double)phi[o + a * plane];
       bad |= !isfinite(ph[a]);
       acc[L.phi_max(a)] = fmax(acc[L.phi_max(a)], ph[a]);
@@ -693,7 +696,8 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
         acc[L.rel_phi(a)] += d * d;
       }
     }
-    for (int k = 0; k < m.K1; k++) {
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
       mm[k] = (double)mu[o + k * plane];
       bad |= !isfinite(mm[k]);
       acc[L.mu_max(k)] = fmax(acc[L.mu_max(k)], mm[k]);
@@ -707,14 +711,19 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
     Th th;
     th.on = m.nonisothermal;
     th.T = m.nonisothermal ? temp.bottom + (double)(y + 3) * temp.grad : m.T;
-    for (int k = 0; k < m.K1; k++) {
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
       double comp = 0.0;
-      for (int a = 0; a < m.N; a++) {
+#pragma unroll
+      for (int a = 0; a < N; a++) {
         double cm = 0.0;
-        for (int l = 0; l < m.K1; l++) cm += m.cmu[a][k][l] * (mm[l] - beff(m, th, a, l));
+#pragma unroll
+        for (int l = 0; l < K1; l++) cm += m.cmu[a][k][l] * (mm[l] - beff(m, th, a, l));
         double h = 3.0 * ph[a] * ph[a] - 2.0 * ph[a] * ph[a] * ph[a], s1 = 0.0;
-        for (int b = 0; b < m.N; b++)
-          for (int c = b + 1; c < m.N; c++)
+#pragma unroll
+        for (int b = 0; b < N; b++)
+#pragma unroll
+          for (int c = b + 1; c < N; c++)
             if (b != a && c != a) s1 += ph[b] * ph[c];
         s1 *= 2.0 * ph[a];
         comp += cm * (h + s1);
@@ -722,7 +731,7 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
       acc[L.solute(k)] += comp;
     }
     double e[4];
-    cell_energy<T>(m, phi, pitch, plane, x, y, ph, mm, e, th);
+    cell_energy<T, N, K1>(m, phi, pitch, plane, x, y, ph, mm, e, th);
     acc[L.energy(0)] += e[0];
     acc[L.energy(1)] += e[1];
     acc[L.energy(2)] += e[2];
@@ -731,6 +740,7 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
   }
   __shared__ double red[8][kStatSlots];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
   for (int s = 0; s < S; s++) {
     double v = acc[s];
     for (int off = 16; off > 0; off >>= 1) v = combine(L, s, v, __shfl_down_sync(0xffffffffu, v, off));
@@ -743,6 +753,23 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ gp_model 
     for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = combine(L, s, v, red[w][s]);
     partials[(int64_t)blockIdx.x * 64 + s] = v;
   }
+}
+
+// k_stats for the model's phase and component counts.
+template <typename T>
+static void launch_stats(const gp_model& m, int blocks, cudaStream_t st, const T* phi, const T* mu, const T* phi_prev,
+                         const T* mu_prev, int have_prev, int pitch, int64_t plane, double* partials,
+                         gp_temp_step temp) {
+#define GP_STATS(NN, KK)                                                                                        \
+  if (m.N == NN && m.K1 == KK) {                                                                                \
+    k_stats<T, NN, KK><<<blocks, 256, 0, st>>>(m, phi, mu, phi_prev, mu_prev, have_prev, pitch, plane, partials, \
+                                               temp);                                                         \
+    return;                                                                                                     \
+  }
+  GP_STATS(2, 1) GP_STATS(2, 2) GP_STATS(2, 3) GP_STATS(3, 1) GP_STATS(3, 2) GP_STATS(3, 3)
+  GP_STATS(4, 1) GP_STATS(4, 2) GP_STATS(4, 3) GP_STATS(5, 1) GP_STATS(5, 2) GP_STATS(5, 3)
+  GP_STATS(6, 1) GP_STATS(6, 2) GP_STATS(6, 3)
+#undef GP_STATS
 }
 
 // Final combine of the block partials, one block per slot (launched with 64 blocks of
@@ -787,13 +814,13 @@ extern "C" int gp_get_stats(gp_ctx* c, gp_stats* out) {
   const int cur = c->cur, prv = 1 - c->cur;
   const gp_temp_step ts = gp_temp_after(m, c->tstep);  // the temperature after the last step
   if (c->precision == GP_FP64)
-    k_stats<double><<<c->red_blocks, 256, 0, c->stream>>>(m, (const double*)c->phi[cur], (const double*)c->mu[cur],
-                                                         (const double*)c->phi[prv], (const double*)c->mu[prv],
-                                                         c->have_prev, c->pitch, c->plane, c->partials, ts);
+    launch_stats<double>(m, c->red_blocks, c->stream, (const double*)c->phi[cur], (const double*)c->mu[cur],
+                         (const double*)c->phi[prv], (const double*)c->mu[prv], c->have_prev, c->pitch, c->plane,
+                         c->partials, ts);
   else
-    k_stats<float><<<c->red_blocks, 256, 0, c->stream>>>(m, (const float*)c->phi[cur], (const float*)c->mu[cur],
-                                                        (const float*)c->phi[prv], (const float*)c->mu[prv],
-                                                        c->have_prev, c->pitch, c->plane, c->partials, ts);
+    launch_stats<float>(m, c->red_blocks, c->stream, (const float*)c->phi[cur], (const float*)c->mu[cur],
+                        (const float*)c->phi[prv], (const float*)c->mu[prv], c->have_prev, c->pitch, c->plane,
+                        c->partials, ts);
   GP_CUDA(cudaGetLastError());
   k_stats_final<<<64, kFinalThreads, 0, c->stream>>>(m.N, m.K1, c->partials, c->red_blocks, c->reduced,
                                          c->f32 ? gp_f32_batch_error_word(c->f32) : nullptr);
@@ -1169,9 +1196,9 @@ extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
   if (!b || i < 0 || i >= b->n || !out) return GP_E_ARG;
   const gp_model& m = b->models[i];
   const int cur = b->parity, prv = 1 - b->parity;
-  k_stats<float><<<b->red_blocks, 256, 0, b->stream>>>(
-      m, b->pool + b->off_phi[cur][i], b->pool + b->off_mu[cur][i], b->pool + b->off_phi[prv][i],
-      b->pool + b->off_mu[prv][i], b->have_prev, b->pitch[i], b->plane[i], b->partials, gp_temp_after(m, b->tstep));
+  launch_stats<float>(m, b->red_blocks, b->stream, b->pool + b->off_phi[cur][i], b->pool + b->off_mu[cur][i],
+                      b->pool + b->off_phi[prv][i], b->pool + b->off_mu[prv][i], b->have_prev, b->pitch[i],
+                      b->plane[i], b->partials, gp_temp_after(m, b->tstep));
   GP_CUDA(cudaGetLastError());
   k_stats_final<<<64, kFinalThreads, 0, b->stream>>>(m.N, m.K1, b->partials, b->red_blocks, b->reduced,
                                          gp_f32_batch_error_word(b->f32));
