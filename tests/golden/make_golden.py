@@ -146,6 +146,34 @@ def cases():
     c.tempgrady = (0.96, 0.05, 24.0, 0.0, 0.2)
     c.bc_T = (3, 3, 0, 0)
     out["tempgrad_three_phase_well"] = (c, [1, 20, 40])
+    # the largest sizes the kernels take: six phases (five solid grains and the liquid), four
+    # components (three independent mu, the reference's LU inverse), non-diagonal A, well potential
+    # with the three-phase term, mixed boundaries
+    N, K1 = 6, 3
+    sol = list(range(N - 1))
+    ceq, cfill, slopes = [], [], []
+    for a in sol:
+        cs = [round(0.1 + 0.05 * a, 2), round(0.3 - 0.04 * a, 2), round(0.05 + 0.03 * a, 2)]
+        cl = [0.2, 0.15, 0.1]
+        ceq += [(a, a, *cs), (a, N - 1, *cl), (N - 1, a, *cl)]
+        cfill += [(a, a, *cs), (a, N - 1, *cl), (N - 1, a, *cl)]
+        slopes += [(a, a, 0.45, 0.4, 0.35), (a, N - 1, 0.45, 0.4, 0.35), (N - 1, a, 0.45, 0.4, 0.35)]
+    ceq.append((N - 1, N - 1, 0.2, 0.15, 0.1))
+    cfill.append((N - 1, N - 1, 0.17, 0.12, 0.08))
+    slopes.append((N - 1, N - 1, 0.45, 0.4, 0.35))
+    pairs = N * (N - 1) // 2
+    c = configs.Case(mesh_x=30, mesh_y=26, dx=1.0, dt=0.02, N=N, K=K1 + 1, ntimesteps=40, epsilon=4.0, tau=1.0,
+                     gamma=[1.0 + 0.05 * i for i in range(pairs)], tau_ab=[1.2] * pairs, aniso=0, dab=[0.0] * pairs,
+                     function_w=2, gamma_abc=[4.0] * (N * (N - 1) * (N - 2) // 6),
+                     diffusivity=[(1, a, 0.05, 0.04, 0.03) for a in sol] + [(1, N - 1, 1.0, 0.8, 0.6)],
+                     A=[(a, 1.0 + 0.1 * a, 1.1, 0.9, 0.1, -0.05, 0.08) for a in range(N)],
+                     ceq=ceq, cfill=cfill, slopes=slopes, solver=None,
+                     bc_phi=(3, 3, 1, 1), bc_mu=(3, 3, 1, 1),
+                     phases=["g1", "g2", "g3", "g4", "g5", "liq"], components=["A", "B", "C", "D"],
+                     fills=[("FILLCYLINDER", [0, 6, 6, 0, 0, 4.0]), ("FILLCYLINDER", [1, 22, 6, 0, 0, 4.5]),
+                            ("FILLCYLINDER", [2, 15, 13, 0, 0, 5.0]), ("FILLCYLINDER", [3, 6, 20, 0, 0, 4.0]),
+                            ("FILLCYLINDER", [4, 23, 20, 0, 0, 4.5])])
+    out["six_phase_four_comp"] = (c, [1, 20, 40])
     return out
 
 

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("case", ["iso_obst_bin", "aniso_obst_bin_per", "four_phase_ternary", "smooth_aniso_obst",
-                                  "tempgrad_three_phase_well"])
+                                  "tempgrad_three_phase_well", "six_phase_four_comp"])
 def test_driver_output_matches_reference(case):
     assert case in golden_cases()
     g = load_golden(case)
