@@ -128,6 +128,57 @@ def test_long_runs_bitexact_vs_oracle(name):
     assert np.array_equal(u, om_), f"mu max |diff| {np.abs(u - om_).max()}"
 
 
+RAGGED = [(4, 4, (1, 1, 1, 1)), (5, 7, (3, 3, 3, 3)), (4, 37, (1, 1, 3, 3)), (33, 5, (3, 3, 1, 1)),
+          (6, 6, (1, 1, 1, 1))]
+
+
+@pytest.mark.parametrize("mx,my,bc", RAGGED)
+def test_smallest_and_ragged_grids(mx, my, bc):
+    """The smallest grids the step takes (4 cells on an axis) and ragged ones, Neumann and periodic:
+    FP64 bit-exact to the oracle, FP32 within its tolerance, and a FP32 batch of all of them
+    (partial tiles only, the narrow band on) equal to FP32 contexts bit for bit."""
+    case = configs.binary_case(mx, my, gap=1.0, supersat=0.5, eps=2.0, delta=0.02, dt=0.05, tau=0.9,
+                               seed=(mx // 2, my // 2, min(mx, my) / 3.0), bc=bc, steps=50)
+    m, phi, mu, op, om_ = _oracle_run(case, 50)
+    with mb.Context(m, mb.GP_FP64) as ctx:
+        ctx.upload(phi, mu)
+        ctx.step(50)
+        p, u = ctx.download()
+    assert np.array_equal(p, op) and np.array_equal(u, om_)
+    with mb.Context(m, mb.GP_FP32) as ctx:
+        ctx.upload(phi, mu)
+        ctx.step(50)
+        p32, u32 = ctx.download()
+    assert np.abs(p32 - p).max() <= 1e-4 and np.abs(u32 - u).max() <= 1e-3
+
+
+def test_ragged_grids_in_one_batch():
+    loaded = [mb.load_case(configs.binary_case(mx, my, gap=1.0, supersat=0.5, eps=2.0, delta=0.02, dt=0.05,
+                                               tau=0.9, seed=(mx // 2, my // 2, min(mx, my) / 3.0), bc=bc,
+                                               steps=50)) for mx, my, bc in RAGGED]
+    ref = []
+    for m, phi, mu in loaded:
+        with mb.Context(m, mb.GP_FP32) as ctx:
+            ctx.upload(phi, mu)
+            ctx.step(50)
+            ref.append(ctx.download())
+    with mb.Batch([m for m, _, _ in loaded]) as b:
+        for i, (_, phi, mu) in enumerate(loaded):
+            b.upload(i, phi, mu)
+        b.step(50)
+        for i, (p0, u0) in enumerate(ref):
+            p1, u1 = b.download(i)
+            assert np.array_equal(p1, p0) and np.array_equal(u1, u0), i
+
+
+def test_grids_below_four_cells_are_refused():
+    case = configs.binary_case(3, 12, gap=1.0, supersat=0.5, eps=2.0, dt=0.05, tau=0.9, seed=(1, 6, 1.0), steps=5)
+    with tempfile.TemporaryDirectory() as d:
+        ip, fp = case.write(d)
+        with pytest.raises(mb.GpError):  # by the input reader or by the context
+            mb.Context(mb.Input(ip, fp).model(), mb.GP_FP64)
+
+
 @pytest.mark.parametrize("name", long_cases())
 def test_config1_full_run_matches_reference(name):
     """200x200, 10,000 steps: every row of the final state equals the reference's."""
