@@ -357,6 +357,15 @@ def test_nonisothermal_batch_equals_contexts_and_resumes():
         p64, u64 = c64.download()
     assert np.abs(ref[0][0] - p64).max() <= 1e-4
     assert np.abs(ref[0][1] - u64).max() <= 1e-3
+    # compensated accumulation under the gradient, blocked pairs: still within the tolerance
+    with mb.Batch(models) as b:
+        b.set_compensated(True)
+        b.set_depth(2)
+        for i in range(2):
+            b.upload(i, phi, mu)
+        b.step(steps)
+        pc, uc = b.download(0)
+    assert np.abs(pc - p64).max() <= 1e-4 and np.abs(uc - u64).max() <= 1e-3
 
 
 def test_async_upload_download_equal_the_waiting_ones():
