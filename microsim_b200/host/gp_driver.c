@@ -10,8 +10,17 @@
  * Differences, stated: the progress extrema are sampled when they are printed
  * (the reference updates them every step, ghost rings included); with fp32
  * the first step after a moving-frame shift reads ghost rows through the
- * boundary map (fp64 reproduces the reference's shifted ghost rows);
- * non-isothermal inputs are rejected with a message.
+ * boundary map (fp64 reproduces the reference's shifted ghost rows); a restart
+ * (STARTTIME > 0) under a frozen temperature gradient is rejected with a
+ * message.
+ *
+ * `microsim_gp_b200 --batch list.txt` (no counterpart in the reference, which
+ * runs one simulation per process) runs many simulations as one FP32 batch: each
+ * line of list.txt is `<directory> <Input.in> <Filling.in> <Out>` (input paths
+ * relative to the directory), every instance writes its own
+ * <directory>/DATA/<Out>_<t>.vtk every SAVET of its own steps up to its own
+ * NTIMESTEPS.  The instances share NUMPHASES, NUMCOMPONENTS and the anisotropy
+ * switch; no moving frame, no restart, no progress lines.
  */
 #include <math.h>
 #include <stdio.h>
@@ -26,7 +35,123 @@ static int fail(const char *what, int rc) {
   return 1;
 }
 
+/* One simulation of a batch run. */
+typedef struct {
+  char dir[512], out[256];
+  gp_input *in;
+  gp_model m;
+  int64_t ntimesteps, saveT;
+  double *phi, *mu;
+} job_t;
+
+static int run_batch(const char *list) {
+  FILE *lf = fopen(list, "r");
+  if (!lf) {
+    fprintf(stderr, "microsim_gp_b200: cannot read %s\n", list);
+    return 2;
+  }
+  job_t *jobs = NULL;
+  int n = 0, cap = 0, rc;
+  char line[2048], ip[1100], fp[1100];
+  while (fgets(line, sizeof line, lf)) {
+    char d[512], i1[256], f1[256], o[256];
+    if (sscanf(line, "%511s %255s %255s %255s", d, i1, f1, o) != 4 || d[0] == '#') continue;
+    if (n == cap) {
+      cap = cap ? 2 * cap : 16;
+      job_t *nj = (job_t *)realloc(jobs, sizeof(job_t) * cap);
+      if (!nj) return fail("host allocation", GP_E_NOMEM);
+      jobs = nj;
+    }
+    job_t *j = &jobs[n];
+    memset(j, 0, sizeof *j);
+    snprintf(j->dir, sizeof j->dir, "%s", d);
+    snprintf(j->out, sizeof j->out, "%s", o);
+    snprintf(ip, sizeof ip, "%s/%s", d, i1);
+    snprintf(fp, sizeof fp, "%s/%s", d, f1);
+    if ((rc = gp_input_read(ip, fp, &j->in)) != GP_OK) return fail("reading inputs", rc);
+    if ((rc = gp_model_from_input(j->in, &j->m)) != GP_OK) return fail("model constants", rc);
+    int64_t nsmooth = 0, starttime = 0, restart = 0, shift = 0;
+    gp_input_get_long(j->in, "NTIMESTEPS", &j->ntimesteps);
+    gp_input_get_long(j->in, "SAVET", &j->saveT);
+    gp_input_get_long(j->in, "NSMOOTH", &nsmooth);
+    gp_input_get_long(j->in, "STARTTIME", &starttime);
+    gp_input_get_long(j->in, "RESTART", &restart);
+    gp_input_get_long(j->in, "Shift", &shift);
+    if (j->saveT <= 0) j->saveT = j->ntimesteps > 0 ? j->ntimesteps : 1;
+    if (shift || starttime || restart) {
+      fprintf(stderr, "microsim_gp_b200: %s: a moving frame or a restart is not available in a batch\n", ip);
+      return 2;
+    }
+    const size_t np = (size_t)j->m.mesh_x * (size_t)j->m.mesh_y;
+    j->phi = (double *)malloc(sizeof(double) * np * j->m.N);
+    j->mu = (double *)malloc(sizeof(double) * np * j->m.K1);
+    if (!j->phi || !j->mu) return fail("host allocation", GP_E_NOMEM);
+    if ((rc = gp_fill(j->in, &j->m, j->phi, j->mu)) != GP_OK) return fail("filling", rc);
+    char name[1400];
+    snprintf(name, sizeof name, "%s/DATA", d);
+    mkdir(name, 0777);
+    snprintf(name, sizeof name, "%s/DATA/%s_0.vtk", d, o);
+    if ((rc = gp_write_vtk(j->in, &j->m, name, j->phi, j->mu)) != GP_OK) return fail("vtk write", rc);
+    if (nsmooth > 1) { /* the smoothing pre-steps in FP64, as for a single fp32 run */
+      gp_ctx *pre = NULL;
+      if ((rc = gp_create(&j->m, GP_FP64, &pre)) != GP_OK) return fail("gp_create", rc);
+      if ((rc = gp_upload(pre, j->phi, j->mu)) != GP_OK) return fail("gp_upload", rc);
+      if ((rc = gp_smooth(pre, nsmooth - 1)) != GP_OK) return fail("gp_smooth", rc);
+      if ((rc = gp_download(pre, j->phi, j->mu)) != GP_OK) return fail("gp_download", rc);
+      gp_destroy(pre);
+    }
+    n++;
+  }
+  fclose(lf);
+  if (n == 0) {
+    fprintf(stderr, "microsim_gp_b200: %s lists no simulation\n", list);
+    return 2;
+  }
+  gp_model *models = (gp_model *)malloc(sizeof(gp_model) * n);
+  if (!models) return fail("host allocation", GP_E_NOMEM);
+  int64_t tmax = 0;
+  for (int i = 0; i < n; i++) {
+    models[i] = jobs[i].m;
+    if (jobs[i].ntimesteps > tmax) tmax = jobs[i].ntimesteps;
+  }
+  gp_batch *b = NULL;
+  if ((rc = gp_batch_create(models, n, &b)) != GP_OK) return fail("gp_batch_create", rc);
+  for (int i = 0; i < n; i++)
+    if ((rc = gp_batch_upload(b, i, jobs[i].phi, jobs[i].mu)) != GP_OK) return fail("gp_batch_upload", rc);
+  int tx, ty;
+  if ((rc = gp_batch_autotune(b, NULL, &tx, &ty)) != GP_OK) return fail("gp_batch_autotune", rc);
+  int64_t t = 0;
+  while (t < tmax) {
+    int64_t next = tmax; /* the next step some instance writes at */
+    for (int i = 0; i < n; i++) {
+      const int64_t ns = (t / jobs[i].saveT + 1) * jobs[i].saveT;
+      if (ns <= jobs[i].ntimesteps && ns < next) next = ns;
+    }
+    if ((rc = gp_batch_step(b, next - t)) != GP_OK) return fail("gp_batch_step", rc);
+    t = next;
+    for (int i = 0; i < n; i++) {
+      if (t > jobs[i].ntimesteps || t % jobs[i].saveT != 0) continue;
+      char name[1400];
+      if ((rc = gp_batch_download(b, i, jobs[i].phi, jobs[i].mu)) != GP_OK) return fail("gp_batch_download", rc);
+      snprintf(name, sizeof name, "%s/DATA/%s_%lld.vtk", jobs[i].dir, jobs[i].out, (long long)t);
+      if ((rc = gp_write_vtk_t(jobs[i].in, &jobs[i].m, name, jobs[i].phi, jobs[i].mu, t)) != GP_OK)
+        return fail("vtk write", rc);
+    }
+  }
+  if ((rc = gp_batch_sync(b)) != GP_OK) return fail("gp_batch_sync", rc);
+  gp_batch_destroy(b);
+  for (int i = 0; i < n; i++) {
+    gp_input_free(jobs[i].in);
+    free(jobs[i].phi);
+    free(jobs[i].mu);
+  }
+  free(jobs);
+  free(models);
+  return 0;
+}
+
 int main(int argc, char *argv[]) {
+  if (argc == 3 && !strcmp(argv[1], "--batch")) return run_batch(argv[2]);
   gp_input *in = NULL;
   gp_model m;
   gp_ctx *ctx = NULL;
@@ -34,7 +159,8 @@ int main(int argc, char *argv[]) {
   int precision = GP_FP64;
   int rc;
   if (argc < 4) {
-    fprintf(stderr, "usage: %s Input.in Filling.in Out [fp64|fp32]\n", argv[0]);
+    fprintf(stderr, "usage: %s Input.in Filling.in Out [fp64|fp32]\n       %s --batch list.txt\n", argv[0],
+            argv[0]);
     return 2;
   }
   if ((argc > 4 && !strcmp(argv[4], "fp32")) || (getenv("GP_PRECISION") && !strcmp(getenv("GP_PRECISION"), "fp32")))

@@ -13,6 +13,7 @@ import pytest
 
 from conftest import golden_cases, interior, load_golden, write_inputs
 import microsim_b200 as mb
+from microsim_b200 import configs
 
 pytestmark = pytest.mark.gpu
 
@@ -56,3 +57,33 @@ def test_driver_moving_frame_matches_reference():
         lines = open(os.path.join(d, "DATA", "shift.dat")).read().split()
     assert np.array_equal(phi, interior(g[f"phi_{t}"])) and np.array_equal(mu, interior(g[f"mu_{t}"]))
     assert int(lines[-2]) == t and int(lines[-1]) == int(g["shifts"][-1][2])
+
+
+def test_driver_batch_mode_equals_single_fp32_runs(tmp_path):
+    """`microsim_gp_b200 --batch list.txt`: two simulations of different sizes and lengths as one
+    FP32 batch write, file for file, the bytes of two single fp32 runs of the same inputs."""
+    cases = [configs.binary_case(40, 32, gap=1.0, supersat=0.5, eps=3.0, delta=0.02, dt=0.05, tau=1.3332,
+                                 seed=(20, 16, 6.0), steps=60, savet=30),
+             configs.binary_case(56, 48, gap=1.0, supersat=0.4, eps=3.0, delta=0.03, dt=0.05, tau=1.3332,
+                                 seed=(0, 0, 8.0), steps=90, savet=30)]
+    lines = []
+    for k, c in enumerate(cases):
+        d = tmp_path / f"sim{k}"
+        d.mkdir()
+        c.write(str(d))
+        lines.append(f"{d} Input.in Filling.in run{k}")
+        single = tmp_path / f"single{k}"
+        single.mkdir()
+        c.write(str(single))
+        r = subprocess.run([mb.DRIVER_PATH, "Input.in", "Filling.in", f"run{k}", "fp32"], cwd=single,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+    (tmp_path / "list.txt").write_text("\n".join(lines) + "\n")
+    r = subprocess.run([mb.DRIVER_PATH, "--batch", str(tmp_path / "list.txt")], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    for k, c in enumerate(cases):
+        for t in range(0, c.ntimesteps + 1, 30):
+            a = (tmp_path / f"sim{k}" / "DATA" / f"run{k}_{t}.vtk").read_bytes()
+            b = (tmp_path / f"single{k}" / "DATA" / f"run{k}_{t}.vtk").read_bytes()
+            assert a == b, (k, t)
