@@ -249,7 +249,10 @@ int64_t gp_launch_count(const gp_ctx *ctx);
 /* ---------------- batches: many independent instances, FP32 chosen form ---------------- */
 
 /* A batch of n instances (uneven sizes and parameters allowed; they must share
- * N, K1 and the anisotropy switch).  One kernel launch per time step covers
+ * N and K1; isotropic and anisotropic instances mix: the batch then runs the
+ * anisotropic kernels, with no anisotropy for the isotropic instances, whose
+ * results then differ from an isotropic batch's by FP32 rounding).  One
+ * kernel launch per time step covers
  * every tile of every instance; gp_batch_step replays the launches from a
  * captured CUDA graph.  No counterpart in the reference (one process = one
  * simulation there). */

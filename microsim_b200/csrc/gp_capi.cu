@@ -916,8 +916,8 @@ extern "C" int gp_batch_create(const gp_model* models, int n, gp_batch** out) {
   for (int i = 0; i < n; i++) {
     int rc = check_model(&models[i]);
     if (rc != GP_OK) return rc;
-    if (models[i].N != models[0].N || models[i].K1 != models[0].K1 || models[i].anisotropy != models[0].anisotropy) {
-      gp_set_error("gp_batch_create: instances of one batch must share N, K1 and the anisotropy switch");
+    if (models[i].N != models[0].N || models[i].K1 != models[0].K1) {
+      gp_set_error("gp_batch_create: instances of one batch must share N and K1");
       return GP_E_ARG;
     }
   }
@@ -1249,7 +1249,9 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
   const gp_model& m0 = b->models[0];
   char key[128];
   const int comp = gp_f32_batch_compensated(b->f32);
-  snprintf(key, sizeof key, "%d %d %d %lld %d %d", m0.N, m0.K1, m0.anisotropy, (long long)cells, b->n, comp);
+  int aniso = 0;  // the batch runs the anisotropic kernels when any instance is anisotropic
+  for (const gp_model& m : b->models) aniso |= m.anisotropy ? 1 : 0;
+  snprintf(key, sizeof key, "%d %d %d %lld %d %d", m0.N, m0.K1, aniso, (long long)cells, b->n, comp);
   if (cache_path) {
     FILE* f = fopen(cache_path, "r");
     if (f) {
@@ -1260,7 +1262,7 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
         double ms;
         if (sscanf(line, "%d %d %d %lld %d %d %d %d %d %d %d %d %d %lf", &N, &K1, &an, &c, &n, &cp, &tx, &ty, &lp,
                    &gq, &th, &sc, &dp, &ms) == 14 &&
-            N == m0.N && K1 == m0.K1 && an == m0.anisotropy && c == cells && n == b->n && cp == comp) {
+            N == m0.N && K1 == m0.K1 && an == aniso && c == cells && n == b->n && cp == comp) {
           fclose(f);
           if (tx_out) *tx_out = tx;
           if (ty_out) *ty_out = ty;

@@ -2082,7 +2082,7 @@ Model make_model(const gp_model& g) {
     for (int b = 0; b < MP; b++) {
       m.Gamma[a][b] = (float)g.Gamma[a][b];
       m.tau_ab[a][b] = (float)g.tau_ab[a][b];
-      m.dab[a][b] = (float)g.dab[a][b];
+      m.dab[a][b] = g.anisotropy ? (float)g.dab[a][b] : 0.f;  // an isotropic instance of an anisotropic batch: a_c = 1
       for (int i = 0; i < 2; i++)
         for (int j = 0; j < 2; j++) {
           m.R[a][b][i][j] = (float)g.R[a][b][i][j];
@@ -2271,16 +2271,20 @@ static void free_tiles(gp_f32_batch* b) {
 
 cudaError_t gp_f32_batch_create(const gp_model* models, int n, gp_f32_batch** out) {
   if (n < 1) return cudaErrorInvalidValue;
-  for (int i = 1; i < n; i++)
-    if (models[i].N != models[0].N || models[i].K1 != models[0].K1 || models[i].anisotropy != models[0].anisotropy)
-      return cudaErrorInvalidValue;
+  // one kernel set serves the batch: the anisotropic one when any instance is anisotropic (an
+  // isotropic instance then runs it with dab = 0, where a_c = 1 and its derivative terms vanish)
+  int aniso = 0;
+  for (int i = 0; i < n; i++) {
+    if (models[i].N != models[0].N || models[i].K1 != models[0].K1) return cudaErrorInvalidValue;
+    aniso |= models[i].anisotropy ? 1 : 0;
+  }
   KernelSet ks;
-  if (!pick(models[0].N, models[0].K1, models[0].anisotropy, 16, 32, &ks)) return cudaErrorNotSupported;
+  if (!pick(models[0].N, models[0].K1, aniso, 16, 32, &ks)) return cudaErrorNotSupported;
   gp_f32_batch* b = new gp_f32_batch();
   b->n = n;
   b->N = models[0].N;
   b->K1 = models[0].K1;
-  b->aniso = models[0].anisotropy;
+  b->aniso = aniso;
   b->gm.assign(models, models + n);
   std::vector<Model> hm(n);
   for (int i = 0; i < n; i++) hm[i] = make_model(models[i]);

@@ -19,8 +19,8 @@
  * line of list.txt is `<directory> <Input.in> <Filling.in> <Out>` (input paths
  * relative to the directory), every instance writes its own
  * <directory>/DATA/<Out>_<t>.vtk every SAVET of its own steps up to its own
- * NTIMESTEPS.  The instances share NUMPHASES, NUMCOMPONENTS and the anisotropy
- * switch; no moving frame, no restart, no progress lines.
+ * NTIMESTEPS.  The instances share NUMPHASES and NUMCOMPONENTS; no moving frame,
+ * no restart, no progress lines.
  */
 #include <math.h>
 #include <stdio.h>

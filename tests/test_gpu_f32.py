@@ -368,6 +368,37 @@ def test_nonisothermal_batch_equals_contexts_and_resumes():
     assert np.abs(pc - p64).max() <= 1e-4 and np.abs(uc - u64).max() <= 1e-3
 
 
+def test_isotropic_and_anisotropic_instances_in_one_batch():
+    """A batch mixing isotropic and anisotropic instances runs the anisotropic kernels with no
+    anisotropy for the isotropic ones: the anisotropic instances equal their own FP32 contexts bit
+    for bit; the isotropic ones go through the anisotropic kernel's (mathematically equal)
+    arithmetic and agree with their isotropic contexts to FP32 rounding."""
+    cases = [configs.binary_case(64, 48, gap=1.0, supersat=0.5, eps=4.0, dt=0.05, tau=1.7776, seed=(32, 24, 8.0)),
+             BINARY["aniso_corner"],
+             configs.binary_case(48, 80, gap=1.0, supersat=0.45, eps=3.0, dt=0.05, tau=1.3332, seed=(24, 40, 7.0),
+                                 bc=(3, 3, 3, 3))]
+    loaded = [mb.load_case(c) for c in cases]
+    assert [int(m.anisotropy) for m, _, _ in loaded] == [0, 1, 0]
+    ref = []
+    for m, phi, mu in loaded:
+        with mb.Context(m, mb.GP_FP32) as c:
+            c.upload(phi, mu)
+            c.step(200)
+            ref.append(c.download())
+    for depth in (1, 2):
+        with mb.Batch([m for m, _, _ in loaded]) as b:
+            b.set_depth(depth)
+            for i, (_, phi, mu) in enumerate(loaded):
+                b.upload(i, phi, mu)
+            b.step(200)
+            for i, (p0, u0) in enumerate(ref):
+                p1, u1 = b.download(i)
+                if loaded[i][0].anisotropy:
+                    assert np.array_equal(p1, p0) and np.array_equal(u1, u0), (depth, i)
+                else:
+                    assert np.abs(p1 - p0).max() <= 1e-5 and np.abs(u1 - u0).max() <= 1e-5, (depth, i)
+
+
 def test_async_upload_download_equal_the_waiting_ones():
     """Queued uploads and downloads of every instance (no host wait between instances, one sync),
     through the staging buffer (pageable arrays) or read and written in place by the conversion
