@@ -465,7 +465,8 @@ __host__ __device__ __forceinline__ int lean_phase(const uint32_t* __restrict__ 
 // THREADS per block (one tile): 256, or 512 for binary alloys (shorter per-thread chains, half
 // the resident blocks: faster when there are few interface tiles); the autotuner picks.
 template <int N, int K1, bool ANISO, int TX, int TY, int THREADS = 256>
-__global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS : (K1 >= 3 || THREADS > 256 ? 1 : 2))
+__global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS
+                                                              : (K1 >= 3 || N >= 5 || THREADS > 256 ? 1 : 2))
     k_step32(const Inst* __restrict__ insts, const Model* __restrict__ models, const int* __restrict__ tile_inst,
              const int2* __restrict__ glist, int* __restrict__ cnt, uint32_t* __restrict__ flags_out, int total,
              const int4* __restrict__ tile_desc, const uint32_t* __restrict__ flags_in, int keep_list) {
@@ -2167,8 +2168,10 @@ template <int N, int K1, bool AN>
 static bool pick_tile(int tx, int ty, KernelSet* k) {
   if (tx == 16 && ty == 32) { *k = make_set<N, K1, AN, 16, 32>(); return true; }
   if (tx == 8 && ty == 32) { *k = make_set<N, K1, AN, 8, 32>(); return true; }
-  if (tx == 32 && ty == 32) { *k = make_set<N, K1, AN, 32, 32>(); return true; }
-  if (tx == 16 && ty == 64) { *k = make_set<N, K1, AN, 16, 64>(); return true; }
+  if constexpr (N <= 4) {  // five or six phases: the larger tiles' shared memory exceeds a block's
+    if (tx == 32 && ty == 32) { *k = make_set<N, K1, AN, 32, 32>(); return true; }
+    if (tx == 16 && ty == 64) { *k = make_set<N, K1, AN, 16, 64>(); return true; }
+  }
   return false;
 }
 
@@ -2176,7 +2179,8 @@ static bool pick(int N, int K1, int an, int tx, int ty, KernelSet* k) {
 #define GP_PICK(NN, KK)                                                                        \
   if (N == NN && K1 == KK) return an ? pick_tile<NN, KK, true>(tx, ty, k) : pick_tile<NN, KK, false>(tx, ty, k);
   GP_PICK(2, 1) GP_PICK(2, 2) GP_PICK(3, 1) GP_PICK(3, 2) GP_PICK(4, 1) GP_PICK(4, 2)
-  GP_PICK(2, 3) GP_PICK(3, 3) GP_PICK(4, 3)
+  GP_PICK(2, 3) GP_PICK(3, 3) GP_PICK(4, 3) GP_PICK(5, 1) GP_PICK(5, 2) GP_PICK(5, 3)
+  GP_PICK(6, 1) GP_PICK(6, 2) GP_PICK(6, 3)
 #undef GP_PICK
   return false;
 }

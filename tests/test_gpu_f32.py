@@ -63,8 +63,7 @@ def test_four_phase_ternary_within_tolerance():
 
 
 @pytest.mark.parametrize("case", [c for c in golden_cases()
-                                  if c != "c1_literal_small" and "shifts" not in load_golden(c)
-                                  and int(np.ravel(load_golden(c)["c_NUMPHASES"])[0]) <= 4])  # the FP32 kernels' range
+                                  if c != "c1_literal_small" and "shifts" not in load_golden(c)])
 def test_golden_cases_within_tolerance_of_reference(case):
     g = load_golden(case)
     with tempfile.TemporaryDirectory() as d:
