@@ -157,7 +157,7 @@ def test_autotune_restores_state_and_caches(tmp_path):
 
 
 def test_tip_velocity_within_half_percent_of_fp64():
-    """The north-star bar on a reduced corner dendrite (256^2, 8,000 steps): the
+    """The accuracy bar of the FP32 form on a reduced corner dendrite (256^2, 8,000 steps): the
     FP32 form's tip velocity within 0.5% of the FP64 form's, solute mass within
     1e-4 (the full 1024^2 x 50,000-step run: python -m microsim_b200.validate)."""
     from microsim_b200 import validate
