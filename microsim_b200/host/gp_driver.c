@@ -19,8 +19,9 @@
  * line of list.txt is `<directory> <Input.in> <Filling.in> <Out>` (input paths
  * relative to the directory), every instance writes its own
  * <directory>/DATA/<Out>_<t>.vtk every SAVET of its own steps up to its own
- * NTIMESTEPS.  The instances share NUMPHASES and NUMCOMPONENTS; no moving frame,
- * no restart, no progress lines.
+ * NTIMESTEPS, and prints its progress lines every TRACK_PROGRESS steps after a
+ * "[<directory>]" line.  The instances share NUMPHASES and NUMCOMPONENTS; no
+ * moving frame, no restart.
  */
 #include <math.h>
 #include <stdio.h>
@@ -40,9 +41,41 @@ typedef struct {
   char dir[512], out[256];
   gp_input *in;
   gp_model m;
-  int64_t ntimesteps, saveT;
+  int64_t ntimesteps, saveT, track;
   double *phi, *mu;
 } job_t;
+
+/* The progress block of one instance (microsim_gp.c:137-147's lines, after a "[<directory>]" line). */
+static int batch_progress(gp_batch *b, int i, const job_t *j, int64_t t) {
+  gp_stats st;
+  int rc = gp_batch_get_stats(b, i, &st);
+  if (rc != GP_OK && rc != GP_E_NONFINITE) return fail("gp_batch_get_stats", rc);
+  char pname[GP_MAX_PHASES][GP_NAME_LEN], cname[GP_MAX_K1][GP_NAME_LEN];
+  int max_length = 0, a, k;
+  for (a = 0; a < j->m.N; a++) {
+    gp_input_name(j->in, 0, a, pname[a], GP_NAME_LEN);
+    if ((int)strlen(pname[a]) > max_length) max_length = (int)strlen(pname[a]);
+  }
+  for (k = 0; k < j->m.K1; k++) {
+    gp_input_name(j->in, 1, k, cname[k], GP_NAME_LEN);
+    if ((int)strlen(cname[k]) > max_length) max_length = (int)strlen(cname[k]);
+  }
+  double dt;
+  gp_input_get_double(j->in, "DELTA_t", &dt);
+  fprintf(stdout, "[%s]\nTime=%le\n", j->dir, t * dt);
+  for (a = 0; a < j->m.N; a++)
+    fprintf(stdout, "%*s, Max = %le, Min = %le, Relative_Change=%le\n", max_length, pname[a], st.phi_max[a],
+            st.phi_min[a], sqrt(st.rel_change_phi[a]));
+  for (k = 0; k < j->m.K1; k++)
+    fprintf(stdout, "%*s, Max = %le, Min = %le, Relative_Change=%le\n", max_length, cname[k], st.mu_max[k],
+            st.mu_min[k], sqrt(st.rel_change_mu[k]));
+  fprintf(stdout, "\n");
+  if (rc == GP_E_NONFINITE) {
+    fprintf(stderr, "microsim_gp_b200: %s: non-finite values at t=%lld (unstable DELTA_t?)\n", j->dir, (long long)t);
+    return 3;
+  }
+  return 0;
+}
 
 static int run_batch(const char *list) {
   FILE *lf = fopen(list, "r");
@@ -77,6 +110,7 @@ static int run_batch(const char *list) {
     gp_input_get_long(j->in, "STARTTIME", &starttime);
     gp_input_get_long(j->in, "RESTART", &restart);
     gp_input_get_long(j->in, "Shift", &shift);
+    gp_input_get_long(j->in, "TRACK_PROGRESS", &j->track);
     if (j->saveT <= 0) j->saveT = j->ntimesteps > 0 ? j->ntimesteps : 1;
     if (shift || starttime || restart) {
       fprintf(stderr, "microsim_gp_b200: %s: a moving frame or a restart is not available in a batch\n", ip);
@@ -122,14 +156,22 @@ static int run_batch(const char *list) {
   if ((rc = gp_batch_autotune(b, NULL, &tx, &ty)) != GP_OK) return fail("gp_batch_autotune", rc);
   int64_t t = 0;
   while (t < tmax) {
-    int64_t next = tmax; /* the next step some instance writes at */
+    int64_t next = tmax; /* the next step some instance writes or prints at */
     for (int i = 0; i < n; i++) {
       const int64_t ns = (t / jobs[i].saveT + 1) * jobs[i].saveT;
       if (ns <= jobs[i].ntimesteps && ns < next) next = ns;
+      if (jobs[i].track > 0) {
+        const int64_t nt = (t / jobs[i].track + 1) * jobs[i].track;
+        if (nt <= jobs[i].ntimesteps && nt < next) next = nt;
+      }
     }
     if ((rc = gp_batch_step(b, next - t)) != GP_OK) return fail("gp_batch_step", rc);
     t = next;
     for (int i = 0; i < n; i++) {
+      if (t <= jobs[i].ntimesteps && jobs[i].track > 0 && t % jobs[i].track == 0) {
+        const int prc = batch_progress(b, i, &jobs[i], t);
+        if (prc) return prc;
+      }
       if (t > jobs[i].ntimesteps || t % jobs[i].saveT != 0) continue;
       char name[1400];
       if ((rc = gp_batch_download(b, i, jobs[i].phi, jobs[i].mu)) != GP_OK) return fail("gp_batch_download", rc);

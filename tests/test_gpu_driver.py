@@ -82,6 +82,9 @@ def test_driver_batch_mode_equals_single_fp32_runs(tmp_path):
     r = subprocess.run([mb.DRIVER_PATH, "--batch", str(tmp_path / "list.txt")], cwd=tmp_path,
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
+    # progress lines every TRACK_PROGRESS (= SAVET here) steps of each instance, under its directory
+    assert r.stdout.count("Time=") == 2 + 3
+    assert r.stdout.count(f"[{tmp_path / 'sim1'}]") == 3
     for k, c in enumerate(cases):
         for t in range(0, c.ntimesteps + 1, 30):
             a = (tmp_path / f"sim{k}" / "DATA" / f"run{k}_{t}.vtk").read_bytes()
