@@ -294,7 +294,8 @@ def fp64_plain_rate(models, fields, steps, warmup, dev, world):
     workload: one context per instance, each on its own stream, all stepped
     concurrently; K steps between a CUDA event on a master stream (which every
     context's stream waits on) and the master's wait on every context's end
-    event."""
+    event.  An isothermal context replays its steps from a CUDA graph (gp_step),
+    captured during the warm-up."""
     import torch
     import microsim_b200 as mb
     ctxs = []
@@ -471,7 +472,9 @@ def run_ours(args, world, rank, local):
     # ---- FP64 plain on the same workload
     fp64 = None
     if not args.no_fp64:
-        fp64 = fp64_plain_rate(models, fields, max(3, min(args.steps, 10)), 1, dev, world)
+        # as many warm-up steps as timed ones: the timed steps then take the launch path (graph
+        # replays of isothermal runs, direct launches of the rest) that the warm-up prepared
+        fp64 = fp64_plain_rate(models, fields, 16, 16, dev, world)
 
     # ---- end to end through the C ABI: pinned host state in, K steps with the
     # progress statistics read back each step, state out

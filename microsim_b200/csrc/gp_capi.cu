@@ -116,6 +116,7 @@ struct gp_ctx {
   int red_blocks;
   int64_t launches;
   int64_t tstep = 0;  // steps taken (the frozen gradient's clock)
+  cudaGraphExec_t g64[2];  // FP64 isothermal: kF64GraphSteps steps from buffer parity 0 / 1, captured on first use
   // running extrema (microsim_gp.c prints running values since t = 0)
   double run_phi_max[GP_MAX_PHASES], run_phi_min[GP_MAX_PHASES];
   double run_mu_max[GP_MAX_K1], run_mu_min[GP_MAX_K1];
@@ -218,6 +219,8 @@ extern "C" int gp_destroy(gp_ctx* c) {
     if (c->phi[i]) cudaFree(c->phi[i]);
     if (c->mu[i]) cudaFree(c->mu[i]);
   }
+  for (int i = 0; i < 2; i++)
+    if (c->g64[i]) cudaGraphExecDestroy(c->g64[i]);
   if (c->dphi) cudaFree(c->dphi);
   if (c->gov) cudaFree(c->gov);
   if (c->f32) gp_f32_batch_destroy(c->f32);
@@ -339,9 +342,48 @@ extern "C" int gp_download_dphi(gp_ctx* c, double* dphi) {
   return GP_OK;
 }
 
+// An isothermal FP64 step is the same two launches every time (no per-step temperature), so
+// runs of kF64GraphSteps steps replay a CUDA graph captured once per starting buffer: one host
+// launch instead of 2 * kF64GraphSteps, which is what bounds many small instances stepped from
+// one host thread.  An even count returns the state to the buffer it started in.
+static const int kF64GraphSteps = 8;
+
+static int f64_graph(gp_ctx* c, cudaGraphExec_t* out) {
+  cudaGraphExec_t& ge = c->g64[c->cur];
+  if (!ge) {
+    const gp_temp_step ts = gp_temp_after(c->m, 0);  // not read by an isothermal step
+    cudaGraph_t g = nullptr;
+    GP_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int t = 0, p = c->cur; t < kF64GraphSteps && e == cudaSuccess; t++, p ^= 1)
+      e = gp_f64_step(c->m, c->pitch, c->plane, c->rpitch, c->rplane, (const double*)c->phi[p],
+                      (const double*)c->mu[p], c->dphi, (double*)c->phi[p ^ 1], (double*)c->mu[p ^ 1], c->stream,
+                      false, nullptr, &ts);
+    const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) ge = nullptr;
+    GP_CUDA(e);
+  }
+  *out = ge;
+  return GP_OK;
+}
+
 extern "C" int gp_step(gp_ctx* c, int64_t nsteps) {
   if (!c || nsteps < 0) return GP_E_ARG;
   for (int64_t t = 0; t < nsteps; t++) {
+    if (c->precision == GP_FP64 && !c->m.nonisothermal && !c->gov_pending && nsteps - t >= kF64GraphSteps) {
+      cudaGraphExec_t ge;
+      const int rc = f64_graph(c, &ge);
+      if (rc != GP_OK) return rc;
+      GP_CUDA(cudaGraphLaunch(ge, c->stream));
+      c->launches += 2 * kF64GraphSteps;
+      c->have_prev = 1;
+      c->tstep += kF64GraphSteps;
+      t += kF64GraphSteps - 1;
+      continue;
+    }
     const int nxt = 1 - c->cur;
     if (c->precision == GP_FP64) {
       const gp_temp_step ts = gp_temp_after(c->m, c->tstep);  // T reset after the previous step

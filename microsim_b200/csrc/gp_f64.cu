@@ -517,6 +517,26 @@ __device__ __forceinline__ void project_simplex_unweighted(const double* phi, co
   }
 }
 
+// True when the 3x3 phi block around a cell holds one value per phase and that value lies in
+// [0, 1] (so no NaN, infinity or negative value).  Every phi gradient of such a cell is then
+// +0 or -0: no phase is active (|divphi| = 0), the projection changes nothing, Delta-phi is
+// +0, and no face next to the cell carries an antitrapping current (each face's |grad phi| is
+// 0).  The kernels skip that arithmetic for such cells and store what it would give.
+template <int N>
+__device__ __forceinline__ bool flat_block(const double (&P)[3][3][N]) {
+  bool flat = true;
+#pragma unroll
+  for (int a = 0; a < N; a++) {
+    const double c = P[1][1][a];
+    flat = flat && c >= 0.0 && c <= 1.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) flat = flat && P[i][j][a] == c;
+  }
+  return flat;
+}
+
 // ---------------------------------------------------------------- kernels
 
 // Delta-phi on [-1, mx] x [-1, my] (interior plus the first ghost ring).
@@ -535,6 +555,12 @@ __global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_dphi(const __grid_const
   for (int i = 0; i < 3; i++)
 #pragma unroll
     for (int j = 0; j < 3; j++) load_phi<N>(phi, g, x + i - 1, y + j - 1, P[i][j]);
+  double* out = dphi + (int64_t)(x + 1) * g.rpitch + (y + 1);
+  if (flat_block<N>(P)) {  // no active phase: Delta-phi is +0
+#pragma unroll
+    for (int a = 0; a < N; a++) out[a * g.rplane] = 0.0;
+    return;
+  }
   double muc[K1];
   load_mu<K1>(mu, g, x, y, muc, N);
   const double two_dy = 2.0 * m.dy;
@@ -573,7 +599,6 @@ __global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_dphi(const __grid_const
   }
   if (SMOOTH) project_simplex_unweighted<N>(ph, divphi, dp);
   else project_simplex<N>(ph, divphi, dp);
-  double* out = dphi + (int64_t)(x + 1) * g.rpitch + (y + 1);
 #pragma unroll
   for (int a = 0; a < N; a++) out[a * g.rplane] = dp[a];
 }
@@ -748,29 +773,32 @@ __global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_update(const __grid_con
       Dr[a] = __ldg(r + a * g.rplane + 1);
     }
   }
-  const double two_dy = 2.0 * m.dy;
-  // gradient pieces the four faces need (calculate_gradients.h:92-131)
-  double gx_c[N], gx_b[N], gy_c[N], gy_l[N];
-  double cy_c[N], cy_b[N], cy_f[N], cx_c[N], cx_l[N], cx_r[N];
-#pragma unroll
-  for (int a = 0; a < N; a++) {
-    gx_c[a] = gp_ddiv((P[2][1][a] - P[1][1][a]), m.dx);
-    gx_b[a] = gp_ddiv((P[1][1][a] - P[0][1][a]), m.dx);
-    gy_c[a] = gp_ddiv((P[1][2][a] - P[1][1][a]), m.dy);
-    gy_l[a] = gp_ddiv((P[1][1][a] - P[1][0][a]), m.dy);
-    cy_c[a] = gp_ddiv((P[1][2][a] - P[1][0][a]), two_dy);
-    cy_b[a] = gp_ddiv((P[0][2][a] - P[0][0][a]), two_dy);
-    cy_f[a] = gp_ddiv((P[2][2][a] - P[2][0][a]), two_dy);
-    cx_c[a] = 0.5 * (gx_c[a] + gx_b[a]);
-    cx_l[a] = 0.5 * (gp_ddiv((P[2][0][a] - P[1][0][a]), m.dx) + gp_ddiv((P[1][0][a] - P[0][0][a]), m.dx));
-    cx_r[a] = 0.5 * (gp_ddiv((P[2][2][a] - P[1][2][a]), m.dx) + gp_ddiv((P[1][2][a] - P[0][2][a]), m.dx));
-  }
   // j_at on the four faces; the y-face at ghosted row MESH_Y-2 carries none
-  // (calculate_fluxes_concentration.h:65), i.e. interior row my-5
+  // (calculate_fluxes_concentration.h:65), i.e. interior row my-5.  A flat phi block
+  // carries none on any face (flat_block).
   double jx_c[K1], jx_b[K1], jy_c[K1], jy_l[K1];
+#pragma unroll
+  for (int k = 0; k < K1; k++) jx_c[k] = jx_b[k] = jy_c[k] = jy_l[k] = 0.0;
   // the cells' temperatures in the concentration half step (ghosts: their boundary copy)
   const Th thc = th_row(m, g, y, false), thl = th_row(m, g, y - 1, false), thr = th_row(m, g, y + 1, false);
-  if (!SMOOTH) {
+  if (!SMOOTH && !flat_block<N>(P)) {
+    const double two_dy = 2.0 * m.dy;
+    // gradient pieces the four faces need (calculate_gradients.h:92-131)
+    double gx_c[N], gx_b[N], gy_c[N], gy_l[N];
+    double cy_c[N], cy_b[N], cy_f[N], cx_c[N], cx_l[N], cx_r[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      gx_c[a] = gp_ddiv((P[2][1][a] - P[1][1][a]), m.dx);
+      gx_b[a] = gp_ddiv((P[1][1][a] - P[0][1][a]), m.dx);
+      gy_c[a] = gp_ddiv((P[1][2][a] - P[1][1][a]), m.dy);
+      gy_l[a] = gp_ddiv((P[1][1][a] - P[1][0][a]), m.dy);
+      cy_c[a] = gp_ddiv((P[1][2][a] - P[1][0][a]), two_dy);
+      cy_b[a] = gp_ddiv((P[0][2][a] - P[0][0][a]), two_dy);
+      cy_f[a] = gp_ddiv((P[2][2][a] - P[2][0][a]), two_dy);
+      cx_c[a] = 0.5 * (gx_c[a] + gx_b[a]);
+      cx_l[a] = 0.5 * (gp_ddiv((P[2][0][a] - P[1][0][a]), m.dx) + gp_ddiv((P[1][0][a] - P[0][0][a]), m.dx));
+      cx_r[a] = 0.5 * (gp_ddiv((P[2][2][a] - P[1][2][a]), m.dx) + gp_ddiv((P[1][2][a] - P[0][2][a]), m.dx));
+    }
     jat_face<N, K1>(m, gx_c, cy_c, cy_f, P[1][1], P[2][1], Mc, Mf, Dc, Df, false, jx_c, thc, thc);
     jat_face<N, K1>(m, gx_b, cy_b, cy_c, P[0][1], P[1][1], Mb, Mc, Db, Dc, false, jx_b, thc, thc);
     jat_face<N, K1>(m, gy_c, cx_c, cx_r, P[1][1], P[1][2], Mc, Mr, Dc, Dr, (y + 3 == g.my - 2), jy_c, thc, thr);
