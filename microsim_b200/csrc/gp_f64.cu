@@ -91,6 +91,27 @@ __device__ __forceinline__ void load_mu(const double* __restrict__ mu, const Geo
   for (int k = 0; k < K1; k++) out[k] = __ldg(p + k * g.plane);
 }
 
+// The 3x3 phi block around (x, y).  A cell whose block lies inside the grid reads it with plain
+// offsets; the others map each neighbour through the boundary copy (the same values).
+template <int N>
+__device__ __forceinline__ void load_block(const double* __restrict__ phi, const Geo& g, int x, int y,
+                                           double (&P)[3][3][N]) {
+  if (x >= 1 && x <= g.mx - 2 && y >= 1 && y <= g.my - 2) {
+    const double* p = phi + (int64_t)(x - 1) * g.pitch + (y - 1);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int a = 0; a < N; a++) P[i][j][a] = __ldg(p + i * g.pitch + j + a * g.plane);
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) load_phi<N>(phi, g, x + i - 1, y + j - 1, P[i][j]);
+}
+
 // ---------------------------------------------------------------- model terms
 
 // h_a(phi), functions/functionH.h:24-36
@@ -539,22 +560,25 @@ __device__ __forceinline__ bool flat_block(const double (&P)[3][3][N]) {
 
 // ---------------------------------------------------------------- kernels
 
+// Blocks of 256 per SM the kernels are compiled for: three for binary alloys (80 registers; the
+// compiler spills some of the interface cells' state, and the occupancy gained pays for it on many
+// small grids stepped at once, with no loss on one large grid), two for the other two-phase
+// kernels, one beyond (two of those spill heavily).
+#define GP_F64_BLOCKS(N, K1) ((N) == 2 && (K1) == 1 ? 3 : ((N) == 2 ? 2 : 1))
+
 // Delta-phi on [-1, mx] x [-1, my] (interior plus the first ghost ring).
 // SMOOTH: the smoothing pre-step (calculate_divergence_phasefield.h:63-158):
 // isotropic gradient energy, no dpsi, the unsigned potential when anisotropic,
 // unweighted projection.
 template <int N, int K1, bool SMOOTH>
-__global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_dphi(const __grid_constant__ gp_model m, Geo g,
+__global__ void __launch_bounds__(256, GP_F64_BLOCKS(N, K1)) k_dphi(const __grid_constant__ gp_model m, Geo g,
                                               const double* __restrict__ phi, const double* __restrict__ mu,
                                               double* __restrict__ dphi) {
   const int y = blockIdx.x * blockDim.x + threadIdx.x - 1;
   const int x = blockIdx.y * blockDim.y + threadIdx.y - 1;
   if (x > g.mx || y > g.my) return;
   double P[3][3][N];
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = 0; j < 3; j++) load_phi<N>(phi, g, x + i - 1, y + j - 1, P[i][j]);
+  load_block<N>(phi, g, x, y, P);
   double* out = dphi + (int64_t)(x + 1) * g.rpitch + (y + 1);
   if (flat_block<N>(P)) {  // no active phase: Delta-phi is +0
 #pragma unroll
@@ -743,7 +767,7 @@ __device__ __forceinline__ void lu_inverse(double (&mm)[K][K], double (&inv)[K][
 // (calculate_divergence_concentration.h:154-253): no antitrapping current, no
 // dh/dt source, the LU inverse (matinvnew) for every mu solve.
 template <int N, int K1, bool SMOOTH>
-__global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_update(const __grid_constant__ gp_model m, Geo g,
+__global__ void __launch_bounds__(256, GP_F64_BLOCKS(N, K1)) k_update(const __grid_constant__ gp_model m, Geo g,
                                                 const double* __restrict__ phi, const double* __restrict__ mu,
                                                 const double* __restrict__ dphi, double* __restrict__ phi_out,
                                                 double* __restrict__ mu_out) {
@@ -751,16 +775,25 @@ __global__ void __launch_bounds__(256, N == 2 ? 2 : 1) k_update(const __grid_con
   const int x = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= g.mx || y >= g.my) return;
   double P[3][3][N];
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = 0; j < 3; j++) load_phi<N>(phi, g, x + i - 1, y + j - 1, P[i][j]);
+  load_block<N>(phi, g, x, y, P);
   double Mc[K1], Mb[K1], Mf[K1], Ml[K1], Mr[K1];
-  load_mu<K1>(mu, g, x, y, Mc);
-  load_mu<K1>(mu, g, x - 1, y, Mb);
-  load_mu<K1>(mu, g, x + 1, y, Mf);
-  load_mu<K1>(mu, g, x, y - 1, Ml);
-  load_mu<K1>(mu, g, x, y + 1, Mr);
+  if (x >= 1 && x <= g.mx - 2 && y >= 1 && y <= g.my - 2) {  // the four neighbours inside the grid
+    const double* q = mu + (int64_t)x * g.pitch + y;
+#pragma unroll
+    for (int k = 0; k < K1; k++) {
+      Mc[k] = __ldg(q + k * g.plane);
+      Mb[k] = __ldg(q + k * g.plane - g.pitch);
+      Mf[k] = __ldg(q + k * g.plane + g.pitch);
+      Ml[k] = __ldg(q + k * g.plane - 1);
+      Mr[k] = __ldg(q + k * g.plane + 1);
+    }
+  } else {
+    load_mu<K1>(mu, g, x, y, Mc);
+    load_mu<K1>(mu, g, x - 1, y, Mb);
+    load_mu<K1>(mu, g, x + 1, y, Mf);
+    load_mu<K1>(mu, g, x, y - 1, Ml);
+    load_mu<K1>(mu, g, x, y + 1, Mr);
+  }
   double Dc[N], Db[N], Df[N], Dl[N], Dr[N];
   {
     const double* r = dphi + (int64_t)(x + 1) * g.rpitch + (y + 1);
