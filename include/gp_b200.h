@@ -194,7 +194,9 @@ int gp_download(gp_ctx *ctx, double *phi, double *mu);
 /* nsteps explicit steps: phase-field half step, ghost fill, concentration
  * half step, ghost fill -- microsim_gp.c:102-106 for t = 1..nsteps.
  * Asynchronous on the context's stream; errors of earlier launches surface here
- * or in gp_sync. */
+ * or in gp_sync.  An isothermal FP64 context replays runs of eight steps from a
+ * CUDA graph captured on the first such run from each of its two buffers (the
+ * same kernels and arguments as direct launches, one host launch instead of 16). */
 int gp_step(gp_ctx *ctx, int64_t nsteps);
 /* The context's step count (the frozen temperature gradient's clock: step t uses the temperature
  * the reference sets after step t - 1).  Starts at 0 on creation; gp_step advances it. */
