@@ -526,8 +526,11 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS
     } else if (glist) {  // block k starts with entry k, then takes entries grid, grid + 1, ... from the queue
       // (claimed when the block is free: the blocks whose first tiles finish early take the rest)
       const int i = iter == 0 ? (int)blockIdx.x : (int)gridDim.x + atomicAdd(&cnt[1], 1);
+      // the front entry is read together with the counts (an in-bounds read, used only when the
+      // count covers it), so the common case waits for one round trip instead of two
+      const int2 front = i < total ? glist[i] : make_int2(-1, 0);
       const int n0 = cnt[0];
-      if (i < n0) e = glist[i];
+      if (i < n0) e = front;
       else if (i < n0 + cnt[3]) e = glist[total - 1 - (i - n0)];
     } else if (iter == 0) {
       e = make_int2((int)blockIdx.x, tile_inst[blockIdx.x]);

@@ -86,6 +86,12 @@ def _oracle_run(case, steps):
         inp = mb.Input(ip, fp)
         m = inp.model()
         phi, mu = inp.fill(m)
+    op, om_ = _oracle_from(m, phi, mu, steps)
+    return m, phi, mu, op, om_
+
+
+def _oracle_from(m, phi, mu, steps):
+    """The oracle's state after `steps` steps from the interior fields phi, mu."""
     om = O.OracleModel(
         N=m.N, K1=m.K1, mesh_x=m.mesh_x, mesh_y=m.mesh_y, dx=m.dx, dy=m.dy, dt=m.dt, epsilon=m.epsilon, tau=m.tau,
         T=m.T, Teq=m.Teq, obstacle=m.obstacle, anisotropy=m.anisotropy, binary=int(m.mu_solver == mb.GP_MU_BINARY),
@@ -103,7 +109,7 @@ def _oracle_run(case, steps):
     gp[:, 3:-3, 3:-3], gm[:, 3:-3, 3:-3] = phi, mu
     O.apply_bc(om, gp, gm)
     O.step(om, gp, gm, steps)
-    return m, phi, mu, interior(gp), interior(gm)
+    return interior(gp), interior(gm)
 
 
 LONG = {
@@ -150,6 +156,32 @@ def test_graph_replayed_steps_equal_single_steps():
             p1, u1 = one.download()
             pn, un = many.download()
             assert np.array_equal(p1, pn) and np.array_equal(u1, un), (done, n)
+
+
+def test_flat_blocks_outside_the_simplex_take_the_full_evaluation():
+    """The kernels skip the arithmetic of cells whose 3x3 phi block is one value per phase in
+    [0, 1].  Flat patches just outside that range (a phase slightly negative, whose projection
+    still changes Delta-phi, and one slightly above one) and a flat patch inside the interface
+    range (0.5 / 0.5) step bit-exactly like the oracle."""
+    case = configs.binary_case(40, 36, gap=1.0, supersat=0.5, eps=2.0, delta=0.02, dt=0.05, tau=0.9,
+                               seed=(10, 10, 5.0), steps=20)
+    with tempfile.TemporaryDirectory() as d:
+        ip, fp = case.write(d)
+        inp = mb.Input(ip, fp)
+        m = inp.model()
+        phi, mu = inp.fill(m)
+    phi = phi.copy()
+    phi[0, 24:34, 4:14], phi[1, 24:34, 4:14] = -1e-3, 1.0 + 1e-3
+    phi[0, 4:14, 22:32], phi[1, 4:14, 22:32] = 0.5, 0.5
+    phi[0, 24:34, 22:32], phi[1, 24:34, 22:32] = 1.0 + 2e-3, -2e-3
+    op, om_ = _oracle_from(m, phi, mu, 20)
+    with mb.Context(m, mb.GP_FP64) as ctx:
+        ctx.upload(phi, mu)
+        for n in (1, 19):  # one direct step, then a graph replay and direct steps
+            ctx.step(n)
+        p, u = ctx.download()
+    assert np.array_equal(p, op), f"phi max |diff| {np.abs(p - op).max()}"
+    assert np.array_equal(u, om_), f"mu max |diff| {np.abs(u - om_).max()}"
 
 
 RAGGED = [(4, 4, (1, 1, 1, 1)), (5, 7, (3, 3, 3, 3)), (4, 37, (1, 1, 3, 3)), (33, 5, (3, 3, 1, 1)),
