@@ -205,6 +205,14 @@ __global__ void __launch_bounds__(256) k_rev_cell(const AM<T> m, Geo g, const T*
   gdj[o] = dj;
 }
 
+// Scatter of one adjoint contribution; a zero one is skipped (most faces of a bulk region carry no
+// antitrapping current, so most of their tangential and Delta-phi adjoints are zero).  The float
+// sums are order-dependent anyway (atomics); skipping a +-0 addend changes at most a zero's sign.
+template <typename T>
+__device__ __forceinline__ void add_nz(T* p, T v) {
+  if (v != (T)0) atomicAdd(p, v);
+}
+
 // 3. reverse of the face fluxes; thread = one face (lower cell (x, y)):
 // x-faces for x in [-1, mx-1], y in [0, my-1]; y-faces for x in [0, mx-1], y in [-1, my-1]
 template <typename T>
@@ -251,25 +259,25 @@ __global__ void __launch_bounds__(256) k_rev_face(const AM<T> m, Geo g, const T*
     if (lJ != (T)0) jface_rev(m, f, lJ, L, lp);
     for (int p = 0; p < NPARAM; p++) lpd[p] = (double)lp[p];
     for (int a = 0; a < 2; a++) {
-      atomicAdd(lam_out + ix_phi(g, x, y, a), L.pc[a]);
-      atomicAdd(lam_out + ix_phi(g, xn, yn, a), L.pn[a]);
+      add_nz(lam_out + ix_phi(g, x, y, a), L.pc[a]);
+      add_nz(lam_out + ix_phi(g, xn, yn, a), L.pn[a]);
       if (dir == 0) {
-        atomicAdd(lam_out + ix_phi(g, x, y + 1, a), L.tc[a] / ty);
-        atomicAdd(lam_out + ix_phi(g, x, y - 1, a), -L.tc[a] / ty);
-        atomicAdd(lam_out + ix_phi(g, xn, y + 1, a), L.tn[a] / ty);
-        atomicAdd(lam_out + ix_phi(g, xn, y - 1, a), -L.tn[a] / ty);
+        add_nz(lam_out + ix_phi(g, x, y + 1, a), L.tc[a] / ty);
+        add_nz(lam_out + ix_phi(g, x, y - 1, a), -L.tc[a] / ty);
+        add_nz(lam_out + ix_phi(g, xn, y + 1, a), L.tn[a] / ty);
+        add_nz(lam_out + ix_phi(g, xn, y - 1, a), -L.tn[a] / ty);
       } else {
         const T hc = (T)0.5 * L.tc[a] / m.dx, hn = (T)0.5 * L.tn[a] / m.dx;
-        atomicAdd(lam_out + ix_phi(g, x + 1, y, a), hc);
-        atomicAdd(lam_out + ix_phi(g, x - 1, y, a), -hc);
-        atomicAdd(lam_out + ix_phi(g, x + 1, yn, a), hn);
-        atomicAdd(lam_out + ix_phi(g, x - 1, yn, a), -hn);
+        add_nz(lam_out + ix_phi(g, x + 1, y, a), hc);
+        add_nz(lam_out + ix_phi(g, x - 1, y, a), -hc);
+        add_nz(lam_out + ix_phi(g, x + 1, yn, a), hn);
+        add_nz(lam_out + ix_phi(g, x - 1, yn, a), -hn);
       }
     }
-    atomicAdd(lam_out + ix_mu(g, x, y), L.muc);
-    atomicAdd(lam_out + ix_mu(g, xn, yn), L.mun);
-    atomicAdd(ldphi + ix_ring(g, x, y, 0), L.dpc);
-    atomicAdd(ldphi + ix_ring(g, xn, yn, 0), L.dpn);
+    add_nz(lam_out + ix_mu(g, x, y), L.muc);
+    add_nz(lam_out + ix_mu(g, xn, yn), L.mun);
+    add_nz(ldphi + ix_ring(g, x, y, 0), L.dpc);
+    add_nz(ldphi + ix_ring(g, xn, yn, 0), L.dpn);
   }
   reduce_params(lpd, grad);
 }
