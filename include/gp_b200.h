@@ -284,6 +284,16 @@ int gp_batch_step(gp_batch *b, int64_t nsteps);
 int gp_batch_prepare(gp_batch *b);
 int gp_batch_sync(gp_batch *b);
 int gp_batch_get_stats(gp_batch *b, int i, gp_stats *out);
+/* gp_batch_get_stats queued on the batch's stream without waiting: the
+ * GP_STAT_VALUES reduced FP64 values of instance i land in raw (page-locked host
+ * memory of GP_STAT_VALUES doubles, left untouched until gp_batch_sync or a call
+ * that waits) when the stream gets there, so a loop can read every step's
+ * statistics back without holding the GPU at each step.  gp_batch_stats_from_raw
+ * then fills a gp_stats from them, with gp_batch_get_stats's return codes
+ * (GP_E_NONFINITE, GP_E_TIMEOUT). */
+#define GP_STAT_VALUES 64
+int gp_batch_get_stats_async(gp_batch *b, int i, double *raw);
+int gp_batch_stats_from_raw(gp_batch *b, int i, const double *raw, gp_stats *out);
 /* Tile shape of the fused kernel (tx along x, ty along y): 16x32, 8x32, 32x32, 16x64. */
 int gp_batch_set_tile(gp_batch *b, int tx, int ty);
 /* Narrow band (on by default): tiles whose cells and two-cell ring were one

@@ -26,6 +26,7 @@ GP_OK, GP_E_ARG, GP_E_IO, GP_E_PARSE, GP_E_UNSUPPORTED, GP_E_CUDA, GP_E_NONFINIT
 GP_MU_BINARY, GP_MU_TERNARY, GP_MU_DILUTE, GP_MU_LU = 0, 1, 2, 3
 GP_FP64, GP_FP32 = 0, 1
 GP_BC_NEUMANN, GP_BC_PERIODIC = 1, 3
+GP_STAT_VALUES = 64  # reduced FP64 values of one statistics read-back (include/gp_b200.h)
 
 _P, _K = GP_MAX_PHASES, GP_MAX_K1
 
@@ -125,6 +126,8 @@ _SIGS = {
     "gp_batch_step": (C.c_int, [C.c_void_p, C.c_int64]),
     "gp_batch_sync": (C.c_int, [C.c_void_p]),
     "gp_batch_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(GpStats)]),
+    "gp_batch_get_stats_async": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "gp_batch_stats_from_raw": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(GpStats)]),
     "gp_batch_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gp_batch_set_narrowband": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_batch_set_grids": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
@@ -483,6 +486,23 @@ class Batch:
         rc = lib().gp_batch_get_stats(self._h, i, C.byref(st))
         if rc != GP_OK and not (allow_nonfinite and rc == GP_E_NONFINITE):
             raise GpError("gp_batch_get_stats", rc)
+        return _stats_dict(st, self.models[i].N, self.models[i].K1)
+
+    def stats_async(self, i: int, raw: np.ndarray):
+        """Queue instance i's statistics read-back into `raw` (page-locked, C-contiguous float64,
+        GP_STAT_VALUES entries) without waiting; after sync(), stats_from_raw(i, raw) decodes it."""
+        if raw.dtype != np.float64 or raw.size < GP_STAT_VALUES or not raw.flags.c_contiguous:
+            raise ValueError(f"raw must be a C-contiguous float64 array of at least {GP_STAT_VALUES} values")
+        _check("gp_batch_get_stats_async", lib().gp_batch_get_stats_async(self._h, i, raw.ctypes.data))
+
+    def stats_from_raw(self, i: int, raw: np.ndarray, allow_nonfinite: bool = False) -> dict:
+        st = GpStats()
+        v = np.ascontiguousarray(raw, dtype=np.float64)
+        if v.size < GP_STAT_VALUES:
+            raise ValueError(f"raw must hold {GP_STAT_VALUES} values")
+        rc = lib().gp_batch_stats_from_raw(self._h, i, v.ctypes.data, C.byref(st))
+        if rc != GP_OK and not (allow_nonfinite and rc == GP_E_NONFINITE):
+            raise GpError("gp_batch_stats_from_raw", rc)
         return _stats_dict(st, self.models[i].N, self.models[i].K1)
 
     def set_tile(self, tx: int, ty: int):

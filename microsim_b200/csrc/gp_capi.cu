@@ -1234,8 +1234,8 @@ extern "C" int gp_batch_sync(gp_batch* b) {
   return GP_OK;
 }
 
-extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
-  if (!b || i < 0 || i >= b->n || !out) return GP_E_ARG;
+// The statistics kernels of instance i, ending with the GP_STAT_VALUES reduced values in b->reduced.
+static int batch_stats_launch(gp_batch* b, int i) {
   const gp_model& m = b->models[i];
   const int cur = b->parity, prv = 1 - b->parity;
   launch_stats<float>(m, b->red_blocks, b->stream, b->pool + b->off_phi[cur][i], b->pool + b->off_mu[cur][i],
@@ -1246,9 +1246,12 @@ extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
                                          gp_f32_batch_error_word(b->f32));
   GP_CUDA(cudaGetLastError());
   b->launches += 2;
-  double v[64];
-  GP_CUDA(cudaMemcpyAsync(v, b->reduced, sizeof v, cudaMemcpyDeviceToHost, b->stream));
-  GP_CUDA(cudaStreamSynchronize(b->stream));
+  return GP_OK;
+}
+
+// gp_stats of instance i from its reduced values v (the layout k_stats_final writes).
+static int batch_stats_decode(const gp_batch* b, int i, const double* v, gp_stats* out) {
+  const gp_model& m = b->models[i];
   if (v[63] != 0.0) return lean_error();
   const StatLayout L{m.N, m.K1};
   memset(out, 0, sizeof *out);
@@ -1267,6 +1270,29 @@ extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
   out->nonfinite = (int64_t)v[L.nonfinite()];
   stats_energies(m, L, v, out);
   return out->nonfinite ? GP_E_NONFINITE : GP_OK;
+}
+
+extern "C" int gp_batch_get_stats(gp_batch* b, int i, gp_stats* out) {
+  if (!b || i < 0 || i >= b->n || !out) return GP_E_ARG;
+  int rc = batch_stats_launch(b, i);
+  if (rc != GP_OK) return rc;
+  double v[GP_STAT_VALUES];
+  GP_CUDA(cudaMemcpyAsync(v, b->reduced, sizeof v, cudaMemcpyDeviceToHost, b->stream));
+  GP_CUDA(cudaStreamSynchronize(b->stream));
+  return batch_stats_decode(b, i, v, out);
+}
+
+extern "C" int gp_batch_get_stats_async(gp_batch* b, int i, double* raw) {
+  if (!b || i < 0 || i >= b->n || !raw) return GP_E_ARG;
+  int rc = batch_stats_launch(b, i);
+  if (rc != GP_OK) return rc;
+  GP_CUDA(cudaMemcpyAsync(raw, b->reduced, GP_STAT_VALUES * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  return GP_OK;
+}
+
+extern "C" int gp_batch_stats_from_raw(gp_batch* b, int i, const double* raw, gp_stats* out) {
+  if (!b || i < 0 || i >= b->n || !raw || !out) return GP_E_ARG;
+  return batch_stats_decode(b, i, raw, out);
 }
 
 extern "C" int gp_batch_set_tile(gp_batch* b, int tx, int ty) {

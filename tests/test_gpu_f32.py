@@ -398,6 +398,42 @@ def test_isotropic_and_anisotropic_instances_in_one_batch():
                     assert np.abs(p1 - p0).max() <= 1e-5 and np.abs(u1 - u0).max() <= 1e-5, (depth, i)
 
 
+def test_queued_statistics_equal_the_waiting_ones():
+    """Statistics read back queued after every step (no host wait per step, one sync at the end)
+    decode to exactly what the waiting call returns after the same steps, for every instance."""
+    cases = [configs.binary_case(96, 64, gap=1.0, supersat=0.55, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
+                                 seed=(0, 0, 8.0)),
+             configs.binary_case(160, 128, gap=1.0, supersat=0.5, eps=4.0, delta=0.02, dt=0.05, tau=1.7776,
+                                 seed=(80, 64, 9.0))]
+    loaded = [mb.load_case(c) for c in cases]
+    models = [m for m, _, _ in loaded]
+    import torch
+    steps = 12
+    raw = torch.zeros((steps, len(models), mb.GP_STAT_VALUES), dtype=torch.float64, pin_memory=True).numpy()
+    want = []
+    with mb.Batch(models) as b:
+        for i, (_, p, u) in enumerate(loaded):
+            b.upload(i, p, u)
+        for t in range(steps):
+            b.step(1)
+            want.append([b.stats(i) for i in range(len(models))])
+    with mb.Batch(models) as b:
+        for i, (_, p, u) in enumerate(loaded):
+            b.upload(i, p, u)
+        for t in range(steps):
+            b.step(1)
+            for i in range(len(models)):
+                b.stats_async(i, raw[t, i])
+        b.sync()
+        for t in range(steps):
+            for i in range(len(models)):
+                got = b.stats_from_raw(i, raw[t, i])
+                for k, v in want[t][i].items():
+                    assert np.array_equal(np.asarray(got[k]), np.asarray(v)), (t, i, k)
+        with pytest.raises(ValueError):
+            b.stats_async(0, np.zeros(8))
+
+
 def test_async_upload_download_equal_the_waiting_ones():
     """Queued uploads and downloads of every instance (no host wait between instances, one sync),
     through the staging buffer (pageable arrays) or read and written in place by the conversion
