@@ -491,6 +491,10 @@ __global__ void __launch_bounds__(THREADS, (N == 2 && K1 == 1) ? 1024 / THREADS
     s_scan_n = s_scan_k = s_chunk = 0;
     s_scan_done = (int)blockIdx.x >= total;
   }
+  // Launched as a programmatic dependent of the tile list (the blocks start while the list kernel
+  // runs): nothing an earlier kernel wrote is read before this wait, which returns once the list
+  // kernel and everything before it have completed.  Without that launch attribute it returns at once.
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
 
   for (int iter = 0;; iter++) {
   __syncthreads();  // the previous tile's shared state is no longer read
@@ -2039,6 +2043,8 @@ __global__ void __launch_bounds__(256) k_general_list(const int4* __restrict__ t
                                                       const uint32_t* __restrict__ flags_in, int total,
                                                       int2* __restrict__ glist, int* __restrict__ cnt,
                                                       uint8_t* __restrict__ genb, int depth) {
+  // the full kernel that reads this list may start its blocks now; they wait for this kernel's end
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   int4 d = make_int4(0, 0, 0, 0);
   if (t < total) d = tile_desc[t];
@@ -2706,6 +2712,24 @@ static cudaError_t timing_slot(gp_f32_batch* b, int steps, cudaEvent_t** E) {
   return cudaSuccess;
 }
 
+// The full kernel launched right after the tile list on the same stream, as its programmatic
+// dependent: its blocks are scheduled while the list kernel runs and wait in the kernel
+// (griddepcontrol.wait) for the list, instead of the launch waiting for the list to finish.
+template <typename Fn, typename... Args>
+static cudaError_t launch_after_list(Fn fn, int grid, int threads, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, fn, args...);
+}
+
 // One step of every instance, reading buffer parity `parity`.
 cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   const KernelSet& k = b->ks;
@@ -2754,10 +2778,16 @@ cudaError_t gp_f32_batch_launch(gp_f32_batch* b, int parity, cudaStream_t s) {
   }
   if (E && ((e = cudaEventRecord(E[3], s)) != cudaSuccess)) return e;
   if (E && ((e = cudaEventRecord(E[4], s)) != cudaSuccess)) return e;
-  (b->step_threads == 512 ? k.general_wide : k.general)<<<b->grid_general, b->step_threads, k.smem_general, s>>>(
-      b->dinst[p], b->dmodel, b->dtile_inst, b->scan ? nullptr : b->dglist, b->scan ? nullptr : b->dcnt, flags_out,
-      b->total_tiles, b->scan ? b->dtile_desc : nullptr, b->scan ? flags_in : nullptr, 0);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  auto full = b->step_threads == 512 ? k.general_wide : k.general;
+  if (b->scan || E)  // no list kernel before it, or timed launches (events between the two)
+    full<<<b->grid_general, b->step_threads, k.smem_general, s>>>(
+        b->dinst[p], b->dmodel, b->dtile_inst, b->scan ? nullptr : b->dglist, b->scan ? nullptr : b->dcnt, flags_out,
+        b->total_tiles, b->scan ? b->dtile_desc : nullptr, b->scan ? flags_in : nullptr, 0);
+  else
+    e = launch_after_list(full, b->grid_general, b->step_threads, k.smem_general, s, (const Inst*)b->dinst[p],
+                          (const Model*)b->dmodel, (const int*)b->dtile_inst, (const int2*)b->dglist, b->dcnt,
+                          flags_out, b->total_tiles, (const int4*)nullptr, (const uint32_t*)nullptr, 0);
+  if (e != cudaSuccess || (e = cudaGetLastError()) != cudaSuccess) return e;
   if (b->noniso) {
     k_tick<<<1, 1, 0, s>>>(b->dtstep);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -2812,9 +2842,15 @@ cudaError_t gp_f32_batch_launch_pair(gp_f32_batch* b, int parity, cudaStream_t s
   }
   if (E && (e = cudaEventRecord(E[1], ls)) != cudaSuccess) return e;
   if (E && (e = cudaEventRecord(E[4], s)) != cudaSuccess) return e;
-  full<<<b->grid_general, b->step_threads, k.smem_general, s>>>(b->dinst_x1[p], b->dmodel, b->dtile_inst, b->dglist,
-                                                                 b->dcnt, flags_x, b->total_tiles, nullptr, nullptr, 1);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (E)
+    full<<<b->grid_general, b->step_threads, k.smem_general, s>>>(b->dinst_x1[p], b->dmodel, b->dtile_inst,
+                                                                   b->dglist, b->dcnt, flags_x, b->total_tiles,
+                                                                   nullptr, nullptr, 1);
+  else
+    e = launch_after_list(full, b->grid_general, b->step_threads, k.smem_general, s, (const Inst*)b->dinst_x1[p],
+                          (const Model*)b->dmodel, (const int*)b->dtile_inst, (const int2*)b->dglist, b->dcnt,
+                          flags_x, b->total_tiles, (const int4*)nullptr, (const uint32_t*)nullptr, 1);
+  if (e != cudaSuccess || (e = cudaGetLastError()) != cudaSuccess) return e;
   if (b->noniso) {
     k_tick<<<1, 1, 0, s>>>(b->dtstep);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
