@@ -1376,22 +1376,24 @@ extern "C" int gp_batch_autotune(gp_batch* b, const char* cache_path, int* tx_ou
       const int lp = c == 0 ? 0 : (c == 1 ? occ_l - 1 : occ_l / 2), gq = cg ? occ_g - 1 : 0;
       gp_f32_batch_set_grids(b->f32, lp, gq);
       gp_f32_batch_set_scan(b->f32, sc);
-      // timed as the steps run: one replay of the step graph (graph_steps steps) to warm up, four timed
+      // timed as the steps run: one replay of the step graph (graph_steps steps) to warm up, kTuneReplays
+      // timed (enough steps that run-to-run noise does not decide between close candidates)
+      constexpr int kTuneReplays = 12;
       batch_drop_graphs(b);
       int rc = batch_capture(b, b->parity);
       if (rc != GP_OK) return rc;
       GP_CUDA(cudaGraphLaunch(b->graph[b->parity], b->stream));
       GP_CUDA(cudaEventRecord(e0, b->stream));
-      for (int r = 0; r < 4; r++) GP_CUDA(cudaGraphLaunch(b->graph[b->parity], b->stream));
+      for (int r = 0; r < kTuneReplays; r++) GP_CUDA(cudaGraphLaunch(b->graph[b->parity], b->stream));
       GP_CUDA(cudaEventRecord(e1, b->stream));
       GP_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
       GP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      ms *= 10.0f / (float)(4 * b->graph_steps);  // per 10 steps, as the cache records
-      b->launches += (int64_t)5 * (b->graph_steps / dp) * batch_launches(b);
+      ms *= 10.0f / (float)(kTuneReplays * b->graph_steps);  // per 10 steps, as the cache records
+      b->launches += (int64_t)(kTuneReplays + 1) * (b->graph_steps / dp) * batch_launches(b);
       batch_drop_graphs(b);
-      // a reduced grid must win by 3%: at equal speed the kernels keep their occupancy
-      if ((c || cg) ? ms < 0.97f * best : ms < best) {
+      // a reduced grid must win by 1%: at equal speed the kernels keep their occupancy
+      if ((c || cg) ? ms < 0.99f * best : ms < best) {
         best = ms;
         best_tx = tx;
         best_ty = ty;
